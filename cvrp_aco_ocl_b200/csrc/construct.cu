@@ -1,0 +1,452 @@
+// construct.cu -- route construction, one CVRP tour per ant.
+//
+// construct_parity_kernel restates construct_solution + independent_roulette
+// (cvrp_ocl/gpu/kernel.cl:325-373, 382-493) bit for bit:
+//   * The reference runs one work-group of nloc work-items per ant; work-item l
+//     owns a Park-Miller state and draws one number for every node
+//     i = l, l+nloc, ... at every step (kernel.cl:331-337).  Here an ant is
+//     32*WPA threads; the node i of thread t is i = t + 32*WPA*j, its lane is
+//     l = i mod nloc (thread t owns exactly the lanes l = t mod 32*WPA) and its
+//     draw index inside the step is k = i / nloc, so the number is
+//     state_l * 16807^(k+1) mod m.  After the step every lane jumps by
+//     16807^(draws of lane l).
+//   * The argmax tournament (kernel.cl:343-366) keeps the left operand on ties;
+//     the winner among equal maxima is the node with the smallest tournament
+//     rank, precomputed on the host.  A 32-bit key ((0xFFFF - rank) << 16 | node)
+//     turns the tournament into two redux.sync.max reductions.
+//   * value == 0 means "no candidate": return to the depot (kernel.cl:461-465).
+// construct_nn_kernel is the throughput mode (no reference counterpart):
+// warp-per-ant roulette over a nearest-neighbour candidate list staged in
+// shared memory by TMA bulk copies, with warp-shuffle prefix sums.
+//
+// Rows of total_info and the lookup tables are staged into shared memory with
+// 1-D cp.async.bulk copies (no cluster multicast) completing on an mbarrier.
+#include <cuda_runtime.h>
+
+#include "aco_device.cuh"
+#include "kernels.h"
+
+namespace aco {
+
+namespace {
+
+__host__ __device__ inline size_t al128(size_t x) { return (x + 127) & ~(size_t)127; }
+
+struct ParityLayout {
+    size_t bar, dem, key, d0, jump, adv, state, red, mat, bytes;
+};
+
+__host__ __device__ inline ParityLayout parity_layout(int n, int nloc, int kmax, int wpa, int apc, bool smat)
+{
+    const size_t n4 = (size_t)((n + 3) & ~3), k4 = (size_t)((kmax + 3) & ~3);
+    ParityLayout L;
+    size_t o = 0;
+    L.bar = o; o = al128(o + 16);
+    L.dem = o; o = al128(o + n4 * 4);
+    L.key = o; o = al128(o + n4 * 4);
+    L.d0 = o; o = al128(o + n4 * 4);
+    L.jump = o; o = al128(o + k4 * 4);
+    L.adv = o; o = al128(o + (size_t)nloc * 4);
+    L.state = o; o = al128(o + (size_t)apc * nloc * 4);
+    L.red = o; o = al128(o + (size_t)apc * 2 * wpa * 2 * 4);
+    L.mat = o;
+    if (smat) o = al128(o + (size_t)n * n4 * 4);
+    L.bytes = o;
+    return L;
+}
+
+__device__ __forceinline__ uint32_t pm_norm(int x)
+{
+    long long r = (long long)x % (long long)kPM;
+    if (r < 0) r += kPM;
+    return (uint32_t)r;
+}
+
+template <int WPA, bool FIN, bool SMAT>
+__global__ void __launch_bounds__(512) construct_parity_kernel(ConstructArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int TPA = 32 * WPA;
+    const int n = a.n, ld = a.ld, nloc = a.nloc;
+    const int n4 = (n + 3) & ~3, k4 = (a.kmax + 3) & ~3;
+    const int apc = blockDim.x / TPA;
+    const ParityLayout L = parity_layout(n, nloc, a.kmax, WPA, apc, SMAT);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar);
+    int *s_dem = reinterpret_cast<int *>(smem + L.dem);
+    uint32_t *s_key = reinterpret_cast<uint32_t *>(smem + L.key);
+    float *s_d0 = reinterpret_cast<float *>(smem + L.d0);
+    uint32_t *s_jump = reinterpret_cast<uint32_t *>(smem + L.jump);
+    uint32_t *s_adv = reinterpret_cast<uint32_t *>(smem + L.adv);
+    uint32_t *s_state = reinterpret_cast<uint32_t *>(smem + L.state);
+    uint32_t *s_red = reinterpret_cast<uint32_t *>(smem + L.red);
+    float *s_mat = reinterpret_cast<float *>(smem + L.mat);
+
+    // ---- stage instance-wide tables (and the whole total_info matrix when it fits)
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t bytes = (uint32_t)(2 * n4 * 4 + k4 * 4 + nloc * 4);
+        if (SMAT) bytes += (uint32_t)(n * n4 * 4);
+        mbar_arrive_expect_tx(bar, bytes);
+        tma_bulk_g2s(s_dem, a.demand, n4 * 4, bar);
+        tma_bulk_g2s(s_key, a.tiekey, n4 * 4, bar);
+        tma_bulk_g2s(s_jump, a.jump, k4 * 4, bar);
+        tma_bulk_g2s(s_adv, a.adv, nloc * 4, bar);
+    }
+    if (SMAT)
+        for (int r = threadIdx.x; r < n; r += blockDim.x)
+            tma_bulk_g2s(s_mat + (size_t)r * n4, a.total + (size_t)r * ld, n4 * 4, bar);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_d0[i] = a.dist[(size_t)i * ld]; // column 0
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) set_status(a.status, ACO_ERR_TIMEOUT);
+        if (!ok) mbar_wait(bar, 0);
+        return;
+    }
+
+    // ---- one ant per 32*WPA threads
+    const int slot = threadIdx.x / TPA;
+    const int t = threadIdx.x - slot * TPA;
+    const int lane = threadIdx.x & 31;
+    const int wsl = t >> 5;
+    const int ant = blockIdx.x * apc + slot;
+    if (ant >= a.n_ants) return;
+    const int nlanes = n < nloc ? n : nloc;
+    uint32_t *st = s_state + (size_t)slot * nloc;
+    int *seeds = a.seeds + (size_t)ant * nloc;
+    for (int l = t; l < nlanes; l += TPA) st[l] = pm_norm(seeds[l]);
+
+    const int J = (n + TPA - 1) / TPA; // nodes per thread (<= 32: visited bits fit one register)
+    uint32_t vis = (t == 0) ? 1u : 0u; // node 0 (the depot) starts visited (kernel.cl:431)
+    int cur = 0, step = 0, vcnt = 1, load = 0, err = 0;
+    float rdist = 0.f, tdist = 0.f, pend = 0.f;
+    int *tour = a.solutions + (size_t)ant * a.T;
+    if (t == 0) tour[0] = 0;
+    const float *base = SMAT ? s_mat : a.total;
+    const size_t stride = SMAT ? (size_t)n4 : (size_t)ld;
+    const int lmask = nloc - 1;
+
+    while (vcnt < n) {
+        if (step >= a.T - 3) { // 2n-3 steps is the longest valid tour
+            err = ACO_ERR_STEP_LIMIT;
+            break;
+        }
+        const float *trow = base + (size_t)cur * stride;
+        const float *drow = a.dist + (size_t)cur * ld;
+        uint32_t bhi = 0u, blo = 0u;
+#pragma unroll 4
+        for (int j = 0; j < J; j++) {
+            const int i = t + TPA * j;
+            if (i < n) {
+                const uint32_t x = pm_mul(st[i & lmask], s_jump[i >> a.log2_nloc]);
+                const float r = __fadd_rn(pm_uniform(x), 0.001f);  // ran01 + 0.001f
+                const float p = __fmul_rn(trow[i], 100.0f);         // total_info * 100
+                const float v = __fmul_rn(r, p);
+                bool c = !((vis >> j) & 1u) && (load + s_dem[i] <= a.capacity);
+                if (FIN)
+                    c = c && (__fadd_rn(__fadd_rn(rdist, __fadd_rn(drow[i], a.serv_time)), s_d0[i]) <= a.max_dist);
+                const uint32_t vb = c ? __float_as_uint(v) : 0u; // r*p*c with c in {0,1}
+                const uint32_t key = s_key[i];
+                if (vb > bhi || (vb == bhi && key > blo)) {
+                    bhi = vb;
+                    blo = key;
+                }
+            }
+        }
+        uint32_t whi = __reduce_max_sync(0xffffffffu, bhi);
+        uint32_t wlo = __reduce_max_sync(0xffffffffu, bhi == whi ? blo : 0u);
+        if (WPA > 1) {
+            uint32_t *red = s_red + ((size_t)(slot * 2 + (step & 1)) * WPA) * 2;
+            if (lane == 0) {
+                red[2 * wsl] = whi;
+                red[2 * wsl + 1] = wlo;
+            }
+            named_barrier(1 + slot, TPA);
+            whi = 0u;
+            wlo = 0u;
+#pragma unroll
+            for (int w = 0; w < WPA; w++) {
+                const uint32_t h = red[2 * w], l2 = red[2 * w + 1];
+                if (h > whi || (h == whi && l2 > wlo)) {
+                    whi = h;
+                    wlo = l2;
+                }
+            }
+        }
+        step++;
+        int nxt;
+        if (whi == 0u) { // no candidate: back to the depot (kernel.cl:461-465)
+            nxt = 0;
+            load = 0;
+            rdist = 0.f;
+        } else {
+            nxt = (int)(wlo & 0xFFFFu);
+            load += s_dem[nxt];
+            if (FIN) rdist = __fadd_rn(rdist, __fadd_rn(drow[nxt], a.serv_time));
+            vcnt++;
+            if (nxt % TPA == t) vis |= 1u << (nxt / TPA);
+        }
+        if (t == 0) { // tour_dist += dist_wrk[nxt] one step late, in the same order
+            tdist = __fadd_rn(tdist, pend);
+            pend = __ldg(drow + nxt);
+            tour[step] = nxt;
+        }
+        cur = nxt;
+        for (int l = t; l < nlanes; l += TPA) st[l] = pm_mul(st[l], s_adv[l]);
+    }
+
+    if (err) {
+        if (t == 0) {
+            tour[a.T - 1] = 0;
+            a.lens[ant] = __int_as_float(0x7f800000);
+            set_status(a.status, err);
+        }
+    } else if (t == 0) { // kernel.cl:482-488
+        tdist = __fadd_rn(tdist, pend);
+        tdist = __fadd_rn(tdist, s_d0[cur]);
+        step++;
+        tour[step] = 0;
+        tour[a.T - 1] = step + 1;
+        a.lens[ant] = tdist;
+    }
+    if (step > 0) // rnd_seeds[gid] = rnd_seed (kernel.cl:492) for every lane that drew
+        for (int l = t; l < nlanes; l += TPA) seeds[l] = (int)st[l];
+}
+
+// ---------------------------------------------------------------------------
+// Throughput mode.
+// ---------------------------------------------------------------------------
+struct NNLayout {
+    size_t bar, dem, d0, nn, chc, vis, mat, bytes;
+};
+
+__host__ __device__ inline NNLayout nn_layout(int n, int Kp, int apc, bool smat)
+{
+    const size_t n4 = (size_t)((n + 3) & ~3);
+    const size_t words = (size_t)((n + 31) / 32);
+    NNLayout L;
+    size_t o = 0;
+    L.bar = o; o = al128(o + 16);
+    L.dem = o; o = al128(o + n4 * 4);
+    L.d0 = o; o = al128(o + n4 * 4);
+    L.nn = o; o = al128(o + (size_t)n * Kp * 2);
+    L.chc = o;
+    if (!smat) o = al128(o + (size_t)n * Kp * 4);
+    L.vis = o; o = al128(o + (size_t)apc * words * 4);
+    L.mat = o;
+    if (smat) o = al128(o + (size_t)n * n4 * 4);
+    L.bytes = o;
+    return L;
+}
+
+template <bool FIN, bool SMAT>
+__global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp;
+    const int n4 = (n + 3) & ~3;
+    const int apc = blockDim.x >> 5;
+    const NNLayout L = nn_layout(n, Kp, apc, SMAT);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar);
+    int *s_dem = reinterpret_cast<int *>(smem + L.dem);
+    float *s_d0 = reinterpret_cast<float *>(smem + L.d0);
+    uint16_t *s_nn = reinterpret_cast<uint16_t *>(smem + L.nn);
+    float *s_chc = reinterpret_cast<float *>(smem + L.chc);
+    uint32_t *s_vis = reinterpret_cast<uint32_t *>(smem + L.vis);
+    float *s_mat = reinterpret_cast<float *>(smem + L.mat);
+    const int words = (n + 31) >> 5;
+
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t bytes = (uint32_t)(n4 * 4 + n * Kp * 2);
+        if (SMAT) bytes += (uint32_t)(n * n4 * 4);
+        mbar_arrive_expect_tx(bar, bytes);
+        tma_bulk_g2s(s_dem, a.demand, n4 * 4, bar);
+        tma_bulk_g2s(s_nn, a.nn16, n * Kp * 2, bar);
+    }
+    if (SMAT) {
+        for (int r = threadIdx.x; r < n; r += blockDim.x)
+            tma_bulk_g2s(s_mat + (size_t)r * n4, a.total + (size_t)r * ld, n4 * 4, bar);
+    } else { // compact choice_info of the candidates, gathered from the L2-resident matrix
+        for (int e = threadIdx.x; e < n * Kp; e += blockDim.x) {
+            const int i = e / Kp, j = e - (e / Kp) * Kp;
+            s_chc[e] = j < K ? __ldg(a.total + (size_t)i * ld + a.nn16[e]) : 0.f;
+        }
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_d0[i] = a.dist[(size_t)i * ld];
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) set_status(a.status, ACO_ERR_TIMEOUT);
+        if (!ok) mbar_wait(bar, 0);
+        return;
+    }
+
+    const int slot = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ant = blockIdx.x * apc + slot;
+    if (ant >= a.n_ants) return;
+    uint32_t *vis = s_vis + (size_t)slot * words;
+    for (int w = lane; w < words; w += 32) vis[w] = w == 0 ? 1u : 0u;
+    __syncwarp();
+    int *seedp = a.seeds + (size_t)ant * a.nloc;
+    uint32_t x = pm_norm(seedp[0]);
+    int cur = 0, step = 0, vcnt = 1, load = 0, err = 0;
+    float rdist = 0.f, tdist = 0.f, pend = 0.f;
+    int *tour = a.solutions + (size_t)ant * a.T;
+    if (lane == 0) tour[0] = 0;
+    const unsigned FULL = 0xffffffffu;
+
+    while (vcnt < n) {
+        if (step >= a.T - 3) {
+            err = ACO_ERR_STEP_LIMIT;
+            break;
+        }
+        x = pm_mul(x, 16807u);
+        const float u = pm_uniform(x);
+        const float *drow = a.dist + (size_t)cur * ld;
+        int c = 0;
+        float w = 0.f;
+        if (lane < K) {
+            c = s_nn[(size_t)cur * Kp + lane];
+            bool f = !((vis[c >> 5] >> (c & 31)) & 1u) && (load + s_dem[c] <= a.capacity);
+            if (FIN && f)
+                f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(drow[c], a.serv_time)), s_d0[c]) <= a.max_dist;
+            if (f) w = SMAT ? s_mat[(size_t)cur * n4 + c] : s_chc[(size_t)cur * Kp + lane];
+        }
+        float sc = w; // inclusive Kogge-Stone scan across the warp
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const float o = __shfl_up_sync(FULL, sc, off);
+            if (lane >= off) sc = __fadd_rn(sc, o);
+        }
+        const float tw = __shfl_sync(FULL, sc, 31);
+        int nxt = -1;
+        if (tw > 0.f) {
+            const float r = __fmul_rn(u, tw);
+            const unsigned pos = __ballot_sync(FULL, w > 0.f);
+            const unsigned hit = __ballot_sync(FULL, w > 0.f && sc > r);
+            const int js = hit ? (__ffs(hit) - 1) : (31 - __clz(pos));
+            nxt = __shfl_sync(FULL, c, js);
+        } else { // no listed candidate fits: best feasible customer of the full row
+            uint32_t bk = 0u, bi = 0xffffffffu;
+            const float *trow = SMAT ? s_mat + (size_t)cur * n4 : a.total + (size_t)cur * ld;
+            for (int i = 1 + lane; i < n; i += 32) {
+                bool f = !((vis[i >> 5] >> (i & 31)) & 1u) && (load + s_dem[i] <= a.capacity);
+                if (FIN && f)
+                    f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(drow[i], a.serv_time)), s_d0[i]) <= a.max_dist;
+                if (f) {
+                    const uint32_t k = __float_as_uint(trow[i]) + 1u;
+                    if (k > bk) {
+                        bk = k;
+                        bi = (uint32_t)i;
+                    }
+                }
+            }
+            const uint32_t hk = __reduce_max_sync(FULL, bk);
+            if (hk != 0u) nxt = (int)__reduce_min_sync(FULL, bk == hk ? bi : 0xffffffffu);
+        }
+        step++;
+        if (nxt < 0) {
+            nxt = 0;
+            load = 0;
+            rdist = 0.f;
+        } else {
+            load += s_dem[nxt];
+            if (FIN) rdist = __fadd_rn(rdist, __fadd_rn(drow[nxt], a.serv_time));
+            vcnt++;
+        }
+        if (lane == 0) {
+            vis[nxt >> 5] |= 1u << (nxt & 31);
+            tdist = __fadd_rn(tdist, pend);
+            pend = __ldg(drow + nxt);
+            tour[step] = nxt;
+        }
+        __syncwarp();
+        cur = nxt;
+    }
+    if (err) {
+        if (lane == 0) {
+            tour[a.T - 1] = 0;
+            a.lens[ant] = __int_as_float(0x7f800000);
+            set_status(a.status, err);
+        }
+    } else if (lane == 0) {
+        tdist = __fadd_rn(tdist, pend);
+        tdist = __fadd_rn(tdist, s_d0[cur]);
+        step++;
+        tour[step] = 0;
+        tour[a.T - 1] = step + 1;
+        a.lens[ant] = tdist;
+    }
+    if (step > 0 && lane == 0) seedp[0] = (int)x;
+}
+
+template <int WPA, bool FIN, bool SMAT>
+cudaError_t launch_parity_t(const ConstructArgs &a, int apc, cudaStream_t st)
+{
+    const ParityLayout L = parity_layout(a.n, a.nloc, a.kmax, WPA, apc, SMAT);
+    auto kern = construct_parity_kernel<WPA, FIN, SMAT>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
+    if (e != cudaSuccess) return e;
+    const int blocks = (a.n_ants + apc - 1) / apc;
+    kern<<<blocks, apc * 32 * WPA, L.bytes, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int WPA>
+cudaError_t launch_parity_w(const ConstructArgs &a, int apc, bool smat, cudaStream_t st)
+{
+    const bool fin = !(a.max_dist == __builtin_huge_valf());
+    if (fin) return smat ? launch_parity_t<WPA, true, true>(a, apc, st) : launch_parity_t<WPA, true, false>(a, apc, st);
+    return smat ? launch_parity_t<WPA, false, true>(a, apc, st) : launch_parity_t<WPA, false, false>(a, apc, st);
+}
+
+template <bool FIN, bool SMAT>
+cudaError_t launch_nn_t(const ConstructArgs &a, int apc, cudaStream_t st)
+{
+    const NNLayout L = nn_layout(a.n, a.Kp, apc, SMAT);
+    auto kern = construct_nn_kernel<FIN, SMAT>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
+    if (e != cudaSuccess) return e;
+    const int blocks = (a.n_ants + apc - 1) / apc;
+    kern<<<blocks, apc * 32, L.bytes, st>>>(a);
+    return cudaGetLastError();
+}
+
+} // namespace
+
+size_t construct_parity_smem(int n, int nloc, int kmax, int wpa, int apc, bool stage_total, bool)
+{
+    return parity_layout(n, nloc, kmax, wpa, apc, stage_total).bytes;
+}
+
+size_t construct_nn_smem(int n, int Kp, int apc, bool stage_total)
+{
+    return nn_layout(n, Kp, apc, stage_total).bytes;
+}
+
+cudaError_t launch_construct_parity(const ConstructArgs &a, int wpa, int apc, bool smat, cudaStream_t st)
+{
+    switch (wpa) {
+    case 1: return launch_parity_w<1>(a, apc, smat, st);
+    case 2: return launch_parity_w<2>(a, apc, smat, st);
+    case 4: return launch_parity_w<4>(a, apc, smat, st);
+    case 8: return launch_parity_w<8>(a, apc, smat, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_construct_nn(const ConstructArgs &a, int apc, bool smat, cudaStream_t st)
+{
+    const bool fin = !(a.max_dist == __builtin_huge_valf());
+    if (fin) return smat ? launch_nn_t<true, true>(a, apc, st) : launch_nn_t<true, false>(a, apc, st);
+    return smat ? launch_nn_t<false, true>(a, apc, st) : launch_nn_t<false, false>(a, apc, st);
+}
+
+} // namespace aco

@@ -136,19 +136,21 @@ def gen_batch(seed: int, count: int = 512, n_min: int = 100, n_max: int = 1000) 
 def write_vrplib(inst: Instance, path: str) -> None:
     """Write an instance in the VRPLIB text layout ``read_instance_file`` parses
     (cvrp_ocl/io.cpp:353-512).  Coordinates are printed with 9 significant
-    digits, which round-trips every fp32 value."""
-    lines = [
-        f"NAME : {inst.name}",
-        f"COMMENT : {inst.optimum:.9g}",
-        "TYPE : CVRP",
-        f"DIMENSION : {inst.n}",
-        "EDGE_WEIGHT_TYPE : " + {v: k for k, v in DIST_TYPES.items()}[inst.dist_type],
-        f"CAPACITY : {inst.capacity}",
+    digits, which round-trips every fp32 value.  DISTANCE, SERVICE_TIME and
+    COMMENT must carry an attached colon: the reader scans a float right after
+    the key token (io.cpp:365-372, 459-474)."""
+    lines = [  # "KEY: value" with the colon attached, as the reference's own datasets write it
+        f"NAME: {inst.name}",
+        f"COMMENT: {inst.optimum:.9g}",
+        "TYPE: CVRP",
+        f"DIMENSION: {inst.n}",
+        "EDGE_WEIGHT_TYPE: " + {v: k for k, v in DIST_TYPES.items()}[inst.dist_type],
+        f"CAPACITY: {inst.capacity}",
     ]
     if math.isfinite(inst.max_distance):
-        lines.append(f"DISTANCE : {inst.max_distance:.9g}")
+        lines.append(f"DISTANCE: {inst.max_distance:.9g}")
     if inst.service_time:
-        lines.append(f"SERVICE_TIME : {inst.service_time:.9g}")
+        lines.append(f"SERVICE_TIME: {inst.service_time:.9g}")
     lines.append("NODE_COORD_SECTION")
     for i in range(inst.n):
         lines.append(f"{i + 1} {float(inst.x[i]):.9g} {float(inst.y[i]):.9g}")

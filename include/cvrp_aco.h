@@ -1,0 +1,187 @@
+/*
+ * cvrp_aco.h -- C ABI of the B200 (sm_100a) CVRP ant-colony solver.
+ *
+ * Drop-in boundary for the reference's hot path (i-sunny/cvrp_aco_ocl): the
+ * C++ class g_ACO (cvrp_ocl/gpu/g_aco.h:16-72) over the Problem struct
+ * (cvrp_ocl/problem.h:82-140) and the parameter globals alpha/beta/rho/ras_ranks
+ * (cvrp_ocl/problem.h:30-33).  The reference has no FFI of its own; these entry
+ * points are what a binding of g_ACO would bind.  Every declaration names the
+ * reference routine it replaces.
+ *
+ * Conventions: plain pointers and sizes, no framework types.  Every call returns
+ * an int status: ACO_OK (0) or a negative ACO_ERR_* code; nothing exits or traps.
+ * Tours use the reference's layout: a tour is a sequence of node ids that starts
+ * and ends at the depot 0 and returns to 0 between routes
+ * (cvrp_ocl/problem.h:68-72).  A solver owns its device memory, one CUDA stream
+ * and the CUDA graph of one iteration; it is not re-entrant, but separate
+ * solvers may be driven from separate host threads.
+ */
+#ifndef CVRP_ACO_H
+#define CVRP_ACO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference exit(1)s instead: g_aco.cpp:607-614) ---- */
+#define ACO_OK 0
+#define ACO_ERR_INVALID (-1)        /* bad argument or parameter */
+#define ACO_ERR_INFEASIBLE (-2)     /* a customer can never be served (demand > capacity, or out of max distance) */
+#define ACO_ERR_CUDA (-3)           /* a CUDA runtime call failed */
+#define ACO_ERR_NO_DEVICE (-4)      /* no usable sm_100 device */
+#define ACO_ERR_NOMEM (-5)          /* device or host allocation failed */
+#define ACO_ERR_STATE (-6)          /* call out of order (e.g. iterate before init) */
+#define ACO_ERR_STEP_LIMIT (-7)     /* a construction exceeded 2n-3 steps (would loop forever in the reference) */
+#define ACO_ERR_LS_LIMIT (-8)       /* 2-opt exceeded its improvement-pass budget */
+#define ACO_ERR_RECORD_OVERFLOW (-9)/* more best-so-far records than record_cap (reference: unchecked, kernel.cl:578-583) */
+#define ACO_ERR_CAPACITY (-10)      /* a caller buffer is too small */
+#define ACO_ERR_IO (-11)            /* instance file missing or malformed */
+#define ACO_ERR_TIMEOUT (-12)       /* a bounded device wait gave up */
+
+/* ---- enums -------------------------------------------------------------- */
+enum { ACO_DIST_EUC_2D = 0, ACO_DIST_CEIL_2D = 1, ACO_DIST_GEO = 2, ACO_DIST_ATT = 3 }; /* problem.h:36-38 */
+enum {
+    ACO_MODE_PARITY = 0,     /* full-row I-Roulette with the reference's RNG stream: bit-exact */
+    ACO_MODE_THROUGHPUT = 1  /* nearest-neighbour candidate lists + prefix-sum roulette */
+};
+
+/* Instance: the fields of Problem the path reads (problem.h:82-99).  Either
+ * coordinates (x, y + dist_type) or a precomputed row-major n*n distance
+ * matrix `dist` must be given; when both are, `dist` wins.  Node 0 is the depot. */
+typedef struct aco_instance {
+    int n;                /* num_node, depot included */
+    const float *x;       /* nodeptr[i].x */
+    const float *y;       /* nodeptr[i].y */
+    const int *demand;    /* nodeptr[i].demand */
+    int capacity;         /* vehicle_capacity */
+    float max_distance;   /* max_distance (INFINITY = unlimited, the reader's default io.cpp:348) */
+    float service_time;   /* service_time */
+    int dist_type;        /* ACO_DIST_* */
+    const float *dist;    /* optional precomputed distances */
+} aco_instance;
+
+/* Parameters: set_default_parameters (problem.cpp:186-220) plus the values the
+ * reference hard-codes or takes from the clock. */
+typedef struct aco_params {
+    int n_ants;           /* n_ants (default n, problem.cpp:189) */
+    float alpha;          /* 1.0 (kernel.cl:10, problem.cpp:207) */
+    float beta;           /* 2.0 (kernel.cl:11) */
+    float rho;            /* 0.1 (kernel.cl:9) */
+    int ras_ranks;        /* 6 (kernel.cl:12): the best-so-far ant + ras_ranks-1 iteration elites */
+    int nn_ants;          /* candidate-list length for ACO_MODE_THROUGHPUT (default min(25, n-2)) */
+    int nn_ls;            /* 2-opt neighbour-list depth (default n-2, problem.cpp:191-193) */
+    int ls_flag;          /* 1 = 2-opt after every construction (default 1, problem.cpp:203) */
+    int mode;             /* ACO_MODE_* (default PARITY) */
+    int nloc;             /* work-items per ant of the reference's construct kernel: maxWorkGroupSize/4
+                             (g_aco.cpp:41); sets the RNG lane layout; a power of two in [32, 1024], default 256 */
+    int seed_time;        /* replaces time(NULL) in the seed formula (g_aco.cpp:718) */
+    int rnd_seed;         /* replaces instance->rnd_seed = time(NULL) (problem.cpp:212) */
+    int max_iteration;    /* 250 (problem.cpp:196); used by aco_run */
+    float max_runtime;    /* 600 s (problem.cpp:213); used by aco_run */
+    int ls_pass_limit;    /* 2-opt improvement passes allowed per route before ACO_ERR_LS_LIMIT (default 4096) */
+    int record_cap;       /* best-so-far record capacity (default 4096, g_aco.cpp:727-729) */
+    int device;           /* CUDA device ordinal (default 0) */
+    int use_graph;        /* 1 = replay one CUDA graph per iteration (default 1) */
+    int ants_per_block;   /* 0 = autotuned; else ants per CTA of the construct kernel */
+    int warps_per_ant;    /* 0 = autotuned; else warps per ant of the parity construct kernel (1,2,4,8) */
+} aco_params;
+
+/* One best-so-far record {iteration, length, seconds since init} (problem.h:62-66). */
+typedef struct aco_record {
+    int iter;
+    float length;
+    float time;
+} aco_record;
+
+typedef struct aco_solver aco_solver;
+
+/* ---- parameters and host-side instance tools ----------------------------- */
+/* set_default_parameters (problem.cpp:186-220) for an instance of n nodes. */
+int aco_params_default(aco_params *p, int n);
+
+/* read_instance_file (io.cpp:334-517): parses a VRPLIB file.  Call once with
+ * x == NULL to get n; then again with arrays of n entries. */
+int aco_read_vrplib(const char *path, int *n, float *x, float *y, int *demand, int *capacity,
+                    float *max_distance, float *service_time, int *dist_type, float *optimum,
+                    char *name, int name_cap);
+
+/* compute_distances (vrpHelper.cpp:160-184): row-major n*n fp32. */
+int aco_compute_distances(int n, const float *x, const float *y, int dist_type, float *dist);
+
+/* compute_nn_lists (vrpHelper.cpp:188-236, sort2 tie order utilities.cpp:246-266):
+ * depth = min(max(nn_ls, nn_ants), n-1) entries per node, written to nn (n*depth). */
+int aco_compute_nn_lists(int n, const float *dist, int nn_ls, int nn_ants, int *nn, int *depth);
+
+/* check_solution (problem.cpp:226-319): 1 valid, 0 invalid, <0 error. */
+int aco_check_solution(const aco_instance *inst, const int *tour, int tour_size);
+
+/* compute_tour_length (vrpHelper.cpp:244-253) in fp32, and the same sum in fp64. */
+int aco_tour_length(int n, const float *dist, const int *tour, int tour_size, float *len32, double *len64);
+
+/* The per-work-item seeds of create_memory_objects (g_aco.cpp:714-722), with
+ * time(NULL) = seed_time; *rnd_seed is advanced as the reference advances it. */
+int aco_make_seeds(int seed_time, int *rnd_seed, int n_ants, int nloc, int *seeds);
+
+/* ---- solver lifecycle: g_ACO (g_aco.h:16-37) ------------------------------ */
+/* g_ACO::g_ACO + create_memory_objects (g_aco.cpp:35-43, 640-761): copies the
+ * instance to the device, computes distances / NN lists / seeds. */
+int aco_create(const aco_instance *inst, const aco_params *params, aco_solver **out);
+/* g_ACO::init_aco (g_aco.cpp:63-93): bootstrap construct, trail_0 = 1/(rho*L). */
+int aco_init(aco_solver *s);
+/* n_iter x (g_ACO::run_aco_iteration (g_aco.cpp:122-134) + iteration++ (main.cpp:86)). */
+int aco_iterate(aco_solver *s, int n_iter);
+/* main.cpp:84-88: iterate until max_iteration / max_runtime / optimum (within 10*EPSILON). */
+int aco_run(aco_solver *s, float optimum, int *iterations_done);
+/* g_ACO::exit_aco + destructor (g_aco.cpp:45-61, 95-117). */
+void aco_destroy(aco_solver *s);
+
+/* ---- the individual phases (public methods of g_ACO) -------------------- */
+int aco_construct_solutions(aco_solver *s); /* g_aco.cpp:141-177 */
+int aco_local_search(aco_solver *s);        /* g_aco.cpp:182-228 */
+int aco_update_statistics(aco_solver *s);   /* g_aco.cpp:407-417 (+ iteration++ of the caller) */
+int aco_pheromone_update(aco_solver *s);    /* g_aco.cpp:233-243 */
+int aco_pheromone_init(aco_solver *s, float trail_0); /* g_aco.cpp:245-263 */
+
+/* ---- results and test taps ----------------------------------------------- */
+/* update_best_so_far_from_device (g_aco.cpp:527-552). */
+int aco_get_best(aco_solver *s, int *tour, int cap, int *tour_size, float *length);
+/* the bsf record stream read by exit_aco (g_aco.cpp:100-113). */
+int aco_get_bsf_records(aco_solver *s, aco_record *out, int cap, int *count);
+/* solutions_mem / solution_lens_mem in the reference layout (g_aco.cpp:652-665):
+ * solutions has 2n*(n_ants+1)+1 ints, lens n_ants+1 floats. */
+int aco_get_solutions(aco_solver *s, int *solutions, size_t cap_ints, float *lens, size_t cap_lens);
+/* pheromone_mem / total_info_mem as dense row-major n*n. */
+int aco_get_pheromone(aco_solver *s, float *tau, float *total_info, size_t cap);
+/* seed_mem: n_ants*nloc ints. */
+int aco_get_seeds(aco_solver *s, int *seeds, size_t cap);
+/* elite_ids_mem: ras_ranks ints. */
+int aco_get_elites(aco_solver *s, int *elites, int cap);
+/* the current iteration counter (Problem::iteration). */
+int aco_get_iteration(aco_solver *s, int *iteration);
+/* overwrite state for phase-level tests: pheromone + total_info (dense n*n),
+ * solutions + lens (reference layout), seeds.  NULL pointers are skipped. */
+int aco_set_state(aco_solver *s, const float *tau, const float *total_info, const int *solutions,
+                  const float *lens, const int *seeds);
+/* sticky device status of the last launches (ACO_OK or an ACO_ERR_* code). */
+int aco_status(aco_solver *s);
+const char *aco_strerror(int code);
+
+/* ---- timing and interop --------------------------------------------------- */
+/* the solver's CUDA stream (a cudaStream_t), for event timing by the caller. */
+void *aco_get_stream(aco_solver *s);
+/* number of kernel launches one iteration makes (graph nodes when graphs are on). */
+int aco_launches_per_iteration(aco_solver *s);
+/* device-timed run of n_iter iterations on the solver's stream (CUDA events). */
+int aco_time_iterations(aco_solver *s, int n_iter, float *ms);
+/* the kernel configuration the solver picked: ants per CTA and warps per ant of
+ * construct, and whether matrices are staged in shared memory (bit 0: total_info
+ * in construct, bit 1: NN lists in 2-opt). */
+int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *staging_flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CVRP_ACO_H */

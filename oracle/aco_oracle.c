@@ -90,7 +90,7 @@ static int dist_ceil(const float *x, const float *y, int i, int j)
     float xd = x[i] - x[j];
     float yd = y[i] - y[j];
     float r = sqrtf(xd * xd + yd * yd);
-    return (int)(ceil(r));
+    return (int)(ceilf(r));
 }
 
 static int dist_geo(const float *x, const float *y, int i, int j)
@@ -102,9 +102,9 @@ static int dist_geo(const float *x, const float *y, int i, int j)
     deg = dtrunc_(x2); min = x2 - deg; latj = PI * (deg + 5.0 * min / 3.0) / 180.0;
     deg = dtrunc_(y1); min = y1 - deg; longi = PI * (deg + 5.0 * min / 3.0) / 180.0;
     deg = dtrunc_(y2); min = y2 - deg; longj = PI * (deg + 5.0 * min / 3.0) / 180.0;
-    q1 = cos(longi - longj);
-    q2 = cos(lati - latj);
-    q3 = cos(lati + latj);
+    q1 = cosf(longi - longj); /* float argument: the C++ float overload */
+    q2 = cosf(lati - latj);
+    q3 = cosf(lati + latj);
     return (int)(6378.388 * acos(0.5 * ((1.0 + q1) * q2 - (1.0 - q1) * q3)) + 1.0);
 }
 
