@@ -307,6 +307,14 @@ class Solver:
         check(lib().aco_time_iterations(self.h, n_iter, ctypes.byref(ms)), "aco_time_iterations")
         return ms.value
 
+    def enqueue(self, n_iter: int = 1):
+        check(lib().aco_enqueue_iterations(self.h, n_iter), "aco_enqueue_iterations")
+
+    def time_phases(self, n_iter: int) -> np.ndarray:
+        ms = np.zeros(4, np.float32)
+        check(lib().aco_time_phases(self.h, n_iter, ptr(ms)), "aco_time_phases")
+        return ms
+
     def config(self) -> Tuple[int, int, int]:
         a, w, f = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(lib().aco_get_config(self.h, ctypes.byref(a), ctypes.byref(w), ctypes.byref(f)), "aco_get_config")

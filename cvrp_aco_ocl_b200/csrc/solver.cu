@@ -798,6 +798,53 @@ int aco_time_iterations(aco_solver *s, int n_iter, float *ms)
     return sync_status(s);
 }
 
+int aco_enqueue_iterations(aco_solver *s, int n_iter)
+{
+    if (!s || n_iter < 0) return ACO_ERR_INVALID;
+    if (!s->initialized) return ACO_ERR_STATE;
+    int rc = set_device(s);
+    if (rc != ACO_OK) return rc;
+    if (s->p.use_graph) {
+        rc = ensure_graph(s);
+        if (rc != ACO_OK) return rc;
+        for (int i = 0; i < n_iter; i++) CK(cudaGraphLaunch(s->exec, s->st));
+        return ACO_OK;
+    }
+    for (int i = 0; i < n_iter && rc == ACO_OK; i++) rc = run_iteration_phases(s);
+    return rc;
+}
+
+int aco_time_phases(aco_solver *s, int n_iter, float *ms4)
+{
+    if (!s || !ms4 || n_iter <= 0) return ACO_ERR_INVALID;
+    if (!s->initialized) return ACO_ERR_STATE;
+    int rc = set_device(s);
+    if (rc != ACO_OK) return rc;
+    cudaEvent_t ev[5];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    for (int k = 0; k < 4; k++) ms4[k] = 0.f;
+    for (int it = 0; it < n_iter && rc == ACO_OK; it++) {
+        CK(cudaEventRecord(ev[0], s->st));
+        rc = do_construct(s);
+        CK(cudaEventRecord(ev[1], s->st));
+        if (rc == ACO_OK && s->p.ls_flag) rc = do_local_search(s);
+        CK(cudaEventRecord(ev[2], s->st));
+        if (rc == ACO_OK) rc = do_stats(s, true);
+        CK(cudaEventRecord(ev[3], s->st));
+        if (rc == ACO_OK) rc = do_update(s);
+        CK(cudaEventRecord(ev[4], s->st));
+        CK(cudaEventSynchronize(ev[4]));
+        for (int k = 0; k < 4; k++) {
+            float m = 0.f;
+            CK(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));
+            ms4[k] += m;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (rc != ACO_OK) return rc;
+    return sync_status(s);
+}
+
 int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *staging_flags)
 {
     if (!s) return ACO_ERR_INVALID;

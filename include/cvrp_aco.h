@@ -176,6 +176,13 @@ void *aco_get_stream(aco_solver *s);
 int aco_launches_per_iteration(aco_solver *s);
 /* device-timed run of n_iter iterations on the solver's stream (CUDA events). */
 int aco_time_iterations(aco_solver *s, int n_iter, float *ms);
+/* enqueue n_iter iterations on the solver's stream and return without waiting
+ * (aco_status waits and reports); lets a caller bracket them with its own events. */
+int aco_enqueue_iterations(aco_solver *s, int n_iter);
+/* n_iter iterations launched phase by phase with CUDA events between the
+ * phases: ms[0] construct, ms[1] 2-opt, ms[2] statistics, ms[3] pheromone pass
+ * (device milliseconds summed over the iterations). */
+int aco_time_phases(aco_solver *s, int n_iter, float *ms4);
 /* the kernel configuration the solver picked: ants per CTA and warps per ant of
  * construct, and whether matrices are staged in shared memory (bit 0: total_info
  * in construct, bit 1: NN lists in 2-opt). */
