@@ -31,6 +31,7 @@ EXPORTED = [
     "aco_get_solutions", "aco_get_pheromone", "aco_get_seeds", "aco_get_elites", "aco_get_iteration",
     "aco_set_state", "aco_status", "aco_strerror", "aco_get_stream", "aco_launches_per_iteration",
     "aco_time_iterations", "aco_enqueue_iterations", "aco_time_phases", "aco_get_config",
+    "aco_pheromone_update_noalloc",
 ]
 
 
@@ -107,6 +108,7 @@ def lib() -> ctypes.CDLL:
         L.aco_time_iterations.argtypes = [vp, ip, ctypes.POINTER(fp)]
         L.aco_enqueue_iterations.argtypes = [vp, ip]
         L.aco_time_phases.argtypes = [vp, ip, vp]
+        L.aco_pheromone_update_noalloc.argtypes = [ip, ip, ip, ip, fp, fp, fp, vp, vp, vp, vp, vp, vp, vp]
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
         _lib = L
     return _lib

@@ -188,6 +188,27 @@ int aco_time_phases(aco_solver *s, int n_iter, float *ms4);
  * in construct, bit 1: NN lists in 2-opt). */
 int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *staging_flags);
 
+/* ---- pheromone update without allocation ---------------------------------
+ * No counterpart in the reference.  For callers that cannot let this library
+ * allocate device memory: hosts whose memory manager owns all device memory,
+ * and loops that cannot take the device-wide synchronisation of cudaMalloc /
+ * cudaFree.  Runs the update of aco_update_statistics' elite selection +
+ * aco_pheromone_update on the caller's device buffers, enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream):
+ *   tau, total_info : n rows of ld floats (ld >= n), tau updated in place;
+ *   dist            : n rows of ld floats, distances;
+ *   solutions, lens : the reference layout (2n*(n_ants+1)+1 ints, n_ants+1
+ *                     floats) after the statistics step (best-so-far in slot n_ants);
+ *   elites_out      : ras_ranks ints, or NULL.
+ * Scratch is a fixed 148 KB array inside the library (kept by every GPU that
+ * loads it until exit): n <= 4096 and ras_ranks <= 8, else ACO_ERR_CAPACITY.
+ * The first call on a device looks up that array's device address; make it
+ * before any stream capture.  Calls share the array, so calls that overlap on
+ * the GPU race.  Allocates nothing, frees nothing. */
+int aco_pheromone_update_noalloc(int n, int ld, int n_ants, int ras_ranks, float rho, float alpha, float beta,
+                                 float *tau, float *total_info, const float *dist, const int *solutions,
+                                 const float *lens, int *elites_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
