@@ -119,12 +119,16 @@ void pick_config(aco_solver *s)
     s->cp_stage = construct_parity_smem(n, s->nloc, s->kmax, wpa, s->cp_apc, true, fin) <= kSmemBudget;
     s->cn_apc = s->p.ants_per_block > 0 ? s->p.ants_per_block : per_block(s->sm_count);
     s->cn_stage = s->K > 0 && construct_nn_smem(n, s->Kp, s->cn_apc, true) <= kSmemBudget;
-    s->ls_apc = per_block(s->sm_count);
-    s->ls_rmax = 64;
-    s->ls_snn = local_search_smem(n, s->nn_ls, s->ls_rmax, s->ls_apc, true) <= kSmemBudget;
-    while (local_search_smem(n, s->nn_ls, s->ls_rmax, s->ls_apc, s->ls_snn) > kSmemBudget) {
-        if (s->ls_rmax > 16) s->ls_rmax /= 2;
-        else if (s->ls_apc > 1) s->ls_apc--;
+    // 2-opt: one CTA per ant, one warp per route (routes estimated from the demand)
+    long long dem = 0;
+    for (int i = 1; i < n; i++) dem += s->demand_h[i];
+    const int est_routes = s->capacity > 0 ? (int)std::min<long long>(n, dem / s->capacity + 1) : 1;
+    s->ls_apc = std::max(1, std::min(16, est_routes));
+    s->ls_rmax = 32;
+    s->ls_snn = false;
+    while (local_search_smem(n, s->nn_ls, s->ls_rmax, s->ls_apc, false) > kSmemBudget) {
+        if (s->ls_apc > 1) s->ls_apc--;
+        else if (s->ls_rmax > 8) s->ls_rmax /= 2;
         else break;
     }
 }
