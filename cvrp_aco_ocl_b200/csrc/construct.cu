@@ -217,13 +217,19 @@ __global__ void __launch_bounds__(512) construct_parity_kernel(ConstructArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// Throughput mode.
+// Throughput mode.  Per CTA: demand and the candidate lists by TMA bulk copy;
+// the total_info matrix too when it fits (SMAT).  Each candidate entry is
+// packed as (node | demand << 16) next to its choice_info value (PACKED), so a
+// step issues one pair of independent shared loads for its 32 lanes, one
+// dependent load of the visited word, the 5-step scan and the selection.  The
+// tour goes to a shared buffer and its length is summed after the last step,
+// in step order (no global load inside the step loop).
 // ---------------------------------------------------------------------------
 struct NNLayout {
-    size_t bar, dem, d0, nn, chc, vis, mat, bytes;
+    size_t bar, dem, d0, nn16, cand, chc, vis, tour, mat, bytes;
 };
 
-__host__ __device__ inline NNLayout nn_layout(int n, int Kp, int apc, bool smat)
+__host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, bool smat, bool packed)
 {
     const size_t n4 = (size_t)((n + 3) & ~3);
     const size_t words = (size_t)((n + 31) / 32);
@@ -232,32 +238,36 @@ __host__ __device__ inline NNLayout nn_layout(int n, int Kp, int apc, bool smat)
     L.bar = o; o = al128(o + 16);
     L.dem = o; o = al128(o + n4 * 4);
     L.d0 = o; o = al128(o + n4 * 4);
-    L.nn = o; o = al128(o + (size_t)n * Kp * 2);
-    L.chc = o;
-    if (!smat) o = al128(o + (size_t)n * Kp * 4);
+    L.nn16 = o; o = al128(o + (size_t)n * Kp * 2);    // TMA destination (the global layout)
+    L.cand = o; if (packed) o = al128(o + (size_t)n * K * 4);
+    L.chc = o; o = al128(o + (size_t)n * K * 4);
     L.vis = o; o = al128(o + (size_t)apc * words * 4);
+    L.tour = o; o = al128(o + (size_t)apc * 2 * n * 2);
     L.mat = o;
     if (smat) o = al128(o + (size_t)n * n4 * 4);
     L.bytes = o;
     return L;
 }
 
-template <bool FIN, bool SMAT>
+template <bool FIN, bool SMAT, bool PACKED>
 __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp;
+    const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp, T = a.T;
     const int n4 = (n + 3) & ~3;
     const int apc = blockDim.x >> 5;
-    const NNLayout L = nn_layout(n, Kp, apc, SMAT);
+    const NNLayout L = nn_layout(n, K, Kp, apc, SMAT, PACKED);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar);
     int *s_dem = reinterpret_cast<int *>(smem + L.dem);
     float *s_d0 = reinterpret_cast<float *>(smem + L.d0);
-    uint16_t *s_nn = reinterpret_cast<uint16_t *>(smem + L.nn);
+    uint16_t *s_nn16 = reinterpret_cast<uint16_t *>(smem + L.nn16);
+    uint32_t *s_cand = reinterpret_cast<uint32_t *>(smem + L.cand);
     float *s_chc = reinterpret_cast<float *>(smem + L.chc);
     uint32_t *s_vis = reinterpret_cast<uint32_t *>(smem + L.vis);
+    uint16_t *s_tour = reinterpret_cast<uint16_t *>(smem + L.tour);
     float *s_mat = reinterpret_cast<float *>(smem + L.mat);
     const int words = (n + 31) >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
@@ -269,55 +279,68 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
         if (SMAT) bytes += (uint32_t)(n * n4 * 4);
         mbar_arrive_expect_tx(bar, bytes);
         tma_bulk_g2s(s_dem, a.demand, n4 * 4, bar);
-        tma_bulk_g2s(s_nn, a.nn16, n * Kp * 2, bar);
+        tma_bulk_g2s(s_nn16, a.nn16, n * Kp * 2, bar);
     }
-    if (SMAT) {
+    if (SMAT)
         for (int r = threadIdx.x; r < n; r += blockDim.x)
             tma_bulk_g2s(s_mat + (size_t)r * n4, a.total + (size_t)r * ld, n4 * 4, bar);
-    } else { // compact choice_info of the candidates, gathered from the L2-resident matrix
-        for (int e = threadIdx.x; e < n * Kp; e += blockDim.x) {
-            const int i = e / Kp, j = e - (e / Kp) * Kp;
-            s_chc[e] = j < K ? __ldg(a.total + (size_t)i * ld + a.nn16[e]) : 0.f;
-        }
-    }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s_d0[i] = a.dist[(size_t)i * ld];
+    if (FIN)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) s_d0[i] = a.dist[(size_t)i * ld];
     const bool ok = mbar_wait(bar, 0);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) set_status(a.status, ACO_ERR_TIMEOUT);
         if (!ok) mbar_wait(bar, 0);
         return;
     }
+    // candidate table: row i, entry j = j-th nearest neighbour of i
+    for (int i = warp; i < n; i += apc) {
+        if (lane < K) {
+            const int c = s_nn16[i * Kp + lane];
+            if (PACKED) s_cand[i * K + lane] = (uint32_t)c | ((uint32_t)s_dem[c] << 16);
+            s_chc[i * K + lane] = SMAT ? s_mat[i * n4 + c] : __ldg(a.total + (size_t)i * ld + c);
+        }
+    }
+    __syncthreads();
 
-    const int slot = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ant = blockIdx.x * apc + slot;
+    const int ant = blockIdx.x * apc + warp;
     if (ant >= a.n_ants) return;
-    uint32_t *vis = s_vis + (size_t)slot * words;
+    uint32_t *vis = s_vis + warp * words;
+    uint16_t *tbuf = s_tour + warp * 2 * n;
     for (int w = lane; w < words; w += 32) vis[w] = w == 0 ? 1u : 0u;
+    if (lane == 0) tbuf[0] = 0;
     __syncwarp();
     int *seedp = a.seeds + (size_t)ant * a.nloc;
     uint32_t x = pm_norm(seedp[0]);
     int cur = 0, step = 0, vcnt = 1, load = 0, err = 0;
-    float rdist = 0.f, tdist = 0.f, pend = 0.f;
-    int *tour = a.solutions + (size_t)ant * a.T;
-    if (lane == 0) tour[0] = 0;
+    float rdist = 0.f;
     const unsigned FULL = 0xffffffffu;
+    const int cap = a.capacity;
 
     while (vcnt < n) {
-        if (step >= a.T - 3) {
+        if (step >= T - 3) {
             err = ACO_ERR_STEP_LIMIT;
             break;
         }
         x = pm_mul(x, 16807u);
         const float u = pm_uniform(x);
-        const float *drow = a.dist + (size_t)cur * ld;
-        int c = 0;
+        int c = 0, dc = 0;
         float w = 0.f;
         if (lane < K) {
-            c = s_nn[(size_t)cur * Kp + lane];
-            bool f = !((vis[c >> 5] >> (c & 31)) & 1u) && (load + s_dem[c] <= a.capacity);
+            const int e = cur * K + lane;
+            const float wv = s_chc[e];
+            if (PACKED) {
+                const uint32_t pk = s_cand[e];
+                c = (int)(pk & 0xFFFFu);
+                dc = (int)(pk >> 16);
+            } else {
+                c = s_nn16[cur * Kp + lane];
+                dc = s_dem[c];
+            }
+            bool f = !((vis[c >> 5] >> (c & 31)) & 1u) && (load + dc <= cap);
             if (FIN && f)
-                f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(drow[c], a.serv_time)), s_d0[c]) <= a.max_dist;
-            if (f) w = SMAT ? s_mat[(size_t)cur * n4 + c] : s_chc[(size_t)cur * Kp + lane];
+                f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + c), a.serv_time)),
+                              s_d0[c]) <= a.max_dist;
+            w = f ? wv : 0.f;
         }
         float sc = w; // inclusive Kogge-Stone scan across the warp
 #pragma unroll
@@ -326,30 +349,39 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
             if (lane >= off) sc = __fadd_rn(sc, o);
         }
         const float tw = __shfl_sync(FULL, sc, 31);
-        int nxt = -1;
+        int nxt = -1, nd = 0;
         if (tw > 0.f) {
             const float r = __fmul_rn(u, tw);
             const unsigned pos = __ballot_sync(FULL, w > 0.f);
             const unsigned hit = __ballot_sync(FULL, w > 0.f && sc > r);
             const int js = hit ? (__ffs(hit) - 1) : (31 - __clz(pos));
             nxt = __shfl_sync(FULL, c, js);
+            nd = __shfl_sync(FULL, dc, js);
         } else { // no listed candidate fits: best feasible customer of the full row
             uint32_t bk = 0u, bi = 0xffffffffu;
-            const float *trow = SMAT ? s_mat + (size_t)cur * n4 : a.total + (size_t)cur * ld;
-            for (int i = 1 + lane; i < n; i += 32) {
-                bool f = !((vis[i >> 5] >> (i & 31)) & 1u) && (load + s_dem[i] <= a.capacity);
-                if (FIN && f)
-                    f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(drow[i], a.serv_time)), s_d0[i]) <= a.max_dist;
-                if (f) {
-                    const uint32_t k = __float_as_uint(trow[i]) + 1u;
-                    if (k > bk) {
-                        bk = k;
-                        bi = (uint32_t)i;
+            for (int k = 0; k < words; k++) {
+                const int i = lane + 32 * k;
+                const uint32_t vw = vis[k];
+                if (i > 0 && i < n && !((vw >> lane) & 1u) && load + s_dem[i] <= cap) {
+                    bool f = true;
+                    if (FIN)
+                        f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + i), a.serv_time)),
+                                      s_d0[i]) <= a.max_dist;
+                    if (f) {
+                        const float v = SMAT ? s_mat[cur * n4 + i] : __ldg(a.total + (size_t)cur * ld + i);
+                        const uint32_t kk = __float_as_uint(v) + 1u;
+                        if (kk > bk) {
+                            bk = kk;
+                            bi = (uint32_t)i;
+                        }
                     }
                 }
             }
             const uint32_t hk = __reduce_max_sync(FULL, bk);
-            if (hk != 0u) nxt = (int)__reduce_min_sync(FULL, bk == hk ? bi : 0xffffffffu);
+            if (hk != 0u) {
+                nxt = (int)__reduce_min_sync(FULL, bk == hk ? bi : 0xffffffffu);
+                nd = s_dem[nxt];
+            }
         }
         step++;
         if (nxt < 0) {
@@ -357,32 +389,42 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
             load = 0;
             rdist = 0.f;
         } else {
-            load += s_dem[nxt];
-            if (FIN) rdist = __fadd_rn(rdist, __fadd_rn(drow[nxt], a.serv_time));
+            load += nd;
+            if (FIN) rdist = __fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + nxt), a.serv_time));
             vcnt++;
         }
         if (lane == 0) {
             vis[nxt >> 5] |= 1u << (nxt & 31);
-            tdist = __fadd_rn(tdist, pend);
-            pend = __ldg(drow + nxt);
-            tour[step] = nxt;
+            tbuf[step] = (uint16_t)nxt;
         }
         __syncwarp();
         cur = nxt;
     }
+    int *tour = a.solutions + (size_t)ant * T;
     if (err) {
         if (lane == 0) {
-            tour[a.T - 1] = 0;
+            tour[T - 1] = 0;
             a.lens[ant] = __int_as_float(0x7f800000);
             set_status(a.status, err);
         }
-    } else if (lane == 0) {
-        tdist = __fadd_rn(tdist, pend);
-        tdist = __fadd_rn(tdist, s_d0[cur]);
+    } else {
         step++;
-        tour[step] = 0;
-        tour[a.T - 1] = step + 1;
-        a.lens[ant] = tdist;
+        if (lane == 0) tbuf[step] = 0;
+        __syncwarp();
+        const int size = step + 1;
+        for (int p = lane; p < size; p += 32) tour[p] = tbuf[p];
+        // tour length: the fp32 sum of the edges in step order (kernel.cl:475,483)
+        float tdist = 0.f;
+        for (int base = 0; base < size - 1; base += 32) {
+            const int p = base + lane;
+            const float e = p < size - 1 ? __ldg(a.dist + (size_t)tbuf[p] * ld + tbuf[p + 1]) : 0.f;
+            const int m = size - 1 - base < 32 ? size - 1 - base : 32;
+            for (int k = 0; k < m; k++) tdist = __fadd_rn(tdist, __shfl_sync(FULL, e, k));
+        }
+        if (lane == 0) {
+            tour[T - 1] = size;
+            a.lens[ant] = tdist;
+        }
     }
     if (step > 0 && lane == 0) seedp[0] = (int)x;
 }
@@ -407,16 +449,23 @@ cudaError_t launch_parity_w(const ConstructArgs &a, int apc, bool smat, cudaStre
     return smat ? launch_parity_t<WPA, false, true>(a, apc, st) : launch_parity_t<WPA, false, false>(a, apc, st);
 }
 
-template <bool FIN, bool SMAT>
+template <bool FIN, bool SMAT, bool PACKED>
 cudaError_t launch_nn_t(const ConstructArgs &a, int apc, cudaStream_t st)
 {
-    const NNLayout L = nn_layout(a.n, a.Kp, apc, SMAT);
-    auto kern = construct_nn_kernel<FIN, SMAT>;
+    const NNLayout L = nn_layout(a.n, a.K, a.Kp, apc, SMAT, PACKED);
+    auto kern = construct_nn_kernel<FIN, SMAT, PACKED>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
     if (e != cudaSuccess) return e;
     const int blocks = (a.n_ants + apc - 1) / apc;
     kern<<<blocks, apc * 32, L.bytes, st>>>(a);
     return cudaGetLastError();
+}
+
+template <bool FIN>
+cudaError_t launch_nn_f(const ConstructArgs &a, int apc, bool smat, bool packed, cudaStream_t st)
+{
+    if (smat) return packed ? launch_nn_t<FIN, true, true>(a, apc, st) : launch_nn_t<FIN, true, false>(a, apc, st);
+    return packed ? launch_nn_t<FIN, false, true>(a, apc, st) : launch_nn_t<FIN, false, false>(a, apc, st);
 }
 
 } // namespace
@@ -426,9 +475,9 @@ size_t construct_parity_smem(int n, int nloc, int kmax, int wpa, int apc, bool s
     return parity_layout(n, nloc, kmax, wpa, apc, stage_total).bytes;
 }
 
-size_t construct_nn_smem(int n, int Kp, int apc, bool stage_total)
+size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool packed)
 {
-    return nn_layout(n, Kp, apc, stage_total).bytes;
+    return nn_layout(n, K, Kp, apc, stage_total, packed).bytes;
 }
 
 cudaError_t launch_construct_parity(const ConstructArgs &a, int wpa, int apc, bool smat, cudaStream_t st)
@@ -442,11 +491,10 @@ cudaError_t launch_construct_parity(const ConstructArgs &a, int wpa, int apc, bo
     }
 }
 
-cudaError_t launch_construct_nn(const ConstructArgs &a, int apc, bool smat, cudaStream_t st)
+cudaError_t launch_construct_nn(const ConstructArgs &a, int apc, bool smat, bool packed, cudaStream_t st)
 {
     const bool fin = !(a.max_dist == __builtin_huge_valf());
-    if (fin) return smat ? launch_nn_t<true, true>(a, apc, st) : launch_nn_t<true, false>(a, apc, st);
-    return smat ? launch_nn_t<false, true>(a, apc, st) : launch_nn_t<false, false>(a, apc, st);
+    return fin ? launch_nn_f<true>(a, apc, smat, packed, st) : launch_nn_f<false>(a, apc, smat, packed, st);
 }
 
 } // namespace aco

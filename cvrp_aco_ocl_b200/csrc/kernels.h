@@ -92,7 +92,8 @@ cudaError_t launch_heur(const float *dist, float *heur, int n, int ld, float bet
 cudaError_t launch_pheromone_init(const InitArgs &a, cudaStream_t st);
 cudaError_t launch_construct_parity(const ConstructArgs &a, int warps_per_ant, int ants_per_block, bool stage_total,
                                     cudaStream_t st);
-cudaError_t launch_construct_nn(const ConstructArgs &a, int ants_per_block, bool stage_total, cudaStream_t st);
+cudaError_t launch_construct_nn(const ConstructArgs &a, int ants_per_block, bool stage_total, bool packed,
+                                cudaStream_t st);
 cudaError_t launch_local_search(const LocalSearchArgs &a, int ants_per_block, bool stage_nn, cudaStream_t st);
 cudaError_t launch_stats(const StatsArgs &a, cudaStream_t st);
 cudaError_t launch_pheromone_update(const UpdateArgs &a, int sm_count, cudaStream_t st);
@@ -102,7 +103,7 @@ cudaError_t launch_t0(unsigned long long *t0, cudaStream_t st);
 // that fit the 227 KB per-CTA limit).
 size_t construct_parity_smem(int n, int nloc, int kmax, int warps_per_ant, int ants_per_block, bool stage_total,
                              bool finite_maxd);
-size_t construct_nn_smem(int n, int Kp, int ants_per_block, bool stage_total);
+size_t construct_nn_smem(int n, int K, int Kp, int ants_per_block, bool stage_total, bool packed);
 size_t local_search_smem(int n, int nn_ls, int rmax, int ants_per_block, bool stage_nn);
 
 } // namespace aco

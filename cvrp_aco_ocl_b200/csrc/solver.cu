@@ -47,7 +47,7 @@ struct aco_solver {
     unsigned long long *d_t0 = nullptr;
     int *h_pin = nullptr; // [0] status, [1] iteration, [2..3] bsf length bits
     int cp_wpa = 1, cp_apc = 1, cn_apc = 1, ls_apc = 1, ls_rmax = 64;
-    bool cp_stage = false, cn_stage = false, ls_snn = false;
+    bool cp_stage = false, cn_stage = false, cn_packed = false, ls_snn = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool initialized = false;
@@ -118,7 +118,29 @@ void pick_config(aco_solver *s)
     const bool fin = !std::isinf(s->max_dist);
     s->cp_stage = construct_parity_smem(n, s->nloc, s->kmax, wpa, s->cp_apc, true, fin) <= kSmemBudget;
     s->cn_apc = s->p.ants_per_block > 0 ? s->p.ants_per_block : per_block(s->sm_count);
-    s->cn_stage = s->K > 0 && construct_nn_smem(n, s->Kp, s->cn_apc, true) <= kSmemBudget;
+    // throughput construct: pack (node | demand << 16) when demands fit 16 bits,
+    // stage the full matrix when it fits next to the candidate tables
+    int maxdem = 0, mindem = 0;
+    for (int i = 0; i < n; i++) {
+        maxdem = std::max(maxdem, s->demand_h[i]);
+        mindem = std::min(mindem, s->demand_h[i]);
+    }
+    const bool packable = maxdem <= 0xFFFF && mindem >= 0;
+    s->cn_packed = false;
+    s->cn_stage = false;
+    if (s->K > 0) {
+        for (int apc = s->cn_apc; apc >= 1 && !s->cn_stage; apc--) {
+            if (packable && construct_nn_smem(n, s->K, s->Kp, apc, true, true) <= kSmemBudget) {
+                s->cn_stage = s->cn_packed = true;
+                s->cn_apc = apc;
+            }
+        }
+        if (!s->cn_stage) {
+            s->cn_packed = packable && construct_nn_smem(n, s->K, s->Kp, s->cn_apc, false, true) <= kSmemBudget;
+            while (s->cn_apc > 1 && construct_nn_smem(n, s->K, s->Kp, s->cn_apc, false, s->cn_packed) > kSmemBudget)
+                s->cn_apc--;
+        }
+    }
     // 2-opt: one CTA per ant, one warp per route (routes estimated from the demand)
     long long dem = 0;
     for (int i = 1; i < n; i++) dem += s->demand_h[i];
@@ -147,7 +169,7 @@ ConstructArgs cargs(aco_solver *s)
 int do_construct(aco_solver *s)
 {
     const ConstructArgs a = cargs(s);
-    if (s->p.mode == ACO_MODE_THROUGHPUT) CK(launch_construct_nn(a, s->cn_apc, s->cn_stage, s->st));
+    if (s->p.mode == ACO_MODE_THROUGHPUT) CK(launch_construct_nn(a, s->cn_apc, s->cn_stage, s->cn_packed, s->st));
     else CK(launch_construct_parity(a, s->cp_wpa, s->cp_apc, s->cp_stage, s->st));
     return ACO_OK;
 }
