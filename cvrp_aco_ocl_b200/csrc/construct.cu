@@ -419,7 +419,11 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
             const int p = base + lane;
             const float e = p < size - 1 ? __ldg(a.dist + (size_t)tbuf[p] * ld + tbuf[p + 1]) : 0.f;
             const int m = size - 1 - base < 32 ? size - 1 - base : 32;
-            for (int k = 0; k < m; k++) tdist = __fadd_rn(tdist, __shfl_sync(FULL, e, k));
+#pragma unroll
+            for (int k = 0; k < 32; k++) {
+                const float y = __shfl_sync(FULL, e, k);
+                if (k < m) tdist = __fadd_rn(tdist, y);
+            }
         }
         if (lane == 0) {
             tour[T - 1] = size;

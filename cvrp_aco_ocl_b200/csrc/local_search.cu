@@ -10,19 +10,23 @@
 // after a pass without a move, and in that pass the depot -- always at the
 // route's first position -- is either skipped with its bit set or examined
 // without a move, which sets it (kernel.cl:232).  So route r starts with the
-// depot bit = (r > 0), and the routes of a tour can run concurrently, each on
-// one warp, with results identical to the sequential order.  (When a route stops
-// at the pass budget the bit may still be clear; that error path reports
-// ACO_ERR_LS_LIMIT and its tours are valid but not matched bit for bit.)
+// depot bit = (r > 0), and the routes of a tour can run concurrently with
+// results identical to the sequential order.  (When a route stops at the pass
+// budget the bit may still be clear; that error path reports ACO_ERR_LS_LIMIT
+// and its tours are valid but not matched bit for bit.)
 //
-// One CTA per ant, W warps, routes dealt round-robin to the warps.  The tour,
-// node positions, edge lengths, don't-look bytes and route ids live in shared
-// memory; every distance a route's 2-opt reads joins two of its nodes (depot
-// included), so each warp gathers its route's distance sub-matrix into a
-// shared-memory tile once (routes longer than rmax read the L2-resident matrix).
-// A node's neighbour scan takes 32 list entries per warp step and keeps the
-// reference's order: the first entry that ends the scan (radius test fails,
-// kernel.cl:197,229) or improves wins, found with ballot + find-first-set.
+// One CTA per ant; its warps pull routes from a shared counter.  A route of at
+// most 32 nodes (depot included) runs entirely in one warp's registers: lane q
+// holds the local node at route position q, its edge length, and the position
+// of local node q; the don't-look bits are one warp-uniform mask; the route's
+// distance sub-matrix is a 32x32 shared tile; and every node's neighbour list
+// is pre-filtered to the neighbours inside the route, in list order.  The scan
+// of kernel.cl:180-230 only ever stops on an in-route entry (others `continue`),
+// so the filtered list visits exactly the entries that decide the outcome: the
+// first that ends the scan (radius test fails) or improves, found with ballot +
+// find-first-set.  A move reverses a position range with shuffles.  Longer
+// routes take the generic path over shared-memory arrays and the L2-resident
+// distance matrix.
 #include <cuda_runtime.h>
 
 #include "aco_device.cuh"
@@ -34,49 +38,154 @@ namespace {
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
+constexpr int kRL = 32; // largest route (nodes, depot included) of the register path
+
 struct LsLayout {
-    size_t tour, pos, li, rid, dlb, rstart, dt, tiles, rnodes, bytes;
+    size_t tour, pos, li, rid, dlb, rstart, dt, tiles, lnn, lcnt, rnodes, bytes;
 };
 
-__host__ __device__ inline LsLayout ls_layout(int n, int T, int rmax, int warps)
+__host__ __device__ inline LsLayout ls_layout(int n, int T, int warps)
 {
     LsLayout L;
     size_t o = 0;
     L.tour = o; o = al16(o + (size_t)T * 2);
     L.pos = o; o = al16(o + (size_t)n * 2);
-    L.li = o; o = al16(o + (size_t)n * 2);
+    L.li = o; o = al16(o + (size_t)n);
     L.rid = o; o = al16(o + (size_t)n * 2);
     L.dlb = o; o = al16(o + (size_t)n);
     L.rstart = o; o = al16(o + (size_t)(n + 1) * 2);
     L.dt = o; o = al16(o + (size_t)T * 4);
-    L.tiles = o; o = al16(o + (size_t)warps * rmax * rmax * 4);
-    L.rnodes = o; o = al16(o + (size_t)warps * rmax * 2);
+    L.tiles = o; o = al16(o + (size_t)warps * kRL * kRL * 4);
+    L.lnn = o; o = al16(o + (size_t)warps * kRL * kRL);
+    L.lcnt = o; o = al16(o + (size_t)warps * kRL);
+    L.rnodes = o; o = al16(o + (size_t)warps * kRL * 2);
     L.bytes = o;
     return L;
 }
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// ---------------------------------------------------------------------------
+// Register path: routes of at most 32 nodes.
+// ---------------------------------------------------------------------------
+__device__ int two_opt_route_regs(int lane, int R, bool first_route, const float *tile, const uint8_t *lnn,
+                                  const uint8_t *lcnt, int &tq, int &pk, float &dq, int pass_limit)
+{
+    // lane q: tq = local node at position q, dq = dist_tour_wrk of position q;
+    // lane k: pk = position of local node k.  Local node 0 is the depot at position 0.
+    uint32_t dlb = first_route ? 0u : 1u; // bit k: don't-look bit of local node k
+    int passes = 0;
+    bool imp = true;
+    while (imp) {
+        if (pass_limit > 0 && passes >= pass_limit) return ACO_ERR_LS_LIMIT;
+        passes++;
+        imp = false;
+        for (int q1 = 0; q1 < R; q1++) {
+            const int k1 = __shfl_sync(FULL, tq, q1);
+            if ((dlb >> k1) & 1u) continue;
+            const int cnt = lcnt[k1];
+            const int j = lane;
+            const int k2 = j < cnt ? lnn[k1 * kRL + j] : 0;
+            const float d12 = tile[k1 * kRL + k2];
+            const int q2 = __shfl_sync(FULL, pk, k2);
+            bool found = false;
+            int h1 = 0, h2 = 0, h3 = 0, h4 = 0;
+            // successor search (kernel.cl:180-198)
+            {
+                const int ks1 = __shfl_sync(FULL, tq, q1 + 1 < R ? q1 + 1 : 0);
+                const float radius = tile[k1 * kRL + ks1];
+                const int ks2 = __shfl_sync(FULL, tq, q2 + 1 < R ? q2 + 1 : 0);
+                const float dq2 = __shfl_sync(FULL, dq, q2);
+                const bool act = j < cnt;
+                const bool cond = act && __fsub_rn(radius, d12) > kEps;
+                bool okm = false;
+                if (cond) {
+                    const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), tile[ks1 * kRL + ks2]), dq2);
+                    okm = g < -kEps;
+                }
+                const unsigned stop = __ballot_sync(FULL, act && (!cond || okm));
+                if (stop) {
+                    const int f = __ffs(stop) - 1;
+                    if (__shfl_sync(FULL, (int)cond, f)) {
+                        found = true;
+                        h1 = k1;
+                        h2 = ks1;
+                        h3 = __shfl_sync(FULL, k2, f);
+                        h4 = __shfl_sync(FULL, ks2, f);
+                    }
+                }
+            }
+            if (!found) { // predecessor search (kernel.cl:202-230)
+                const int kp1 = __shfl_sync(FULL, tq, q1 > 0 ? q1 - 1 : R - 1);
+                const float radius = tile[kp1 * kRL + k1];
+                const int kpp2 = __shfl_sync(FULL, tq, q2 > 0 ? q2 - 1 : R - 1);
+                const float dqp2 = __shfl_sync(FULL, dq, q2 > 0 ? q2 - 1 : 0);
+                const bool act = j < cnt;
+                const bool cond = act && __fsub_rn(radius, d12) > kEps;
+                bool okm = false;
+                if (cond && !(kpp2 == k1 || kp1 == k2)) {
+                    const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), tile[kp1 * kRL + kpp2]), dqp2);
+                    okm = g < -kEps;
+                }
+                const unsigned stop = __ballot_sync(FULL, act && (!cond || okm));
+                if (stop) {
+                    const int f = __ffs(stop) - 1;
+                    if (__shfl_sync(FULL, (int)cond, f)) {
+                        found = true;
+                        h1 = kp1;
+                        h2 = k1;
+                        h3 = __shfl_sync(FULL, kpp2, f);
+                        h4 = __shfl_sync(FULL, k2, f);
+                    }
+                }
+            }
+            if (!found) {
+                dlb |= 1u << k1; // kernel.cl:232
+                continue;
+            }
+            // exchange (kernel.cl:235-270)
+            imp = true;
+            dlb &= ~((1u << h1) | (1u << h2) | (1u << h3) | (1u << h4));
+            int p1 = __shfl_sync(FULL, pk, h1), p3 = __shfl_sync(FULL, pk, h3);
+            if (p3 < p1) {
+                int t = h1; h1 = h3; h3 = t;
+                t = h2; h2 = h4; h4 = t;
+                t = p1; p1 = p3; p3 = t;
+            }
+            const int i = p1, jj = p3, a = __shfl_sync(FULL, pk, h2);
+            const float d13 = tile[h1 * kRL + h3], d24 = tile[h2 * kRL + h4];
+            // dist_tour_wrk: [i] = d(h1,h3), [jj] = d(h2,h4), (i, jj) reversed
+            const float dsrc = __shfl_sync(FULL, dq, (lane > i && lane < jj) ? i + jj - lane : lane);
+            if (lane == jj) dq = d24; // written after [i], as kernel.cl:249-250
+            else if (lane == i) dq = d13;
+            else if (lane > i && lane < jj) dq = dsrc;
+            // tour positions [a, jj] reversed; positions of the moved nodes mirrored
+            const int tsrc = __shfl_sync(FULL, tq, (lane >= a && lane <= jj) ? a + jj - lane : lane);
+            if (lane >= a && lane <= jj) tq = tsrc;
+            if (pk >= a && pk <= jj) pk = a + jj - pk;
+        }
+    }
+    return ACO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Generic path: any route length, shared-memory arrays, global distances.
+// ---------------------------------------------------------------------------
 struct Route {
-    uint16_t *tour, *pos, *li, *rid, *rnode;
+    uint16_t *tour, *pos, *rid;
     uint8_t *dlb;
-    float *dt, *tile;
+    float *dt;
     const float *dist;
     const int *nn;
-    int ld, nn_ls, lane, r, rb, re, R;
-    bool tiled, dlb0; // dlb0: the depot's don't-look bit inside this route
+    int ld, nn_ls, lane, r, rb, re;
+    bool dlb0; // the depot's don't-look bit inside this route
 
-    __device__ __forceinline__ float D(int a, int b) const
-    {
-        if (tiled) return tile[li[a] * R + li[b]];
-        return __ldg(dist + (size_t)a * ld + b);
-    }
+    __device__ __forceinline__ float D(int a, int b) const { return __ldg(dist + (size_t)a * ld + b); }
     __device__ __forceinline__ int P(int v) const { return v == 0 ? rb : (int)pos[v]; } // tour_node_pos[0] = route_beg
     __device__ __forceinline__ bool in_route(int v) const { return v != 0 && rid[v] == r; }
     __device__ __forceinline__ bool dlb_get(int v) const { return v == 0 ? dlb0 : dlb[v] != 0; }
 };
 
-// kernel.cl:235-270 with all lanes.
 __device__ __forceinline__ void apply_move(Route &c, int h1, int h2, int h3, int h4)
 {
     if (h1 == 0 || h2 == 0 || h3 == 0 || h4 == 0) c.dlb0 = false;
@@ -97,14 +206,14 @@ __device__ __forceinline__ void apply_move(Route &c, int h1, int h2, int h3, int
         c.dt[i] = d13;
         c.dt[j] = d24;
     }
-    const int L1 = j - i - 1; // dist_tour_wrk[i+1 .. j-1] reversed
+    const int L1 = j - i - 1;
     for (int k = c.lane; k < L1 / 2; k += 32) {
         const int x = i + 1 + k, y = j - 1 - k;
         const float tx = c.dt[x];
         c.dt[x] = c.dt[y];
         c.dt[y] = tx;
     }
-    const int L2 = j - a + 1; // tour[pos[h2] .. pos[h3]] reversed
+    const int L2 = j - a + 1;
     for (int k = c.lane; k < L2 / 2; k += 32) {
         const int x = a + k, y = j - k;
         const uint16_t tx = c.tour[x], ty = c.tour[y];
@@ -116,8 +225,7 @@ __device__ __forceinline__ void apply_move(Route &c, int h1, int h2, int h3, int
     __syncwarp();
 }
 
-// two_opt_single_route (kernel.cl:126-277).
-__device__ int two_opt_route(Route &c, int pass_limit)
+__device__ int two_opt_route_generic(Route &c, int pass_limit)
 {
     const int lane = c.lane, rb = c.rb, re = c.re;
     const int nr = re - rb + 1;
@@ -135,7 +243,6 @@ __device__ int two_opt_route(Route &c, int pass_limit)
             float radius = c.D(n1, s1);
             bool found = false;
             int h1 = 0, h2 = 0, h3 = 0, h4 = 0;
-            // successor search (kernel.cl:180-198)
             for (int h0 = 0; h0 < c.nn_ls; h0 += 32) {
                 const int h = h0 + lane;
                 const bool valid = h < c.nn_ls;
@@ -166,7 +273,7 @@ __device__ int two_opt_route(Route &c, int pass_limit)
                     break;
                 }
             }
-            if (!found) { // predecessor search (kernel.cl:202-230)
+            if (!found) {
                 const int p1 = pos1 == rb ? c.tour[re] : c.tour[pos1 - 1];
                 radius = c.D(p1, n1);
                 for (int h0 = 0; h0 < c.nn_ls; h0 += 32) {
@@ -203,7 +310,7 @@ __device__ int two_opt_route(Route &c, int pass_limit)
                     }
                 }
             }
-            if (!found) { // dlb[n1] = TRUE (kernel.cl:232)
+            if (!found) {
                 if (n1 == 0) c.dlb0 = true;
                 else if (lane == 0) c.dlb[n1] = 1;
                 __syncwarp();
@@ -216,21 +323,25 @@ __device__ int two_opt_route(Route &c, int pass_limit)
     return ACO_OK;
 }
 
-__global__ void __launch_bounds__(512) local_search_kernel(LocalSearchArgs a)
+__global__ void __launch_bounds__(1024) local_search_kernel(LocalSearchArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const int n = a.n, T = a.T;
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const LsLayout L = ls_layout(n, T, a.rmax, W);
+    const LsLayout L = ls_layout(n, T, W);
     uint16_t *tour = reinterpret_cast<uint16_t *>(smem + L.tour);
     uint16_t *pos = reinterpret_cast<uint16_t *>(smem + L.pos);
-    uint16_t *li = reinterpret_cast<uint16_t *>(smem + L.li);
+    uint8_t *li = reinterpret_cast<uint8_t *>(smem + L.li);
     uint16_t *rid = reinterpret_cast<uint16_t *>(smem + L.rid);
     uint8_t *dlb = reinterpret_cast<uint8_t *>(smem + L.dlb);
     uint16_t *rstart = reinterpret_cast<uint16_t *>(smem + L.rstart);
     float *dt = reinterpret_cast<float *>(smem + L.dt);
-    __shared__ int s_routes;
+    float *tile = reinterpret_cast<float *>(smem + L.tiles) + (size_t)warp * kRL * kRL;
+    uint8_t *lnn = reinterpret_cast<uint8_t *>(smem + L.lnn) + (size_t)warp * kRL * kRL;
+    uint8_t *lcnt = reinterpret_cast<uint8_t *>(smem + L.lcnt) + (size_t)warp * kRL;
+    uint16_t *rnode = reinterpret_cast<uint16_t *>(smem + L.rnodes) + (size_t)warp * kRL;
+    __shared__ int s_routes, s_next;
 
     const int ant = blockIdx.x;
     int *gtour = a.solutions + (size_t)ant * T;
@@ -244,12 +355,10 @@ __global__ void __launch_bounds__(512) local_search_kernel(LocalSearchArgs a)
         if (v != 0) pos[v] = (uint16_t)p;
     }
     for (int v = threadIdx.x; v < n; v += blockDim.x) dlb[v] = 0;
-    if (threadIdx.x == 0) li[0] = 0; // the depot is local node 0 of every route tile
     __syncthreads();
     for (int p = threadIdx.x; p < size - 1; p += blockDim.x)
         dt[p] = __ldg(a.dist + (size_t)tour[p] * a.ld + tour[p + 1]);
-    // route table: positions of the depots, in order (warp 0 compacts with ballots)
-    if (warp == 0) {
+    if (warp == 0) { // route table: depot positions in order
         int count = 0;
         for (int base = 0; base < size; base += 32) {
             const int p = base + lane;
@@ -258,64 +367,99 @@ __global__ void __launch_bounds__(512) local_search_kernel(LocalSearchArgs a)
             if (dep) rstart[count + __popc(m & ((1u << lane) - 1u))] = (uint16_t)p;
             count += __popc(m);
         }
-        if (lane == 0) s_routes = count - 1; // depots at both ends of each route
+        if (lane == 0) {
+            s_routes = count - 1;
+            s_next = W;
+        }
     }
     __syncthreads();
     const int routes = s_routes;
-    for (int r = warp; r < routes; r += W) // route id of every customer
-        for (int p = rstart[r] + 1 + lane; p < rstart[r + 1]; p += 32) rid[tour[p]] = (uint16_t)r;
+    for (int r = warp; r < routes; r += W) // route id and local index of every customer
+        for (int p = rstart[r] + 1 + lane; p < rstart[r + 1]; p += 32) {
+            rid[tour[p]] = (uint16_t)r;
+            li[tour[p]] = (uint8_t)(p - rstart[r] < 256 ? p - rstart[r] : 0);
+        }
     __syncthreads();
 
-    Route c;
-    c.tour = tour; c.pos = pos; c.li = li; c.rid = rid; c.dlb = dlb; c.dt = dt;
-    c.tile = reinterpret_cast<float *>(smem + L.tiles) + (size_t)warp * a.rmax * a.rmax;
-    c.rnode = reinterpret_cast<uint16_t *>(smem + L.rnodes) + (size_t)warp * a.rmax;
-    c.dist = a.dist; c.nn = a.nn_list; c.ld = a.ld; c.nn_ls = a.nn_ls; c.lane = lane;
     int status = ACO_OK;
-    for (int r = warp; r < routes; r += W) {
-        c.r = r;
-        c.rb = rstart[r];
-        c.re = rstart[r + 1] - 1;
-        c.R = c.re - c.rb + 1;
-        c.dlb0 = r > 0;
-        c.tiled = c.R <= a.rmax;
-        if (c.tiled) {
-            for (int k = lane; k < c.R; k += 32) {
-                const int v = tour[c.rb + k];
-                if (v != 0) li[v] = (uint16_t)k;
-                c.rnode[k] = (uint16_t)v;
+    for (int r = warp; r < routes;) {
+        const int rb = rstart[r], re = rstart[r + 1] - 1, R = re - rb + 1;
+        int st;
+        if (R <= kRL) {
+            // route-local state: node ids, distance tile, in-route neighbour lists
+            const int v = lane < R ? (int)tour[rb + lane] : 0;
+            if (lane < R) rnode[lane] = (uint16_t)v;
+            __syncwarp();
+            for (int e = lane; e < R * kRL; e += 32) {
+                const int k1 = e >> 5, k2 = e & 31;
+                tile[e] = k2 < R ? __ldg(a.dist + (size_t)rnode[k1] * a.ld + rnode[k2]) : 0.f;
+            }
+            for (int k = 0; k < R; k++) {
+                const int node = rnode[k];
+                int cnt = 0;
+                for (int h0 = 0; h0 < a.nn_ls && cnt < R - 1; h0 += 32) {
+                    const int h = h0 + lane;
+                    const int n2 = h < a.nn_ls ? __ldg(a.nn_list + (size_t)node * a.nn_ls + h) : 0;
+                    const bool in = h < a.nn_ls && n2 != 0 && rid[n2] == r;
+                    const unsigned m = __ballot_sync(FULL, in);
+                    const int slot = cnt + __popc(m & ((1u << lane) - 1u));
+                    if (in && slot < kRL) lnn[k * kRL + slot] = li[n2];
+                    cnt += __popc(m);
+                }
+                if (lane == 0) lcnt[k] = (uint8_t)(cnt < R - 1 ? cnt : R - 1);
             }
             __syncwarp();
-            for (int e = lane; e < c.R * c.R; e += 32) {
-                const int k1 = e / c.R, k2 = e - (e / c.R) * c.R;
-                c.tile[e] = __ldg(a.dist + (size_t)c.rnode[k1] * a.ld + c.rnode[k2]);
+            int tq = lane < R ? lane : 0;
+            int pk = lane < R ? lane : 0;
+            float dq = lane < R ? dt[rb + lane] : 0.f;
+            st = two_opt_route_regs(lane, R, r == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
+            const int node = __shfl_sync(FULL, v, tq);
+            if (lane < R) {
+                tour[rb + lane] = (uint16_t)node;
+                dt[rb + lane] = dq;
             }
             __syncwarp();
+        } else {
+            Route c;
+            c.tour = tour; c.pos = pos; c.rid = rid; c.dlb = dlb; c.dt = dt;
+            c.dist = a.dist; c.nn = a.nn_list; c.ld = a.ld; c.nn_ls = a.nn_ls; c.lane = lane;
+            c.r = r; c.rb = rb; c.re = re; c.dlb0 = r > 0;
+            st = two_opt_route_generic(c, a.pass_limit);
         }
-        const int st = two_opt_route(c, a.pass_limit);
         if (st != ACO_OK && status == ACO_OK) status = st;
+        int nxt = 0;
+        if (lane == 0) nxt = atomicAdd(&s_next, 1);
+        r = __shfl_sync(FULL, nxt, 0);
     }
     if (status != ACO_OK && lane == 0) set_status(a.status, status);
     __syncthreads();
 
     for (int p = threadIdx.x; p < size; p += blockDim.x) gtour[p] = tour[p]; // kernel.cl:530-532
-    if (threadIdx.x == 0) {                                                  // kernel.cl:534-538
+    if (warp == 0) { // kernel.cl:534-538: fp32 sum of dist_tour_wrk in position order
         float len = 0.f;
-        for (int p = 0; p < size - 1; p++) len = __fadd_rn(len, dt[p]);
-        a.lens[ant] = len;
+        for (int base = 0; base < size - 1; base += 32) {
+            const float e = base + lane < size - 1 ? dt[base + lane] : 0.f;
+            const int m = size - 1 - base < 32 ? size - 1 - base : 32;
+#pragma unroll
+            for (int k = 0; k < 32; k++) {
+                const float x = __shfl_sync(FULL, e, k);
+                if (k < m) len = __fadd_rn(len, x);
+            }
+        }
+        if (lane == 0) a.lens[ant] = len;
     }
 }
 
 } // namespace
 
-size_t local_search_smem(int n, int /*nn_ls*/, int rmax, int warps, bool /*stage_nn*/)
+size_t local_search_smem(int n, int /*nn_ls*/, int /*rmax*/, int warps, bool /*stage_nn*/)
 {
-    return ls_layout(n, 2 * n, rmax, warps).bytes;
+    return ls_layout(n, 2 * n, warps).bytes;
 }
 
 cudaError_t launch_local_search(const LocalSearchArgs &a, int warps, bool /*stage_nn*/, cudaStream_t st)
 {
-    const size_t bytes = ls_layout(a.n, a.T, a.rmax, warps).bytes;
+    const size_t bytes = ls_layout(a.n, a.T, warps).bytes;
     cudaError_t e = cudaFuncSetAttribute(local_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     local_search_kernel<<<a.n_ants, warps * 32, bytes, st>>>(a);

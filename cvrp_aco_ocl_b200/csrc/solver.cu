@@ -145,14 +145,11 @@ void pick_config(aco_solver *s)
     long long dem = 0;
     for (int i = 1; i < n; i++) dem += s->demand_h[i];
     const int est_routes = s->capacity > 0 ? (int)std::min<long long>(n, dem / s->capacity + 1) : 1;
-    s->ls_apc = std::max(1, std::min(16, est_routes));
+    s->ls_apc = std::max(1, std::min(32, est_routes + 2)); // warps per ant: about one per route
     s->ls_rmax = 32;
     s->ls_snn = false;
-    while (local_search_smem(n, s->nn_ls, s->ls_rmax, s->ls_apc, false) > kSmemBudget) {
-        if (s->ls_apc > 1) s->ls_apc--;
-        else if (s->ls_rmax > 8) s->ls_rmax /= 2;
-        else break;
-    }
+    while (s->ls_apc > 1 && local_search_smem(n, s->nn_ls, s->ls_rmax, s->ls_apc, false) > kSmemBudget)
+        s->ls_apc--;
 }
 
 ConstructArgs cargs(aco_solver *s)
@@ -378,7 +375,7 @@ int aco_create(const aco_instance *inst, const aco_params *params, aco_solver **
     if (p.n_ants <= 0) p.n_ants = n;
     if (p.nloc < 32 || p.nloc > 1024 || (p.nloc & (p.nloc - 1))) return ACO_ERR_INVALID;
     if (p.ras_ranks < 1 || p.ras_ranks > 32) return ACO_ERR_INVALID;
-    if (p.nn_ls < 0 || p.nn_ls > n - 1) return ACO_ERR_INVALID;
+    if (p.nn_ls < 0 || p.nn_ls > n - 2) return ACO_ERR_INVALID; // depth n-1 would list the node itself
     if (p.mode != ACO_MODE_PARITY && p.mode != ACO_MODE_THROUGHPUT) return ACO_ERR_INVALID;
     if (p.mode == ACO_MODE_THROUGHPUT && (p.nn_ants < 1 || p.nn_ants > 32 || p.nn_ants > n - 1))
         return ACO_ERR_INVALID;

@@ -72,7 +72,7 @@ typedef struct aco_params {
     float rho;            /* 0.1 (kernel.cl:9) */
     int ras_ranks;        /* 6 (kernel.cl:12): the best-so-far ant + ras_ranks-1 iteration elites */
     int nn_ants;          /* candidate-list length for ACO_MODE_THROUGHPUT (default min(25, n-2)) */
-    int nn_ls;            /* 2-opt neighbour-list depth (default n-2, problem.cpp:191-193) */
+    int nn_ls;            /* 2-opt neighbour-list depth, <= n-2 (default n-2, problem.cpp:191-193) */
     int ls_flag;          /* 1 = 2-opt after every construction (default 1, problem.cpp:203) */
     int mode;             /* ACO_MODE_* (default PARITY) */
     int nloc;             /* work-items per ant of the reference's construct kernel: maxWorkGroupSize/4

@@ -58,7 +58,7 @@ def test_invalid_params_rejected_before_device():
     inst = I.gen_uniform_small(1, 10)
     prob = Problem.from_instance(inst)
     from cvrp_aco_ocl_b200 import Solver
-    for field, val in [("nloc", 48), ("nloc", 2048), ("ras_ranks", 0), ("ras_ranks", 33), ("nn_ls", 11),
+    for field, val in [("nloc", 48), ("nloc", 2048), ("ras_ranks", 0), ("ras_ranks", 33), ("nn_ls", 10),
                        ("warps_per_ant", 3), ("rho", 0.0)]:
         p = default_params(inst.n)
         setattr(p, field, val)
