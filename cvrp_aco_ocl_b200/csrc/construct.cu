@@ -217,19 +217,25 @@ __global__ void __launch_bounds__(512) construct_parity_kernel(ConstructArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// Throughput mode.  Per CTA: demand and the candidate lists by TMA bulk copy;
-// the total_info matrix too when it fits (SMAT).  Each candidate entry is
-// packed as (node | demand << 16) next to its choice_info value (PACKED), so a
-// step issues one pair of independent shared loads for its 32 lanes, one
-// dependent load of the visited word, the 5-step scan and the selection.  The
-// tour goes to a shared buffer and its length is summed after the last step,
-// in step order (no global load inside the step loop).
+// Throughput mode.  Per CTA: demand, the candidate table and (SMAT) the
+// total_info matrix arrive by TMA bulk copies; the choice_info value of every
+// candidate is gathered once into a compact table.  A candidate entry is packed
+// as (node | demand << 16) when demands fit 16 bits (PACKED), else it is a
+// uint16 node id and the demand is looked up.  Per ant (one warp):
+//   * the Park-Miller draws are made 32 steps at a time, one per lane
+//     (x_{s+j+1} = x_s * 16807^(j+1) mod m), and read with one shuffle per step;
+//   * with n <= 1024 the visited set lives in registers (lane l holds bit j for
+//     node l + 32j): a candidate's bit is one shuffle away, the update needs no
+//     memory operation, and the full-row fallback tests its own bits;
+//   * the 5-step shuffle scan and ballot select the candidate;
+//   * the tour goes to a shared buffer and its length is summed after the last
+//     step, in step order.
 // ---------------------------------------------------------------------------
 struct NNLayout {
-    size_t bar, dem, d0, nn16, cand, chc, vis, tour, mat, bytes;
+    size_t bar, dem, d0, cand, chc, vis, tour, mat, bytes;
 };
 
-__host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, bool smat, bool packed)
+__host__ __device__ inline NNLayout nn_layout(int n, int K, int Kc, int apc, bool smat, bool packed)
 {
     const size_t n4 = (size_t)((n + 3) & ~3);
     const size_t words = (size_t)((n + 31) / 32);
@@ -238,8 +244,7 @@ __host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, boo
     L.bar = o; o = al128(o + 16);
     L.dem = o; o = al128(o + n4 * 4);
     L.d0 = o; o = al128(o + n4 * 4);
-    L.nn16 = o; o = al128(o + (size_t)n * Kp * 2);    // TMA destination (the global layout)
-    L.cand = o; if (packed) o = al128(o + (size_t)n * K * 4);
+    L.cand = o; o = al128(o + (size_t)n * Kc * (packed ? 4 : 2)); // TMA destination, global layout
     L.chc = o; o = al128(o + (size_t)n * K * 4);
     L.vis = o; o = al128(o + (size_t)apc * words * 4);
     L.tour = o; o = al128(o + (size_t)apc * 2 * n * 2);
@@ -249,99 +254,115 @@ __host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, boo
     return L;
 }
 
-template <bool FIN, bool SMAT, bool PACKED>
+template <bool FIN, bool SMAT, bool PACKED, bool REGVIS>
 __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp, T = a.T;
+    const int n = a.n, ld = a.ld, K = a.K, Kc = a.Kp, T = a.T;
     const int n4 = (n + 3) & ~3;
-    const int apc = blockDim.x >> 5;
-    const NNLayout L = nn_layout(n, K, Kp, apc, SMAT, PACKED);
+    const int nwarps = blockDim.x >> 5;
+    const int apc = a.ants_per_cta; // warps beyond the ant warps only help with the prologue
+    const NNLayout L = nn_layout(n, K, Kc, apc, SMAT, PACKED);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar);
     int *s_dem = reinterpret_cast<int *>(smem + L.dem);
     float *s_d0 = reinterpret_cast<float *>(smem + L.d0);
-    uint16_t *s_nn16 = reinterpret_cast<uint16_t *>(smem + L.nn16);
     uint32_t *s_cand = reinterpret_cast<uint32_t *>(smem + L.cand);
+    uint16_t *s_nn = reinterpret_cast<uint16_t *>(smem + L.cand);
     float *s_chc = reinterpret_cast<float *>(smem + L.chc);
     uint32_t *s_vis = reinterpret_cast<uint32_t *>(smem + L.vis);
     uint16_t *s_tour = reinterpret_cast<uint16_t *>(smem + L.tour);
     float *s_mat = reinterpret_cast<float *>(smem + L.mat);
     const int words = (n + 31) >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
 
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         fence_mbar_init();
     }
     __syncthreads();
+    const uint32_t cand_bytes = (uint32_t)(n * Kc * (PACKED ? 4 : 2));
     if (threadIdx.x == 0) {
-        uint32_t bytes = (uint32_t)(n4 * 4 + n * Kp * 2);
+        uint32_t bytes = (uint32_t)(n4 * 4) + cand_bytes;
         if (SMAT) bytes += (uint32_t)(n * n4 * 4);
         mbar_arrive_expect_tx(bar, bytes);
         tma_bulk_g2s(s_dem, a.demand, n4 * 4, bar);
-        tma_bulk_g2s(s_nn16, a.nn16, n * Kp * 2, bar);
+        tma_bulk_g2s(s_cand, PACKED ? (const void *)a.cand32 : (const void *)a.nn16, cand_bytes, bar);
     }
     if (SMAT)
         for (int r = threadIdx.x; r < n; r += blockDim.x)
             tma_bulk_g2s(s_mat + (size_t)r * n4, a.total + (size_t)r * ld, n4 * 4, bar);
     if (FIN)
         for (int i = threadIdx.x; i < n; i += blockDim.x) s_d0[i] = a.dist[(size_t)i * ld];
+    // powers 16807^(lane+1) for the batched draws
+    uint32_t pw = 16807u;
+    for (int k = 0; k < lane; k++) pw = pm_mul(pw, 16807u);
     const bool ok = mbar_wait(bar, 0);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) set_status(a.status, ACO_ERR_TIMEOUT);
         if (!ok) mbar_wait(bar, 0);
         return;
     }
-    // candidate table: row i, entry j = j-th nearest neighbour of i
-    for (int i = warp; i < n; i += apc) {
-        if (lane < K) {
-            const int c = s_nn16[i * Kp + lane];
-            if (PACKED) s_cand[i * K + lane] = (uint32_t)c | ((uint32_t)s_dem[c] << 16);
-            s_chc[i * K + lane] = SMAT ? s_mat[i * n4 + c] : __ldg(a.total + (size_t)i * ld + c);
+    // choice_info of every candidate (row i, entry j: j-th nearest neighbour of i)
+    if (lane < K) {
+        for (int i0 = warp * 4; i0 < n; i0 += nwarps * 4) {
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = i0 + u;
+                if (i < n) {
+                    const int c = PACKED ? (int)(s_cand[i * Kc + lane] & 0xFFFFu) : (int)s_nn[i * Kc + lane];
+                    s_chc[i * K + lane] = SMAT ? s_mat[i * n4 + c] : __ldg(a.total + (size_t)i * ld + c);
+                }
+            }
         }
     }
     __syncthreads();
 
     const int ant = blockIdx.x * apc + warp;
-    if (ant >= a.n_ants) return;
-    uint32_t *vis = s_vis + warp * words;
+    if (warp >= apc || ant >= a.n_ants) return;
     uint16_t *tbuf = s_tour + warp * 2 * n;
-    for (int w = lane; w < words; w += 32) vis[w] = w == 0 ? 1u : 0u;
+    uint32_t *vism = s_vis + warp * words;
+    uint32_t vis = lane == 0 ? 1u : 0u; // register visited set (REGVIS): node 0 = lane 0, bit 0
+    if (!REGVIS) {
+        for (int w = lane; w < words; w += 32) vism[w] = w == 0 ? 1u : 0u;
+        __syncwarp();
+    }
     if (lane == 0) tbuf[0] = 0;
-    __syncwarp();
     int *seedp = a.seeds + (size_t)ant * a.nloc;
-    uint32_t x = pm_norm(seedp[0]);
+    uint32_t xb = pm_norm(seedp[0]), xl = 0u;
+    float ul = 0.f;
     int cur = 0, step = 0, vcnt = 1, load = 0, err = 0;
     float rdist = 0.f;
-    const unsigned FULL = 0xffffffffu;
     const int cap = a.capacity;
+    const int jl = lane < K ? lane : K - 1;
 
     while (vcnt < n) {
         if (step >= T - 3) {
             err = ACO_ERR_STEP_LIMIT;
             break;
         }
-        x = pm_mul(x, 16807u);
-        const float u = pm_uniform(x);
-        int c = 0, dc = 0;
-        float w = 0.f;
-        if (lane < K) {
-            const int e = cur * K + lane;
-            const float wv = s_chc[e];
-            if (PACKED) {
-                const uint32_t pk = s_cand[e];
-                c = (int)(pk & 0xFFFFu);
-                dc = (int)(pk >> 16);
-            } else {
-                c = s_nn16[cur * Kp + lane];
-                dc = s_dem[c];
-            }
-            bool f = !((vis[c >> 5] >> (c & 31)) & 1u) && (load + dc <= cap);
-            if (FIN && f)
-                f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + c), a.serv_time)),
-                              s_d0[c]) <= a.max_dist;
-            w = f ? wv : 0.f;
+        if ((step & 31) == 0) { // the next 32 draws of the ant's stream, one per lane
+            xl = pm_mul(xb, pw);
+            ul = pm_uniform(xl);
+            xb = __shfl_sync(FULL, xl, 31);
         }
+        const float u = __shfl_sync(FULL, ul, step & 31);
+        int c, dc;
+        if (PACKED) {
+            const uint32_t pk = s_cand[cur * Kc + jl];
+            c = (int)(pk & 0xFFFFu);
+            dc = (int)(pk >> 16);
+        } else {
+            c = s_nn[cur * Kc + jl];
+            dc = s_dem[c];
+        }
+        const float wv = s_chc[cur * K + jl];
+        const uint32_t vw = REGVIS ? __shfl_sync(FULL, vis, c & 31) : vism[c >> 5];
+        bool f = lane < K && !((vw >> (REGVIS ? (c >> 5) : (c & 31))) & 1u) && (load + dc <= cap);
+        if (FIN && f)
+            f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + c), a.serv_time)),
+                          s_d0[c]) <= a.max_dist;
+        const float w = f ? wv : 0.f;
         float sc = w; // inclusive Kogge-Stone scan across the warp
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
@@ -352,30 +373,27 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
         int nxt = -1, nd = 0;
         if (tw > 0.f) {
             const float r = __fmul_rn(u, tw);
-            const unsigned pos = __ballot_sync(FULL, w > 0.f);
-            const unsigned hit = __ballot_sync(FULL, w > 0.f && sc > r);
-            const int js = hit ? (__ffs(hit) - 1) : (31 - __clz(pos));
-            nxt = __shfl_sync(FULL, c, js);
-            nd = __shfl_sync(FULL, dc, js);
+            unsigned js = __reduce_min_sync(FULL, (w > 0.f && sc > r) ? (unsigned)lane : 32u);
+            if (js == 32u) js = __reduce_max_sync(FULL, w > 0.f ? (unsigned)lane : 0u); // rounding: last positive
+            const uint32_t pick = __shfl_sync(FULL, (uint32_t)c | ((uint32_t)dc << 16), js);
+            nxt = (int)(pick & 0xFFFFu);
+            nd = (int)(pick >> 16);
         } else { // no listed candidate fits: best feasible customer of the full row
             uint32_t bk = 0u, bi = 0xffffffffu;
-            for (int k = 0; k < words; k++) {
+            const float *row = SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld;
+#pragma unroll 8
+            for (int k = 0; k < words; k++) { // branch-free: every lane tests its own nodes
                 const int i = lane + 32 * k;
-                const uint32_t vw = vis[k];
-                if (i > 0 && i < n && !((vw >> lane) & 1u) && load + s_dem[i] <= cap) {
-                    bool f = true;
-                    if (FIN)
-                        f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + i), a.serv_time)),
-                                      s_d0[i]) <= a.max_dist;
-                    if (f) {
-                        const float v = SMAT ? s_mat[cur * n4 + i] : __ldg(a.total + (size_t)cur * ld + i);
-                        const uint32_t kk = __float_as_uint(v) + 1u;
-                        if (kk > bk) {
-                            bk = kk;
-                            bi = (uint32_t)i;
-                        }
-                    }
-                }
+                const int ic = i < n ? i : 0;
+                const uint32_t vk = REGVIS ? vis : vism[k];
+                bool ff = i > 0 && i < n && !((vk >> (REGVIS ? k : lane)) & 1u) && load + s_dem[ic] <= cap;
+                if (FIN)
+                    ff = ff && __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + ic), a.serv_time)),
+                                         s_d0[ic]) <= a.max_dist;
+                const uint32_t kk = ff ? __float_as_uint(row[ic]) + 1u : 0u;
+                const bool better = kk > bk;
+                bk = better ? kk : bk;
+                bi = better ? (uint32_t)i : bi;
             }
             const uint32_t hk = __reduce_max_sync(FULL, bk);
             if (hk != 0u) {
@@ -393,13 +411,16 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
             if (FIN) rdist = __fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + nxt), a.serv_time));
             vcnt++;
         }
-        if (lane == 0) {
-            vis[nxt >> 5] |= 1u << (nxt & 31);
-            tbuf[step] = (uint16_t)nxt;
+        if (REGVIS) {
+            if (lane == (nxt & 31)) vis |= 1u << (nxt >> 5);
+        } else {
+            if (lane == 0) vism[nxt >> 5] |= 1u << (nxt & 31);
+            __syncwarp();
         }
-        __syncwarp();
+        if (lane == 0) tbuf[step] = (uint16_t)nxt;
         cur = nxt;
     }
+    __syncwarp();
     int *tour = a.solutions + (size_t)ant * T;
     if (err) {
         if (lane == 0) {
@@ -408,10 +429,9 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
             set_status(a.status, err);
         }
     } else {
-        step++;
-        if (lane == 0) tbuf[step] = 0;
+        const int size = step + 2;
+        if (lane == 0) tbuf[step + 1] = 0;
         __syncwarp();
-        const int size = step + 1;
         for (int p = lane; p < size; p += 32) tour[p] = tbuf[p];
         // tour length: the fp32 sum of the edges in step order (kernel.cl:475,483)
         float tdist = 0.f;
@@ -430,7 +450,10 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
             a.lens[ant] = tdist;
         }
     }
-    if (step > 0 && lane == 0) seedp[0] = (int)x;
+    if (step > 0) { // state after the last draw
+        const uint32_t xf = __shfl_sync(FULL, xl, (step - 1) & 31);
+        if (lane == 0) seedp[0] = (int)xf;
+    }
 }
 
 template <int WPA, bool FIN, bool SMAT>
@@ -453,23 +476,27 @@ cudaError_t launch_parity_w(const ConstructArgs &a, int apc, bool smat, cudaStre
     return smat ? launch_parity_t<WPA, false, true>(a, apc, st) : launch_parity_t<WPA, false, false>(a, apc, st);
 }
 
-template <bool FIN, bool SMAT, bool PACKED>
+template <bool FIN, bool SMAT, bool PACKED, bool REGVIS>
 cudaError_t launch_nn_t(const ConstructArgs &a, int apc, cudaStream_t st)
 {
     const NNLayout L = nn_layout(a.n, a.K, a.Kp, apc, SMAT, PACKED);
-    auto kern = construct_nn_kernel<FIN, SMAT, PACKED>;
+    auto kern = construct_nn_kernel<FIN, SMAT, PACKED, REGVIS>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
     if (e != cudaSuccess) return e;
+    ConstructArgs b = a;
+    b.ants_per_cta = apc;
     const int blocks = (a.n_ants + apc - 1) / apc;
-    kern<<<blocks, apc * 32, L.bytes, st>>>(a);
+    const int warps = apc < 8 ? 8 : apc; // helper warps share the prologue (TMA + candidate gather)
+    kern<<<blocks, warps * 32, L.bytes, st>>>(b);
     return cudaGetLastError();
 }
 
-template <bool FIN>
+template <bool FIN, bool REGVIS>
 cudaError_t launch_nn_f(const ConstructArgs &a, int apc, bool smat, bool packed, cudaStream_t st)
 {
-    if (smat) return packed ? launch_nn_t<FIN, true, true>(a, apc, st) : launch_nn_t<FIN, true, false>(a, apc, st);
-    return packed ? launch_nn_t<FIN, false, true>(a, apc, st) : launch_nn_t<FIN, false, false>(a, apc, st);
+    if (smat)
+        return packed ? launch_nn_t<FIN, true, true, REGVIS>(a, apc, st) : launch_nn_t<FIN, true, false, REGVIS>(a, apc, st);
+    return packed ? launch_nn_t<FIN, false, true, REGVIS>(a, apc, st) : launch_nn_t<FIN, false, false, REGVIS>(a, apc, st);
 }
 
 } // namespace
@@ -498,7 +525,9 @@ cudaError_t launch_construct_parity(const ConstructArgs &a, int wpa, int apc, bo
 cudaError_t launch_construct_nn(const ConstructArgs &a, int apc, bool smat, bool packed, cudaStream_t st)
 {
     const bool fin = !(a.max_dist == __builtin_huge_valf());
-    return fin ? launch_nn_f<true>(a, apc, smat, packed, st) : launch_nn_f<false>(a, apc, smat, packed, st);
+    if (a.n <= 1024)
+        return fin ? launch_nn_f<true, true>(a, apc, smat, packed, st) : launch_nn_f<false, true>(a, apc, smat, packed, st);
+    return fin ? launch_nn_f<true, false>(a, apc, smat, packed, st) : launch_nn_f<false, false>(a, apc, smat, packed, st);
 }
 
 } // namespace aco

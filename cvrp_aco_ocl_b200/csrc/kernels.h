@@ -27,8 +27,10 @@ struct ConstructArgs {
     const uint32_t *tiekey;// n (padded): ((0xFFFF - prio) << 16) | node
     const uint32_t *jump;  // kmax (padded): 16807^(k+1) mod m
     const uint32_t *adv;   // nloc: 16807^(draws of lane l per step) mod m
-    const uint16_t *nn16;  // n x Kp candidate lists (throughput)
-    int K, Kp;             // candidate-list length and padded row length
+    const uint16_t *nn16;  // n x Kp candidate lists (throughput), uint16 node ids
+    const uint32_t *cand32;// n x Kp candidate lists, packed node | demand << 16
+    int K, Kp;             // candidate-list length and padded row length (multiple of 8)
+    int ants_per_cta;      // throughput construct: ant warps per CTA (the CTA may have helper warps)
     int *seeds;
     int *solutions;
     float *lens;

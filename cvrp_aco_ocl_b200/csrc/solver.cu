@@ -41,6 +41,7 @@ struct aco_solver {
     int *d_demand = nullptr, *d_nnls = nullptr, *d_seeds = nullptr, *d_sol = nullptr;
     uint32_t *d_key = nullptr, *d_jump = nullptr, *d_adv = nullptr, *d_depmask = nullptr;
     uint16_t *d_nn16 = nullptr;
+    uint32_t *d_cand32 = nullptr;
     float *d_lens = nullptr, *d_dtau = nullptr;
     int *d_elites = nullptr, *d_succ = nullptr, *d_num_bsf = nullptr, *d_iter = nullptr, *d_status = nullptr;
     aco_record *d_records = nullptr;
@@ -130,7 +131,7 @@ void pick_config(aco_solver *s)
     s->cn_stage = false;
     if (s->K > 0) {
         for (int apc = s->cn_apc; apc >= 1 && !s->cn_stage; apc--) {
-            if (packable && construct_nn_smem(n, s->K, s->Kp, apc, true, true) <= kSmemBudget) {
+            if (packable && n <= 1024 && construct_nn_smem(n, s->K, s->Kp, apc, true, true) <= kSmemBudget) {
                 s->cn_stage = s->cn_packed = true;
                 s->cn_apc = apc;
             }
@@ -158,7 +159,7 @@ ConstructArgs cargs(aco_solver *s)
     a.n = s->n; a.ld = s->ld; a.n_ants = s->A; a.T = s->T; a.nloc = s->nloc; a.log2_nloc = s->lg; a.kmax = s->kmax;
     a.capacity = s->capacity; a.max_dist = s->max_dist; a.serv_time = s->serv_time;
     a.total = s->d_total; a.dist = s->d_dist; a.demand = s->d_demand; a.tiekey = s->d_key; a.jump = s->d_jump;
-    a.adv = s->d_adv; a.nn16 = s->d_nn16; a.K = s->K; a.Kp = s->Kp;
+    a.adv = s->d_adv; a.nn16 = s->d_nn16; a.cand32 = s->d_cand32; a.K = s->K; a.Kp = s->Kp;
     a.seeds = s->d_seeds; a.solutions = s->d_sol; a.lens = s->d_lens; a.status = s->d_status;
     return a;
 }
@@ -461,6 +462,7 @@ int aco_create(const aco_instance *inst, const aco_params *params, aco_solver **
     if (rc == ACO_OK) rc = dalloc(s, &s->d_jump, (size_t)((s->kmax + 3) & ~3));
     if (rc == ACO_OK) rc = dalloc(s, &s->d_adv, (size_t)s->nloc);
     if (rc == ACO_OK) rc = dalloc(s, &s->d_nn16, (size_t)n * s->Kp);
+    if (rc == ACO_OK) rc = dalloc(s, &s->d_cand32, (size_t)n * s->Kp);
     if (rc == ACO_OK) rc = dalloc(s, &s->d_nnls, (size_t)n * std::max(1, s->nn_ls));
     if (rc == ACO_OK) rc = dalloc(s, &s->d_seeds, (size_t)s->A * s->nloc);
     if (rc == ACO_OK) rc = dalloc(s, &s->d_sol, (size_t)s->T * (s->A + 1) + 1);
@@ -491,8 +493,13 @@ int aco_create(const aco_instance *inst, const aco_params *params, aco_solver **
     std::vector<uint32_t> adv(s->nloc, 1);
     for (int l = 0; l < s->nloc; l++) adv[l] = pm_pow(l < n ? (uint64_t)((n - l + s->nloc - 1) / s->nloc) : 0);
     std::vector<uint16_t> nn16((size_t)n * s->Kp, 0);
+    std::vector<uint32_t> cand32((size_t)n * s->Kp, 0); // padding entries: node 0 (always visited)
     for (int i = 0; i < n && s->K > 0; i++)
-        for (int j = 0; j < s->K; j++) nn16[(size_t)i * s->Kp + j] = (uint16_t)nn[(size_t)i * depth + j];
+        for (int j = 0; j < s->K; j++) {
+            const int c = nn[(size_t)i * depth + j];
+            nn16[(size_t)i * s->Kp + j] = (uint16_t)c;
+            cand32[(size_t)i * s->Kp + j] = (uint32_t)c | ((uint32_t)(s->demand_h[c] & 0xFFFF) << 16);
+        }
     std::vector<int> nnls((size_t)n * std::max(1, s->nn_ls), 0);
     for (int i = 0; i < n; i++)
         for (int j = 0; j < s->nn_ls; j++) nnls[(size_t)i * s->nn_ls + j] = nn[(size_t)i * depth + j];
@@ -511,6 +518,7 @@ int aco_create(const aco_instance *inst, const aco_params *params, aco_solver **
     ok = ok && up(s->d_jump, jump.data(), jump.size() * 4);
     ok = ok && up(s->d_adv, adv.data(), adv.size() * 4);
     ok = ok && up(s->d_nn16, nn16.data(), nn16.size() * 2);
+    ok = ok && up(s->d_cand32, cand32.data(), cand32.size() * 4);
     ok = ok && up(s->d_nnls, nnls.data(), nnls.size() * 4);
     ok = ok && up(s->d_seeds, seeds.data(), seeds.size() * 4);
     ok = ok && launch_heur(s->d_dist, s->d_heur, n, s->ld, p.beta, s->beta_int, st) == cudaSuccess;
