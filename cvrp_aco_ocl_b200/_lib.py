@@ -31,7 +31,10 @@ EXPORTED = [
     "aco_get_solutions", "aco_get_pheromone", "aco_get_seeds", "aco_get_elites", "aco_get_iteration",
     "aco_set_state", "aco_status", "aco_strerror", "aco_get_stream", "aco_launches_per_iteration",
     "aco_time_iterations", "aco_enqueue_iterations", "aco_time_phases", "aco_get_config",
-    "aco_pheromone_update_noalloc",
+    "aco_pheromone_update_noalloc", "aco_batch_create", "aco_batch_init", "aco_batch_iterate",
+    "aco_batch_enqueue_iterations", "aco_batch_status", "aco_batch_size", "aco_batch_get_best",
+    "aco_batch_get_solutions", "aco_batch_get_pheromone", "aco_batch_time_phases", "aco_batch_get_stream",
+    "aco_batch_destroy",
 ]
 
 
@@ -109,6 +112,20 @@ def lib() -> ctypes.CDLL:
         L.aco_enqueue_iterations.argtypes = [vp, ip]
         L.aco_time_phases.argtypes = [vp, ip, vp]
         L.aco_pheromone_update_noalloc.argtypes = [ip, ip, ip, ip, fp, fp, fp, vp, vp, vp, vp, vp, vp, vp]
+        L.aco_batch_create.argtypes = [ctypes.POINTER(AcoInstance), ip, ctypes.POINTER(AcoParams), ctypes.POINTER(vp)]
+        for name in ("aco_batch_init", "aco_batch_status"):
+            getattr(L, name).argtypes = [vp]
+        L.aco_batch_iterate.argtypes = [vp, ip]
+        L.aco_batch_enqueue_iterations.argtypes = [vp, ip]
+        L.aco_batch_size.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+        L.aco_batch_get_best.argtypes = [vp, ip, vp, ip, ctypes.POINTER(ip), ctypes.POINTER(fp)]
+        L.aco_batch_get_solutions.argtypes = [vp, ip, vp, ctypes.c_size_t, vp, ctypes.c_size_t]
+        L.aco_batch_get_pheromone.argtypes = [vp, ip, vp, vp, ctypes.c_size_t]
+        L.aco_batch_time_phases.argtypes = [vp, ip, vp]
+        L.aco_batch_get_stream.argtypes = [vp]
+        L.aco_batch_get_stream.restype = vp
+        L.aco_batch_destroy.argtypes = [vp]
+        L.aco_batch_destroy.restype = None
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
         _lib = L
     return _lib

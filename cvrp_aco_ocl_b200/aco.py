@@ -321,6 +321,101 @@ class Solver:
         return a.value, w.value, f.value
 
 
+class Batch:
+    """Many independent instances solved by the same launches (throughput mode).
+
+    Instance ``b`` runs exactly the iteration a single ``Solver`` with
+    ``rnd_seed + b`` runs on it; the batch only shares launches, the work
+    queue of the construct kernel and one device arena."""
+
+    def __init__(self, problems: List[Problem], params: Optional[AcoParams] = None, **overrides):
+        self.problems = list(problems)
+        if params is None:
+            params = default_params(max(p.num_node for p in self.problems))
+            params.mode = _lib.MODE_THROUGHPUT
+        for k, v in overrides.items():
+            setattr(params, k, v)
+        self.params = params
+        cis, self._keep = [], []
+        for p in self.problems:
+            ci, keep = p.c_instance()
+            cis.append(ci)
+            self._keep.append(keep)
+        arr = (AcoInstance * len(cis))(*cis)
+        h = ctypes.c_void_p()
+        check(lib().aco_batch_create(arr, len(cis), ctypes.byref(params), ctypes.byref(h)), "aco_batch_create")
+        self.h = h
+        self.A = params.n_ants
+
+    def __len__(self) -> int:
+        return len(self.problems)
+
+    def init(self):
+        check(lib().aco_batch_init(self.h), "aco_batch_init")
+
+    def iterate(self, n_iter: int = 1):
+        check(lib().aco_batch_iterate(self.h, n_iter), "aco_batch_iterate")
+
+    def enqueue(self, n_iter: int = 1):
+        check(lib().aco_batch_enqueue_iterations(self.h, n_iter), "aco_batch_enqueue_iterations")
+
+    def status(self) -> int:
+        return lib().aco_batch_status(self.h)
+
+    def size(self) -> Tuple[int, int]:
+        c, a = ctypes.c_int(), ctypes.c_int()
+        check(lib().aco_batch_size(self.h, ctypes.byref(c), ctypes.byref(a)), "aco_batch_size")
+        return c.value, a.value
+
+    def stream(self) -> int:
+        return lib().aco_batch_get_stream(self.h)
+
+    def best(self, b: int) -> Tuple[np.ndarray, float]:
+        T = 2 * self.problems[b].num_node
+        buf = np.zeros(T, np.int32)
+        size, length = ctypes.c_int(), ctypes.c_float()
+        check(lib().aco_batch_get_best(self.h, b, ptr(buf), T, ctypes.byref(size), ctypes.byref(length)),
+              "aco_batch_get_best")
+        return buf[: size.value].copy(), length.value
+
+    def solutions(self, b: int) -> Tuple[np.ndarray, np.ndarray]:
+        T = 2 * self.problems[b].num_node
+        sol = np.zeros(T * (self.A + 1) + 1, np.int32)
+        lens = np.zeros(self.A + 1, np.float32)
+        check(lib().aco_batch_get_solutions(self.h, b, ptr(sol), sol.size, ptr(lens), lens.size),
+              "aco_batch_get_solutions")
+        return sol, lens
+
+    def pheromone(self, b: int) -> Tuple[np.ndarray, np.ndarray]:
+        n = self.problems[b].num_node
+        tau = np.zeros(n * n, np.float32)
+        tot = np.zeros(n * n, np.float32)
+        check(lib().aco_batch_get_pheromone(self.h, b, ptr(tau), ptr(tot), tau.size), "aco_batch_get_pheromone")
+        return tau, tot
+
+    def time_phases(self, n_iter: int) -> np.ndarray:
+        ms = np.zeros(4, np.float32)
+        check(lib().aco_batch_time_phases(self.h, n_iter, ptr(ms)), "aco_batch_time_phases")
+        return ms
+
+    def close(self):
+        if self.h:
+            lib().aco_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 class GACO:
     """The reference's g_ACO (g_aco.h:16-37) over a Problem: same method names."""
 

@@ -1,0 +1,531 @@
+// colony.cu -- host side of one ACO iteration over one or more instances:
+// preprocessing (g_ACO::create_memory_objects, g_aco.cpp:640-761, and
+// init_problem, problem.cpp:43-56), the device arena, the launch sequence of
+// run_aco_iteration (g_aco.cpp:122-134) and its CUDA graph.
+#include "colony.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <thread>
+
+#include "host.h"
+
+namespace aco {
+
+#define CK(x)                                                                                                  \
+    do {                                                                                                       \
+        cudaError_t e_ = (x);                                                                                  \
+        if (e_ != cudaSuccess) return ACO_ERR_CUDA;                                                            \
+    } while (0)
+
+namespace {
+
+constexpr size_t kSmemBudget = 227 * 1024;
+
+int exp_as_int(float e)
+{
+    if (e >= 0.0f && e <= 8.0f && e == (float)(int)e) return (int)e;
+    return -1;
+}
+
+int ilog2(int v)
+{
+    int r = 0;
+    while ((1 << r) < v) r++;
+    return r;
+}
+
+size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Per-instance host preparation: distances, feasibility, NN lists.
+int prep_instance(const InstanceSpec &sp, const aco_params &p, InstHost &ih)
+{
+    const int n = sp.n;
+    ih.n = n;
+    ih.ld = (n + 31) & ~31;
+    ih.n4 = (n + 3) & ~3;
+    ih.A = p.n_ants > 0 ? p.n_ants : n;
+    ih.T = 2 * n;
+    ih.K = p.mode == ACO_MODE_THROUGHPUT ? std::min(p.nn_ants, n - 2) : 0;
+    if (ih.K < 0) ih.K = 0;
+    ih.Kp = ih.K > 0 ? (ih.K + 7) & ~7 : 8;
+    ih.nn_ls = std::max(0, std::min(p.nn_ls, n - 2));
+    ih.R = p.ras_ranks;
+    ih.nloc = p.nloc;
+    ih.lg = ilog2(p.nloc);
+    ih.kmax = (n + p.nloc - 1) / p.nloc;
+    ih.capacity = sp.capacity;
+    ih.max_dist = sp.max_dist;
+    ih.serv_time = sp.serv_time;
+    ih.dist.resize((size_t)n * n);
+    if (sp.dist) std::memcpy(ih.dist.data(), sp.dist, sizeof(float) * (size_t)n * n);
+    else compute_distances(n, sp.x, sp.y, sp.dist_type, ih.dist.data());
+    ih.demand.assign(sp.demand, sp.demand + n);
+    for (int i = 1; i < n; i++) { // a customer nobody can serve makes construct loop forever (kernel.cl:438,461)
+        if (ih.demand[i] > ih.capacity) return ACO_ERR_INFEASIBLE;
+        const float reach = (0.0f + (ih.dist[i] + ih.serv_time)) + ih.dist[(size_t)i * n];
+        if (!(reach <= ih.max_dist)) return ACO_ERR_INFEASIBLE;
+    }
+    ih.depth = compute_nn_lists(n, ih.dist.data(), ih.nn_ls, ih.K, ih.nn);
+    return ACO_OK;
+}
+
+} // namespace
+
+Colony::~Colony()
+{
+    if (dev >= 0) cudaSetDevice(dev);
+    if (st) cudaStreamSynchronize(st);
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    for (void *q : allocs_) cudaFree(q);
+    if (h_pin) cudaFreeHost(h_pin);
+    if (st) cudaStreamDestroy(st);
+}
+
+int Colony::set_device() const
+{
+    CK(cudaSetDevice(dev));
+    return ACO_OK;
+}
+
+int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
+{
+    p = pin;
+    dev = p.device;
+    inst.resize(count);
+    // ---- host preparation, one thread per core over the instances
+    {
+        std::atomic<int> next{0}, err{ACO_OK};
+        auto work = [&]() {
+            for (;;) {
+                const int b = next.fetch_add(1);
+                if (b >= count) break;
+                const int rc = prep_instance(specs[b], p, inst[b]);
+                if (rc != ACO_OK) err.store(rc);
+            }
+        };
+        const int nth = std::max(1, std::min<int>(count, (int)std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (int t = 1; t < nth; t++) th.emplace_back(work);
+        work();
+        for (auto &t : th) t.join();
+        if (err.load() != ACO_OK) return err.load();
+    }
+    // ---- device
+    int dc = 0;
+    if (cudaGetDeviceCount(&dc) != cudaSuccess || dc <= p.device || p.device < 0) return ACO_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, p.device) != cudaSuccess || prop.major < 10) return ACO_ERR_NO_DEVICE;
+    sm_count = prop.multiProcessorCount;
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaMallocHost(&h_pin, 64));
+
+    // ---- arena layout
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = al256(off + std::max<size_t>(bytes, 16));
+        return o;
+    };
+    struct Offs {
+        size_t dist, heur, tau, total, chc, dem, key, jump, adv, cand32, nn16, nnls, seeds, sol, lens, elites, succ,
+            dep, dtau, rec, nbsf, iter;
+    };
+    std::vector<Offs> offs(count);
+    for (int b = 0; b < count; b++) {
+        const InstHost &ih = inst[b];
+        const size_t nl = (size_t)ih.n * ih.ld * 4;
+        Offs &o = offs[b];
+        o.dist = take(nl); o.heur = take(nl); o.tau = take(nl); o.total = take(nl);
+        o.chc = take((size_t)ih.n * ih.Kp * 4);
+        o.dem = take((size_t)ih.n4 * 4);
+        o.key = take((size_t)ih.n4 * 4);
+        o.jump = take((size_t)((ih.kmax + 3) & ~3) * 4);
+        o.adv = take((size_t)ih.nloc * 4);
+        o.cand32 = take((size_t)ih.n * ih.Kp * 4);
+        o.nn16 = take((size_t)ih.n * ih.Kp * 2);
+        o.nnls = take((size_t)ih.n * std::max(1, ih.nn_ls) * 4);
+        o.seeds = take((size_t)ih.A * ih.nloc * 4);
+        o.sol = take(((size_t)ih.T * (ih.A + 1) + 1) * 4);
+        o.lens = take(((size_t)ih.A + 1) * 4);
+        o.elites = take((size_t)ih.R * 4);
+        o.succ = take((size_t)ih.R * ih.n * 4);
+        o.dep = take((size_t)ih.n * 4);
+        o.dtau = take((size_t)ih.R * 4);
+        o.rec = take((size_t)p.record_cap * sizeof(aco_record));
+        o.nbsf = take(4);
+        o.iter = take(4);
+    }
+    const size_t o_status = take(4), o_t0 = take(8), o_queue = take(4);
+    total_ants = 0;
+    total_rows = 0;
+    ld_max = 32;
+    for (const InstHost &ih : inst) {
+        total_ants += ih.A;
+        total_rows += ih.n;
+        ld_max = std::max(ld_max, ih.ld);
+    }
+    const size_t o_ant_inst = take((size_t)total_ants * 4), o_ant_base = take((size_t)(count + 1) * 4);
+    const size_t o_row_base = take((size_t)(count + 1) * 4);
+    const size_t o_cargs = take(sizeof(ConstructArgs) * count), o_largs = take(sizeof(LocalSearchArgs) * count);
+    const size_t o_sargs = take(sizeof(StatsArgs) * count), o_uargs = take(sizeof(UpdateArgs) * count);
+    // construct work items {instance, first ant}, larger instances first
+    // (set after cn_apc is known; sized for apc = 1)
+    const size_t o_items = take((size_t)total_ants * sizeof(int2));
+
+    void *arena = nullptr;
+    if (cudaMalloc(&arena, off) != cudaSuccess) return ACO_ERR_NOMEM;
+    allocs_.push_back(arena);
+    arena_ = arena;
+    CK(cudaMemsetAsync(arena, 0, off, st));
+    char *base = static_cast<char *>(arena);
+    for (int b = 0; b < count; b++) {
+        InstHost &ih = inst[b];
+        const Offs &o = offs[b];
+        ih.dist_d = (float *)(base + o.dist); ih.heur_d = (float *)(base + o.heur);
+        ih.tau_d = (float *)(base + o.tau); ih.total_d = (float *)(base + o.total);
+        ih.chc_d = (float *)(base + o.chc); ih.dem_d = (int *)(base + o.dem);
+        ih.key_d = (uint32_t *)(base + o.key); ih.jump_d = (uint32_t *)(base + o.jump);
+        ih.adv_d = (uint32_t *)(base + o.adv); ih.cand32_d = (uint32_t *)(base + o.cand32);
+        ih.nn16_d = (uint16_t *)(base + o.nn16); ih.nnls_d = (int *)(base + o.nnls);
+        ih.seeds_d = (int *)(base + o.seeds); ih.sol_d = (int *)(base + o.sol);
+        ih.lens_d = (float *)(base + o.lens); ih.elites_d = (int *)(base + o.elites);
+        ih.succ_d = (int *)(base + o.succ); ih.dep_d = (uint32_t *)(base + o.dep);
+        ih.dtau_d = (float *)(base + o.dtau); ih.rec_d = (aco_record *)(base + o.rec);
+        ih.nbsf_d = (int *)(base + o.nbsf); ih.iter_d = (int *)(base + o.iter);
+    }
+    status_d = (int *)(base + o_status);
+    t0_d_ = (unsigned long long *)(base + o_t0);
+    queue_d_ = (int *)(base + o_queue);
+    ant_inst_d_ = (int *)(base + o_ant_inst);
+    ant_base_d_ = (int *)(base + o_ant_base);
+    row_base_d_ = (int *)(base + o_row_base);
+    cargs_d_ = (ConstructArgs *)(base + o_cargs);
+    largs_d_ = (LocalSearchArgs *)(base + o_largs);
+    sargs_d_ = (StatsArgs *)(base + o_sargs);
+    uargs_d_ = (UpdateArgs *)(base + o_uargs);
+    items_d_ = (int2 *)(base + o_items);
+
+    // ---- configuration (shared-memory budgets over the largest instance)
+    const bool throughput = p.mode == ACO_MODE_THROUGHPUT;
+    fin_any = false;
+    long long max_routes = 1;
+    int A_max = 1;
+    for (const InstHost &ih : inst) {
+        fin_any = fin_any || !std::isinf(ih.max_dist);
+        long long dem = 0;
+        for (int i = 1; i < ih.n; i++) dem += ih.demand[i];
+        max_routes = std::max<long long>(max_routes, ih.capacity > 0 ? dem / ih.capacity + 1 : 1);
+        A_max = std::max(A_max, ih.A);
+    }
+    if (!throughput) { // parity construct: warps per ant so that a thread owns <= 32 nodes of a row
+        const InstHost &ih = inst[0];
+        int wpa = 1;
+        while (wpa < 8 && 32 * wpa * 32 < ih.n) wpa *= 2;
+        while (wpa < 8 && ih.n > 256 * wpa && 32 * wpa * 2 <= ih.nloc) wpa *= 2;
+        wpa = std::min(wpa, ih.nloc / 32);
+        if (p.warps_per_ant > 0) wpa = p.warps_per_ant;
+        cp_wpa = wpa;
+        const int per_block = std::max(1, std::min(8, (ih.A + sm_count - 1) / sm_count));
+        cp_apc = p.ants_per_block > 0 ? p.ants_per_block : std::max(1, per_block / wpa);
+        cp_stage = construct_parity_smem(ih.n, ih.nloc, ih.kmax, wpa, cp_apc, true, fin_any) <= kSmemBudget;
+    } else {
+        // ants per work item: enough CTAs to cover the SMs for one instance,
+        // larger items for big batches (the staging is shared by the item's ants)
+        // (one warp per ant, at most 16 warps: the kernel's launch bound is 512 threads)
+        if (p.ants_per_block > 0) cn_apc = std::min(16, p.ants_per_block);
+        else if (count == 1) cn_apc = std::max(1, std::min(8, (inst[0].A + sm_count - 1) / sm_count));
+        else cn_apc = std::max(1, std::min(16, total_ants / (sm_count * 2)));
+        bool fits = false;
+        while (!fits) {
+            cn_smem = 0;
+            fits = true;
+            for (InstHost &ih : inst) {
+                bool packable = true;
+                for (int i = 0; i < ih.n; i++)
+                    if (ih.demand[i] < 0 || ih.demand[i] > 0xFFFF) packable = false;
+                ih.smat = ih.n <= 1024 && packable && construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, true, true) <= kSmemBudget;
+                ih.packed = packable && construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, ih.smat, true) <= kSmemBudget;
+                const size_t need = construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, ih.smat, ih.packed);
+                if (need > kSmemBudget) fits = false;
+                cn_smem = std::max(cn_smem, need);
+            }
+            if (!fits) {
+                if (cn_apc > 1) cn_apc--;
+                else return ACO_ERR_INVALID; // candidate table of this size cannot be staged
+            }
+        }
+    }
+    ls_warps = (int)std::max<long long>(1, std::min<long long>(32, max_routes + 2));
+    ls_smem = 0;
+    for (const InstHost &ih : inst) ls_smem = std::max(ls_smem, local_search_smem(ih.n, ls_warps));
+    while (ls_warps > 1 && ls_smem > kSmemBudget) {
+        ls_warps--;
+        ls_smem = 0;
+        for (const InstHost &ih : inst) ls_smem = std::max(ls_smem, local_search_smem(ih.n, ls_warps));
+    }
+    stats_smem = (size_t)A_max * sizeof(float);
+    if (stats_smem > kSmemBudget) return ACO_ERR_INVALID; // n_ants lengths must fit in shared memory
+
+    // ---- host tables and uploads
+    std::vector<int> ant_inst(total_ants), ant_base(count + 1), row_base(count + 1);
+    std::vector<int2> items;
+    {
+        int a0 = 0, r0 = 0;
+        for (int b = 0; b < count; b++) {
+            ant_base[b] = a0;
+            row_base[b] = r0;
+            for (int k = 0; k < inst[b].A; k++) ant_inst[a0 + k] = b;
+            a0 += inst[b].A;
+            r0 += inst[b].n;
+        }
+        ant_base[count] = a0;
+        row_base[count] = r0;
+        std::vector<int> order(count);
+        for (int b = 0; b < count; b++) order[b] = b;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return inst[x].n > inst[y].n; });
+        for (int b : order)
+            for (int a0 = 0; a0 < inst[b].A; a0 += cn_apc) items.push_back(make_int2(b, a0));
+        n_items = (int)items.size();
+    }
+    cargs_h_.resize(count);
+    std::vector<LocalSearchArgs> largs(count);
+    std::vector<StatsArgs> sargs(count);
+    std::vector<UpdateArgs> uargs(count);
+    const int ai = exp_as_int(p.alpha), bi = exp_as_int(p.beta);
+    bool ok = true;
+    auto up = [&](void *dst, const void *src, size_t bytes) {
+        ok = ok && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    };
+    for (int b = 0; b < count; b++) {
+        InstHost &ih = inst[b];
+        const int n = ih.n;
+        ok = ok && cudaMemcpy2DAsync(ih.dist_d, (size_t)ih.ld * 4, ih.dist.data(), (size_t)n * 4, (size_t)n * 4, n,
+                                     cudaMemcpyHostToDevice, st) == cudaSuccess;
+        std::vector<int> dem4(ih.n4, 0);
+        std::copy(ih.demand.begin(), ih.demand.end(), dem4.begin());
+        up(ih.dem_d, dem4.data(), dem4.size() * 4);
+        if (!throughput) {
+            const std::vector<int> prio = tournament_priority(n);
+            std::vector<uint32_t> key(ih.n4, 0);
+            for (int i = 0; i < n; i++) key[i] = ((uint32_t)(0xFFFF - prio[i]) << 16) | (uint32_t)i;
+            std::vector<uint32_t> jump((ih.kmax + 3) & ~3, 0);
+            for (int k = 0; k < ih.kmax; k++) jump[k] = pm_pow((uint64_t)k + 1);
+            std::vector<uint32_t> adv(ih.nloc, 1);
+            for (int l = 0; l < ih.nloc; l++)
+                adv[l] = pm_pow(l < n ? (uint64_t)((n - l + ih.nloc - 1) / ih.nloc) : 0);
+            up(ih.key_d, key.data(), key.size() * 4);
+            up(ih.jump_d, jump.data(), jump.size() * 4);
+            up(ih.adv_d, adv.data(), adv.size() * 4);
+        }
+        if (ih.K > 0) {
+            std::vector<uint16_t> nn16((size_t)n * ih.Kp, 0);
+            std::vector<uint32_t> cand32((size_t)n * ih.Kp, 0); // padding entries: node 0 (always visited)
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < ih.K; j++) {
+                    const int c = ih.nn[(size_t)i * ih.depth + j];
+                    nn16[(size_t)i * ih.Kp + j] = (uint16_t)c;
+                    cand32[(size_t)i * ih.Kp + j] = (uint32_t)c | ((uint32_t)(ih.demand[c] & 0xFFFF) << 16);
+                }
+            up(ih.nn16_d, nn16.data(), nn16.size() * 2);
+            up(ih.cand32_d, cand32.data(), cand32.size() * 4);
+        }
+        std::vector<int> nnls((size_t)n * std::max(1, ih.nn_ls), 0);
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < ih.nn_ls; j++) nnls[(size_t)i * ih.nn_ls + j] = ih.nn[(size_t)i * ih.depth + j];
+        up(ih.nnls_d, nnls.data(), nnls.size() * 4);
+        std::vector<int> seeds((size_t)ih.A * ih.nloc);
+        int rs = p.rnd_seed + b; // instance b of a batch: rnd_seed + b
+        make_seeds(p.seed_time, &rs, ih.A, ih.nloc, seeds.data());
+        up(ih.seeds_d, seeds.data(), seeds.size() * 4);
+
+        ConstructArgs &c = cargs_h_[b];
+        c = ConstructArgs{};
+        c.n = n; c.ld = ih.ld; c.n_ants = ih.A; c.T = ih.T; c.nloc = ih.nloc; c.log2_nloc = ih.lg; c.kmax = ih.kmax;
+        c.capacity = ih.capacity; c.max_dist = ih.max_dist; c.serv_time = ih.serv_time;
+        c.total = ih.total_d; c.dist = ih.dist_d; c.demand = ih.dem_d; c.tiekey = ih.key_d; c.jump = ih.jump_d;
+        c.adv = ih.adv_d; c.nn16 = ih.nn16_d; c.cand32 = ih.cand32_d; c.chc = ih.chc_d; c.K = ih.K; c.Kp = ih.Kp;
+        c.smat = ih.smat ? 1 : 0; c.packed = ih.packed ? 1 : 0;
+        c.seeds = ih.seeds_d; c.solutions = ih.sol_d; c.lens = ih.lens_d; c.status = status_d;
+        LocalSearchArgs &l = largs[b];
+        l = LocalSearchArgs{};
+        l.n = n; l.ld = ih.ld; l.n_ants = ih.A; l.T = ih.T; l.nn_ls = ih.nn_ls; l.rmax = 32;
+        l.pass_limit = p.ls_pass_limit; l.dist = ih.dist_d; l.nn_list = ih.nnls_d; l.solutions = ih.sol_d;
+        l.lens = ih.lens_d; l.status = status_d;
+        StatsArgs &s = sargs[b];
+        s = StatsArgs{};
+        s.n = n; s.n_ants = ih.A; s.T = ih.T; s.nloc = ih.nloc; s.log2_nloc = ih.lg; s.ras_ranks = ih.R;
+        s.record_cap = p.record_cap; s.solutions = ih.sol_d; s.lens = ih.lens_d; s.elites = ih.elites_d;
+        s.succ = ih.succ_d; s.depmask = ih.dep_d; s.d_tau = ih.dtau_d; s.num_bsf = ih.nbsf_d; s.records = ih.rec_d;
+        s.iteration = ih.iter_d; s.t0_ns = t0_d_; s.status = status_d;
+        UpdateArgs &u = uargs[b];
+        u = UpdateArgs{};
+        u.n = n; u.ld = ih.ld; u.ras_ranks = ih.R; u.evap = 1.0f - p.rho; u.alpha = p.alpha; u.beta = p.beta;
+        u.alpha_int = ai; u.beta_int = bi; u.rho = p.rho; u.tau = ih.tau_d; u.total = ih.total_d; u.heur = ih.heur_d;
+        u.dist = ih.dist_d; u.succ = ih.succ_d; u.depmask = ih.dep_d; u.d_tau = ih.dtau_d; u.bsf_len = ih.lens_d + ih.A;
+        u.chc = ih.K > 0 ? ih.chc_d : nullptr; u.nn16 = ih.nn16_d; u.K = ih.K; u.Kp = ih.Kp;
+    }
+    up(cargs_d_, cargs_h_.data(), sizeof(ConstructArgs) * count);
+    up(largs_d_, largs.data(), sizeof(LocalSearchArgs) * count);
+    up(sargs_d_, sargs.data(), sizeof(StatsArgs) * count);
+    up(uargs_d_, uargs.data(), sizeof(UpdateArgs) * count);
+    up(ant_inst_d_, ant_inst.data(), ant_inst.size() * 4);
+    up(ant_base_d_, ant_base.data(), ant_base.size() * 4);
+    up(row_base_d_, row_base.data(), row_base.size() * 4);
+    up(items_d_, items.data(), items.size() * sizeof(int2));
+    if (!ok) return ACO_ERR_CUDA;
+    rc = run_rows(ROW_HEUR, 0.f);
+    if (rc != ACO_OK) return rc;
+    CK(cudaStreamSynchronize(st));
+    for (InstHost &ih : inst) { // the host copies of the lists are no longer needed
+        std::vector<int>().swap(ih.nn);
+    }
+    return ACO_OK;
+}
+
+int Colony::run_rows(int mode, float trail)
+{
+    CK(launch_rows(uargs_d_, row_base_d_, (int)inst.size(), total_rows, mode, trail, ld_max, sm_count, st));
+    return ACO_OK;
+}
+
+int Colony::construct()
+{
+    if (p.mode != ACO_MODE_THROUGHPUT) {
+        CK(launch_construct_parity(cargs_h_[0], cp_wpa, cp_apc, cp_stage, st));
+        return ACO_OK;
+    }
+    CK(cudaMemsetAsync(queue_d_, 0, sizeof(int), st));
+    CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st));
+    return ACO_OK;
+}
+
+int Colony::local_search()
+{
+    CK(launch_local_search(largs_d_, ant_inst_d_, ant_base_d_, total_ants, ls_warps, ls_smem, st));
+    return ACO_OK;
+}
+
+int Colony::stats(bool elites)
+{
+    CK(launch_stats(sargs_d_, (int)inst.size(), elites ? 1 : 0, stats_smem, st));
+    return ACO_OK;
+}
+
+int Colony::update() { return run_rows(ROW_UPDATE, 0.f); }
+
+int Colony::pheromone_init(float trail, bool from_bsf)
+{
+    return run_rows(from_bsf ? ROW_INIT_BSF : ROW_INIT_TRAIL, trail);
+}
+
+int Colony::gather_candidates() { return p.mode == ACO_MODE_THROUGHPUT ? run_rows(ROW_GATHER, 0.f) : ACO_OK; }
+
+int Colony::run_phases()
+{
+    int rc = construct();
+    if (rc == ACO_OK && p.ls_flag) rc = local_search();
+    if (rc == ACO_OK) rc = stats(true);
+    if (rc == ACO_OK) rc = update();
+    return rc;
+}
+
+int Colony::sync_status()
+{
+    CK(cudaMemcpyAsync(h_pin, status_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return h_pin[0];
+}
+
+int Colony::ensure_graph()
+{
+    if (exec_) return ACO_OK;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = run_phases();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != ACO_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return rc != ACO_OK ? rc : ACO_ERR_CUDA;
+    }
+    graph_ = g;
+    CK(cudaGraphInstantiate(&exec_, g, 0));
+    return ACO_OK;
+}
+
+int Colony::init()
+{
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    const float inf = INFINITY;
+    for (InstHost &ih : inst) {
+        CK(cudaMemcpyAsync(ih.lens_d + ih.A, &inf, sizeof(float), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(ih.nbsf_d, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(ih.iter_d, 0, sizeof(int), st));
+    }
+    CK(cudaMemsetAsync(status_d, 0, sizeof(int), st));
+    CK(launch_t0(t0_d_, st));
+    t_init = std::chrono::steady_clock::now();
+    // g_aco.cpp:79-92
+    rc = pheromone_init(0.5f, false);
+    if (rc == ACO_OK) rc = construct();
+    if (rc == ACO_OK && p.ls_flag) rc = local_search();
+    if (rc == ACO_OK) rc = stats(false);
+    if (rc == ACO_OK) rc = pheromone_init(0.f, true);
+    if (rc != ACO_OK) return rc;
+    const int status = sync_status();
+    initialized = status == ACO_OK;
+    return status;
+}
+
+int Colony::enqueue(int n_iter)
+{
+    if (!initialized) return ACO_ERR_STATE;
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    if (p.use_graph) {
+        rc = ensure_graph();
+        if (rc != ACO_OK) return rc;
+        for (int i = 0; i < n_iter; i++) CK(cudaGraphLaunch(exec_, st));
+        return ACO_OK;
+    }
+    for (int i = 0; i < n_iter && rc == ACO_OK; i++) rc = run_phases();
+    return rc;
+}
+
+int Colony::time_phases(int n_iter, float *ms4)
+{
+    if (!initialized) return ACO_ERR_STATE;
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    cudaEvent_t ev[5];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    for (int k = 0; k < 4; k++) ms4[k] = 0.f;
+    for (int it = 0; it < n_iter && rc == ACO_OK; it++) {
+        CK(cudaEventRecord(ev[0], st));
+        rc = construct();
+        CK(cudaEventRecord(ev[1], st));
+        if (rc == ACO_OK && p.ls_flag) rc = local_search();
+        CK(cudaEventRecord(ev[2], st));
+        if (rc == ACO_OK) rc = stats(true);
+        CK(cudaEventRecord(ev[3], st));
+        if (rc == ACO_OK) rc = update();
+        CK(cudaEventRecord(ev[4], st));
+        CK(cudaEventSynchronize(ev[4]));
+        for (int k = 0; k < 4; k++) {
+            float m = 0.f;
+            CK(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));
+            ms4[k] += m;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (rc != ACO_OK) return rc;
+    return sync_status();
+}
+
+} // namespace aco

@@ -1,0 +1,104 @@
+// colony.h -- device state of one or more independent CVRP instances (a
+// "colony" each) and the launch sequence of one ACO iteration over all of them.
+// A single solver is a colony of one instance; a batch is a colony of many,
+// all in one device arena, served by the same launches.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/cvrp_aco.h"
+#include "kernels.h"
+
+namespace aco {
+
+struct InstanceSpec { // the fields of aco_instance
+    int n;
+    const float *x, *y;
+    const int *demand;
+    int capacity;
+    float max_dist, serv_time;
+    int dist_type;
+    const float *dist;
+};
+
+struct InstHost {
+    int n = 0, ld = 0, n4 = 0, A = 0, T = 0, K = 0, Kp = 8, nn_ls = 0, R = 0, nloc = 0, lg = 0, kmax = 0;
+    int capacity = 0;
+    float max_dist = 0, serv_time = 0;
+    bool smat = false, packed = false;
+    std::vector<float> dist; // n*n
+    std::vector<int> demand;
+    std::vector<int> nn;     // n x depth
+    int depth = 0;
+    // device pointers inside the arena
+    float *dist_d = nullptr, *heur_d = nullptr, *tau_d = nullptr, *total_d = nullptr, *chc_d = nullptr;
+    int *dem_d = nullptr, *nnls_d = nullptr, *seeds_d = nullptr, *sol_d = nullptr, *elites_d = nullptr;
+    int *succ_d = nullptr, *nbsf_d = nullptr, *iter_d = nullptr;
+    uint32_t *key_d = nullptr, *jump_d = nullptr, *adv_d = nullptr, *cand32_d = nullptr, *dep_d = nullptr;
+    uint16_t *nn16_d = nullptr;
+    float *lens_d = nullptr, *dtau_d = nullptr;
+    aco_record *rec_d = nullptr;
+};
+
+class Colony {
+public:
+    ~Colony();
+    // Host preprocessing (distances, NN lists, seeds, tables), one device arena,
+    // uploads.  `parity` allows ACO_MODE_PARITY (single instance only).
+    int create(const InstanceSpec *specs, int count, const aco_params &p);
+
+    int init();                  // g_ACO::init_aco for every instance
+    int enqueue(int n_iter);     // n_iter iterations (graph replays), no sync
+    int sync_status();           // wait for the stream, read the sticky status
+    int construct();
+    int local_search();
+    int stats(bool elites);
+    int update();
+    int pheromone_init(float trail, bool from_bsf);
+    int gather_candidates();     // refresh the compact candidate table from total_info
+    int time_phases(int n_iter, float *ms4);
+    int set_device() const;
+
+    aco_params p{};
+    int dev = 0, sm_count = 148;
+    cudaStream_t st = nullptr;
+    std::vector<InstHost> inst;
+    bool initialized = false;
+    std::chrono::steady_clock::time_point t_init;
+    int *h_pin = nullptr;
+    int *status_d = nullptr;
+
+    // launch configuration
+    int cp_wpa = 1, cp_apc = 1;
+    bool cp_stage = false;
+    int cn_apc = 1;
+    size_t cn_smem = 0;
+    int ls_warps = 1;
+    size_t ls_smem = 0, stats_smem = 0;
+    int ld_max = 32, total_ants = 0, total_rows = 0, n_items = 0;
+    bool fin_any = false;
+
+private:
+    int run_phases();
+    int ensure_graph();
+    int run_rows(int mode, float trail);
+    std::vector<void *> allocs_;
+    void *arena_ = nullptr;
+    unsigned long long *t0_d_ = nullptr;
+    int2 *items_d_ = nullptr;
+    int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
+    int *row_base_d_ = nullptr;
+    ConstructArgs *cargs_d_ = nullptr;
+    LocalSearchArgs *largs_d_ = nullptr;
+    StatsArgs *sargs_d_ = nullptr;
+    UpdateArgs *uargs_d_ = nullptr;
+    std::vector<ConstructArgs> cargs_h_;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+};
+
+} // namespace aco

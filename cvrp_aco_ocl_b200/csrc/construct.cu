@@ -217,17 +217,18 @@ __global__ void __launch_bounds__(512) construct_parity_kernel(ConstructArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// Throughput mode.  Per CTA: demand, the candidate table and (SMAT) the
-// total_info matrix arrive by TMA bulk copies; the choice_info value of every
-// candidate is gathered once into a compact table.  A candidate entry is packed
-// as (node | demand << 16) when demands fit 16 bits (PACKED), else it is a
-// uint16 node id and the demand is looked up.  Per ant (one warp):
+// Throughput mode.  A persistent kernel: each CTA pulls work items (instance,
+// group of `apc` ants) from a device queue, stages the instance's demand,
+// candidate table (cand32 packed as node | demand << 16, or uint16 nodes),
+// candidate choice_info (chc) and -- when it fits (smat) -- the whole
+// total_info matrix into shared memory with TMA bulk copies, then runs one
+// warp per ant.  Per ant:
 //   * the Park-Miller draws are made 32 steps at a time, one per lane
 //     (x_{s+j+1} = x_s * 16807^(j+1) mod m), and read with one shuffle per step;
 //   * with n <= 1024 the visited set lives in registers (lane l holds bit j for
 //     node l + 32j): a candidate's bit is one shuffle away, the update needs no
 //     memory operation, and the full-row fallback tests its own bits;
-//   * the 5-step shuffle scan and ballot select the candidate;
+//   * the 5-step shuffle scan and a redux over lane ids select the candidate;
 //   * the tour goes to a shared buffer and its length is summed after the last
 //     step, in step order.
 // ---------------------------------------------------------------------------
@@ -235,7 +236,7 @@ struct NNLayout {
     size_t bar, dem, d0, cand, chc, vis, tour, mat, bytes;
 };
 
-__host__ __device__ inline NNLayout nn_layout(int n, int K, int Kc, int apc, bool smat, bool packed)
+__host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, bool smat, bool packed)
 {
     const size_t n4 = (size_t)((n + 3) & ~3);
     const size_t words = (size_t)((n + 31) / 32);
@@ -244,25 +245,26 @@ __host__ __device__ inline NNLayout nn_layout(int n, int K, int Kc, int apc, boo
     L.bar = o; o = al128(o + 16);
     L.dem = o; o = al128(o + n4 * 4);
     L.d0 = o; o = al128(o + n4 * 4);
-    L.cand = o; o = al128(o + (size_t)n * Kc * (packed ? 4 : 2)); // TMA destination, global layout
-    L.chc = o; o = al128(o + (size_t)n * K * 4);
+    L.cand = o; o = al128(o + (size_t)n * Kp * (packed ? 4 : 2));
+    L.chc = o; o = al128(o + (size_t)n * Kp * 4);
     L.vis = o; o = al128(o + (size_t)apc * words * 4);
     L.tour = o; o = al128(o + (size_t)apc * 2 * n * 2);
     L.mat = o;
     if (smat) o = al128(o + (size_t)n * n4 * 4);
     L.bytes = o;
+    (void)K;
     return L;
 }
 
+// One work item: ants [ant0, ant0 + apc) of instance a.  Returns false if the
+// staging copies did not arrive in time (uniform over the CTA).
 template <bool FIN, bool SMAT, bool PACKED, bool REGVIS>
-__global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
+__device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int apc, int ant0, unsigned char *smem, uint32_t phase,
+                                  uint32_t pw)
 {
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int n = a.n, ld = a.ld, K = a.K, Kc = a.Kp, T = a.T;
+    const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp, T = a.T;
     const int n4 = (n + 3) & ~3;
-    const int nwarps = blockDim.x >> 5;
-    const int apc = a.ants_per_cta; // warps beyond the ant warps only help with the prologue
-    const NNLayout L = nn_layout(n, K, Kc, apc, SMAT, PACKED);
+    const NNLayout L = nn_layout(n, K, Kp, apc, SMAT, PACKED);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar);
     int *s_dem = reinterpret_cast<int *>(smem + L.dem);
     float *s_d0 = reinterpret_cast<float *>(smem + L.d0);
@@ -276,183 +278,204 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(ConstructArgs a)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
 
+    const uint32_t cand_bytes = (uint32_t)(n * Kp * (PACKED ? 4 : 2));
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    const uint32_t cand_bytes = (uint32_t)(n * Kc * (PACKED ? 4 : 2));
-    if (threadIdx.x == 0) {
-        uint32_t bytes = (uint32_t)(n4 * 4) + cand_bytes;
+        uint32_t bytes = (uint32_t)(n4 * 4) + cand_bytes + (uint32_t)(n * Kp * 4);
         if (SMAT) bytes += (uint32_t)(n * n4 * 4);
         mbar_arrive_expect_tx(bar, bytes);
         tma_bulk_g2s(s_dem, a.demand, n4 * 4, bar);
         tma_bulk_g2s(s_cand, PACKED ? (const void *)a.cand32 : (const void *)a.nn16, cand_bytes, bar);
+        tma_bulk_g2s(s_chc, a.chc, n * Kp * 4, bar);
     }
     if (SMAT)
         for (int r = threadIdx.x; r < n; r += blockDim.x)
             tma_bulk_g2s(s_mat + (size_t)r * n4, a.total + (size_t)r * ld, n4 * 4, bar);
     if (FIN)
         for (int i = threadIdx.x; i < n; i += blockDim.x) s_d0[i] = a.dist[(size_t)i * ld];
-    // powers 16807^(lane+1) for the batched draws
-    uint32_t pw = 16807u;
-    for (int k = 0; k < lane; k++) pw = pm_mul(pw, 16807u);
-    const bool ok = mbar_wait(bar, 0);
+    const bool ok = mbar_wait(bar, phase);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) set_status(a.status, ACO_ERR_TIMEOUT);
-        if (!ok) mbar_wait(bar, 0);
-        return;
+        if (!ok) mbar_wait(bar, phase);
+        return false;
     }
-    // choice_info of every candidate (row i, entry j: j-th nearest neighbour of i)
-    if (lane < K) {
-        for (int i0 = warp * 4; i0 < n; i0 += nwarps * 4) {
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int i = i0 + u;
-                if (i < n) {
-                    const int c = PACKED ? (int)(s_cand[i * Kc + lane] & 0xFFFFu) : (int)s_nn[i * Kc + lane];
-                    s_chc[i * K + lane] = SMAT ? s_mat[i * n4 + c] : __ldg(a.total + (size_t)i * ld + c);
-                }
-            }
-        }
-    }
-    __syncthreads();
 
-    const int ant = blockIdx.x * apc + warp;
-    if (warp >= apc || ant >= a.n_ants) return;
-    uint16_t *tbuf = s_tour + warp * 2 * n;
-    uint32_t *vism = s_vis + warp * words;
-    uint32_t vis = lane == 0 ? 1u : 0u; // register visited set (REGVIS): node 0 = lane 0, bit 0
-    if (!REGVIS) {
-        for (int w = lane; w < words; w += 32) vism[w] = w == 0 ? 1u : 0u;
-        __syncwarp();
-    }
-    if (lane == 0) tbuf[0] = 0;
-    int *seedp = a.seeds + (size_t)ant * a.nloc;
-    uint32_t xb = pm_norm(seedp[0]), xl = 0u;
-    float ul = 0.f;
-    int cur = 0, step = 0, vcnt = 1, load = 0, err = 0;
-    float rdist = 0.f;
-    const int cap = a.capacity;
-    const int jl = lane < K ? lane : K - 1;
-
-    while (vcnt < n) {
-        if (step >= T - 3) {
-            err = ACO_ERR_STEP_LIMIT;
-            break;
-        }
-        if ((step & 31) == 0) { // the next 32 draws of the ant's stream, one per lane
-            xl = pm_mul(xb, pw);
-            ul = pm_uniform(xl);
-            xb = __shfl_sync(FULL, xl, 31);
-        }
-        const float u = __shfl_sync(FULL, ul, step & 31);
-        int c, dc;
-        if (PACKED) {
-            const uint32_t pk = s_cand[cur * Kc + jl];
-            c = (int)(pk & 0xFFFFu);
-            dc = (int)(pk >> 16);
-        } else {
-            c = s_nn[cur * Kc + jl];
-            dc = s_dem[c];
-        }
-        const float wv = s_chc[cur * K + jl];
-        const uint32_t vw = REGVIS ? __shfl_sync(FULL, vis, c & 31) : vism[c >> 5];
-        bool f = lane < K && !((vw >> (REGVIS ? (c >> 5) : (c & 31))) & 1u) && (load + dc <= cap);
-        if (FIN && f)
-            f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + c), a.serv_time)),
-                          s_d0[c]) <= a.max_dist;
-        const float w = f ? wv : 0.f;
-        float sc = w; // inclusive Kogge-Stone scan across the warp
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const float o = __shfl_up_sync(FULL, sc, off);
-            if (lane >= off) sc = __fadd_rn(sc, o);
-        }
-        const float tw = __shfl_sync(FULL, sc, 31);
-        int nxt = -1, nd = 0;
-        if (tw > 0.f) {
-            const float r = __fmul_rn(u, tw);
-            unsigned js = __reduce_min_sync(FULL, (w > 0.f && sc > r) ? (unsigned)lane : 32u);
-            if (js == 32u) js = __reduce_max_sync(FULL, w > 0.f ? (unsigned)lane : 0u); // rounding: last positive
-            const uint32_t pick = __shfl_sync(FULL, (uint32_t)c | ((uint32_t)dc << 16), js);
-            nxt = (int)(pick & 0xFFFFu);
-            nd = (int)(pick >> 16);
-        } else { // no listed candidate fits: best feasible customer of the full row
-            uint32_t bk = 0u, bi = 0xffffffffu;
-            const float *row = SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld;
-#pragma unroll 8
-            for (int k = 0; k < words; k++) { // branch-free: every lane tests its own nodes
-                const int i = lane + 32 * k;
-                const int ic = i < n ? i : 0;
-                const uint32_t vk = REGVIS ? vis : vism[k];
-                bool ff = i > 0 && i < n && !((vk >> (REGVIS ? k : lane)) & 1u) && load + s_dem[ic] <= cap;
-                if (FIN)
-                    ff = ff && __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + ic), a.serv_time)),
-                                         s_d0[ic]) <= a.max_dist;
-                const uint32_t kk = ff ? __float_as_uint(row[ic]) + 1u : 0u;
-                const bool better = kk > bk;
-                bk = better ? kk : bk;
-                bi = better ? (uint32_t)i : bi;
-            }
-            const uint32_t hk = __reduce_max_sync(FULL, bk);
-            if (hk != 0u) {
-                nxt = (int)__reduce_min_sync(FULL, bk == hk ? bi : 0xffffffffu);
-                nd = s_dem[nxt];
-            }
-        }
-        step++;
-        if (nxt < 0) {
-            nxt = 0;
-            load = 0;
-            rdist = 0.f;
-        } else {
-            load += nd;
-            if (FIN) rdist = __fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + nxt), a.serv_time));
-            vcnt++;
-        }
-        if (REGVIS) {
-            if (lane == (nxt & 31)) vis |= 1u << (nxt >> 5);
-        } else {
-            if (lane == 0) vism[nxt >> 5] |= 1u << (nxt & 31);
+    const int ant = ant0 + warp;
+    if (warp < apc && ant < a.n_ants) {
+        uint16_t *tbuf = s_tour + warp * 2 * n;
+        uint32_t *vism = s_vis + warp * words;
+        uint32_t vis = lane == 0 ? 1u : 0u; // register visited set (REGVIS): node 0 = lane 0, bit 0
+        if (!REGVIS) {
+            for (int w = lane; w < words; w += 32) vism[w] = w == 0 ? 1u : 0u;
             __syncwarp();
         }
-        if (lane == 0) tbuf[step] = (uint16_t)nxt;
-        cur = nxt;
-    }
-    __syncwarp();
-    int *tour = a.solutions + (size_t)ant * T;
-    if (err) {
-        if (lane == 0) {
-            tour[T - 1] = 0;
-            a.lens[ant] = __int_as_float(0x7f800000);
-            set_status(a.status, err);
-        }
-    } else {
-        const int size = step + 2;
-        if (lane == 0) tbuf[step + 1] = 0;
-        __syncwarp();
-        for (int p = lane; p < size; p += 32) tour[p] = tbuf[p];
-        // tour length: the fp32 sum of the edges in step order (kernel.cl:475,483)
-        float tdist = 0.f;
-        for (int base = 0; base < size - 1; base += 32) {
-            const int p = base + lane;
-            const float e = p < size - 1 ? __ldg(a.dist + (size_t)tbuf[p] * ld + tbuf[p + 1]) : 0.f;
-            const int m = size - 1 - base < 32 ? size - 1 - base : 32;
+        if (lane == 0) tbuf[0] = 0;
+        int *seedp = a.seeds + (size_t)ant * a.nloc;
+        uint32_t xb = pm_norm(seedp[0]), xl = 0u;
+        float ul = 0.f;
+        int cur = 0, step = 0, vcnt = 1, load = 0, err = 0;
+        float rdist = 0.f;
+        const int cap = a.capacity;
+        const int jl = lane < K ? lane : K - 1;
+
+        while (vcnt < n) {
+            if (step >= T - 3) {
+                err = ACO_ERR_STEP_LIMIT;
+                break;
+            }
+            if ((step & 31) == 0) { // the next 32 draws of the ant's stream, one per lane
+                xl = pm_mul(xb, pw);
+                ul = pm_uniform(xl);
+                xb = __shfl_sync(FULL, xl, 31);
+            }
+            const float u = __shfl_sync(FULL, ul, step & 31);
+            int c, dc;
+            if (PACKED) {
+                const uint32_t pk = s_cand[cur * Kp + jl];
+                c = (int)(pk & 0xFFFFu);
+                dc = (int)(pk >> 16);
+            } else {
+                c = s_nn[cur * Kp + jl];
+                dc = s_dem[c];
+            }
+            const float wv = s_chc[cur * Kp + jl];
+            const uint32_t vw = REGVIS ? __shfl_sync(FULL, vis, c & 31) : vism[c >> 5];
+            bool f = lane < K && !((vw >> (REGVIS ? (c >> 5) : (c & 31))) & 1u) && (load + dc <= cap);
+            if (FIN && f)
+                f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + c), a.serv_time)),
+                              s_d0[c]) <= a.max_dist;
+            const float w = f ? wv : 0.f;
+            float sc = w; // inclusive Kogge-Stone scan across the warp
 #pragma unroll
-            for (int k = 0; k < 32; k++) {
-                const float y = __shfl_sync(FULL, e, k);
-                if (k < m) tdist = __fadd_rn(tdist, y);
+            for (int off = 1; off < 32; off <<= 1) {
+                const float o = __shfl_up_sync(FULL, sc, off);
+                if (lane >= off) sc = __fadd_rn(sc, o);
+            }
+            const float tw = __shfl_sync(FULL, sc, 31);
+            int nxt = -1, nd = 0;
+            if (tw > 0.f) {
+                const float r = __fmul_rn(u, tw);
+                unsigned js = __reduce_min_sync(FULL, (w > 0.f && sc > r) ? (unsigned)lane : 32u);
+                if (js == 32u) js = __reduce_max_sync(FULL, w > 0.f ? (unsigned)lane : 0u); // rounding: last positive
+                const uint32_t pick = __shfl_sync(FULL, (uint32_t)c | ((uint32_t)dc << 16), js);
+                nxt = (int)(pick & 0xFFFFu);
+                nd = (int)(pick >> 16);
+            } else { // no listed candidate fits: best feasible customer of the full row
+                uint32_t bk = 0u, bi = 0xffffffffu;
+                const float *row = SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld;
+#pragma unroll 8
+                for (int k = 0; k < words; k++) { // branch-free: every lane tests its own nodes
+                    const int i = lane + 32 * k;
+                    const int ic = i < n ? i : 0;
+                    const uint32_t vk = REGVIS ? vis : vism[k];
+                    bool ff = i > 0 && i < n && !((vk >> (REGVIS ? k : lane)) & 1u) && load + s_dem[ic] <= cap;
+                    if (FIN)
+                        ff = ff && __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + ic),
+                                                                        a.serv_time)),
+                                             s_d0[ic]) <= a.max_dist;
+                    const uint32_t kk = ff ? __float_as_uint(row[ic]) + 1u : 0u;
+                    const bool better = kk > bk;
+                    bk = better ? kk : bk;
+                    bi = better ? (uint32_t)i : bi;
+                }
+                const uint32_t hk = __reduce_max_sync(FULL, bk);
+                if (hk != 0u) {
+                    nxt = (int)__reduce_min_sync(FULL, bk == hk ? bi : 0xffffffffu);
+                    nd = s_dem[nxt];
+                }
+            }
+            step++;
+            if (nxt < 0) {
+                nxt = 0;
+                load = 0;
+                rdist = 0.f;
+            } else {
+                load += nd;
+                if (FIN) rdist = __fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + nxt), a.serv_time));
+                vcnt++;
+            }
+            if (REGVIS) {
+                if (lane == (nxt & 31)) vis |= 1u << (nxt >> 5);
+            } else {
+                if (lane == 0) vism[nxt >> 5] |= 1u << (nxt & 31);
+                __syncwarp();
+            }
+            if (lane == 0) tbuf[step] = (uint16_t)nxt;
+            cur = nxt;
+        }
+        __syncwarp();
+        int *tour = a.solutions + (size_t)ant * T;
+        if (err) {
+            if (lane == 0) {
+                tour[T - 1] = 0;
+                a.lens[ant] = __int_as_float(0x7f800000);
+                set_status(a.status, err);
+            }
+        } else {
+            const int size = step + 2;
+            if (lane == 0) tbuf[step + 1] = 0;
+            __syncwarp();
+            for (int p = lane; p < size; p += 32) tour[p] = tbuf[p];
+            // tour length: the fp32 sum of the edges in step order (kernel.cl:475,483)
+            float tdist = 0.f;
+            for (int base = 0; base < size - 1; base += 32) {
+                const int p = base + lane;
+                const float e = p < size - 1 ? __ldg(a.dist + (size_t)tbuf[p] * ld + tbuf[p + 1]) : 0.f;
+                const int m = size - 1 - base < 32 ? size - 1 - base : 32;
+#pragma unroll
+                for (int k = 0; k < 32; k++) {
+                    const float y = __shfl_sync(FULL, e, k);
+                    if (k < m) tdist = __fadd_rn(tdist, y);
+                }
+            }
+            if (lane == 0) {
+                tour[T - 1] = size;
+                a.lens[ant] = tdist;
             }
         }
-        if (lane == 0) {
-            tour[T - 1] = size;
-            a.lens[ant] = tdist;
+        if (step > 0) { // state after the last draw
+            const uint32_t xf = __shfl_sync(FULL, xl, (step - 1) & 31);
+            if (lane == 0) seedp[0] = (int)xf;
         }
     }
-    if (step > 0) { // state after the last draw
-        const uint32_t xf = __shfl_sync(FULL, xl, (step - 1) & 31);
-        if (lane == 0) seedp[0] = (int)xf;
+    return true;
+}
+
+template <bool FIN>
+__global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *args, const int2 *items, int n_items,
+                                                           int *queue, int apc)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_item;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem); // offset 0 in every layout
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    // 16807^(lane+1) for the batched draws
+    uint32_t pw = 16807u;
+    for (int k = 0; k < (int)(threadIdx.x & 31); k++) pw = pm_mul(pw, 16807u);
+    uint32_t phase = 0;
+    for (;;) {
+        __syncthreads(); // the previous item is done with shared memory
+        if (threadIdx.x == 0) s_item = atomicAdd(queue, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const int2 code = __ldg(items + it); // {instance, first ant of the group}
+        const ConstructArgs a = args[code.x];
+        const int ant0 = code.y;
+        bool ok;
+        if (a.n <= 1024) {
+            if (a.smat) ok = a.packed ? construct_nn_item<FIN, true, true, true>(a, apc, ant0, smem, phase, pw)
+                                      : construct_nn_item<FIN, true, false, true>(a, apc, ant0, smem, phase, pw);
+            else ok = a.packed ? construct_nn_item<FIN, false, true, true>(a, apc, ant0, smem, phase, pw)
+                               : construct_nn_item<FIN, false, false, true>(a, apc, ant0, smem, phase, pw);
+        } else {
+            ok = a.packed ? construct_nn_item<FIN, false, true, false>(a, apc, ant0, smem, phase, pw)
+                          : construct_nn_item<FIN, false, false, false>(a, apc, ant0, smem, phase, pw);
+        }
+        if (!ok) break; // uniform: decided by __syncthreads_or
+        phase ^= 1u;
     }
 }
 
@@ -476,29 +499,6 @@ cudaError_t launch_parity_w(const ConstructArgs &a, int apc, bool smat, cudaStre
     return smat ? launch_parity_t<WPA, false, true>(a, apc, st) : launch_parity_t<WPA, false, false>(a, apc, st);
 }
 
-template <bool FIN, bool SMAT, bool PACKED, bool REGVIS>
-cudaError_t launch_nn_t(const ConstructArgs &a, int apc, cudaStream_t st)
-{
-    const NNLayout L = nn_layout(a.n, a.K, a.Kp, apc, SMAT, PACKED);
-    auto kern = construct_nn_kernel<FIN, SMAT, PACKED, REGVIS>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
-    if (e != cudaSuccess) return e;
-    ConstructArgs b = a;
-    b.ants_per_cta = apc;
-    const int blocks = (a.n_ants + apc - 1) / apc;
-    const int warps = apc < 8 ? 8 : apc; // helper warps share the prologue (TMA + candidate gather)
-    kern<<<blocks, warps * 32, L.bytes, st>>>(b);
-    return cudaGetLastError();
-}
-
-template <bool FIN, bool REGVIS>
-cudaError_t launch_nn_f(const ConstructArgs &a, int apc, bool smat, bool packed, cudaStream_t st)
-{
-    if (smat)
-        return packed ? launch_nn_t<FIN, true, true, REGVIS>(a, apc, st) : launch_nn_t<FIN, true, false, REGVIS>(a, apc, st);
-    return packed ? launch_nn_t<FIN, false, true, REGVIS>(a, apc, st) : launch_nn_t<FIN, false, false, REGVIS>(a, apc, st);
-}
-
 } // namespace
 
 size_t construct_parity_smem(int n, int nloc, int kmax, int wpa, int apc, bool stage_total, bool)
@@ -509,6 +509,22 @@ size_t construct_parity_smem(int n, int nloc, int kmax, int wpa, int apc, bool s
 size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool packed)
 {
     return nn_layout(n, K, Kp, apc, stage_total, packed).bytes;
+}
+
+cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue, int apc,
+                                size_t smem, int sm_count, bool finite_maxd, cudaStream_t st)
+{
+    auto kern = finite_maxd ? construct_nn_kernel<true> : construct_nn_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = (int)(228 * 1024 / (smem + 1024));
+    if (per_sm < 1) per_sm = 1;
+    int blocks = sm_count * per_sm;
+    if (blocks > n_items) blocks = n_items;
+    if (blocks < 1) blocks = 1;
+    const int warps = apc < 8 ? 8 : apc; // helper warps share the staging of each item
+    kern<<<blocks, warps * 32, smem, st>>>(d_args, d_items, n_items, d_queue, apc);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_construct_parity(const ConstructArgs &a, int wpa, int apc, bool smat, cudaStream_t st)
@@ -522,12 +538,5 @@ cudaError_t launch_construct_parity(const ConstructArgs &a, int wpa, int apc, bo
     }
 }
 
-cudaError_t launch_construct_nn(const ConstructArgs &a, int apc, bool smat, bool packed, cudaStream_t st)
-{
-    const bool fin = !(a.max_dist == __builtin_huge_valf());
-    if (a.n <= 1024)
-        return fin ? launch_nn_f<true, true>(a, apc, smat, packed, st) : launch_nn_f<false, true>(a, apc, smat, packed, st);
-    return fin ? launch_nn_f<true, false>(a, apc, smat, packed, st) : launch_nn_f<false, false>(a, apc, smat, packed, st);
-}
 
 } // namespace aco

@@ -7,7 +7,15 @@
 //   solutions              : T*(A+1)+1 int32 in the reference layout, T = 2n
 //   lens                   : A+1 fp32 (slot A = best so far)
 //   seeds                  : A*nloc int32 (one Park-Miller state per work-item lane)
-//   nn_ls_list             : n x nn_ls int32 (2-opt); nn16 : n x Kp uint16 (candidate lists)
+//   nn_ls_list             : n x nn_ls int32 (2-opt); nn16 / cand32 : n x Kp candidate
+//                            lists (uint16 node ids / node | demand << 16)
+//   chc                    : n x Kp fp32, total_info of every candidate (throughput mode),
+//                            written by the pheromone pass
+//
+// Every kernel except the parity construct reads its instance from an array of
+// argument blocks in device memory, so one launch serves one instance or a
+// batch of independent instances of different sizes (the batch is a
+// concatenation of per-instance buffers; each block holds its own pointers).
 #pragma once
 
 #include <cstdint>
@@ -29,8 +37,10 @@ struct ConstructArgs {
     const uint32_t *adv;   // nloc: 16807^(draws of lane l per step) mod m
     const uint16_t *nn16;  // n x Kp candidate lists (throughput), uint16 node ids
     const uint32_t *cand32;// n x Kp candidate lists, packed node | demand << 16
+    const float *chc;      // n x Kp total_info of the candidates
     int K, Kp;             // candidate-list length and padded row length (multiple of 8)
-    int ants_per_cta;      // throughput construct: ant warps per CTA (the CTA may have helper warps)
+    int smat;              // throughput construct: stage the whole total_info matrix
+    int packed;            // throughput construct: use cand32 (else nn16 + demand lookups)
     int *seeds;
     int *solutions;
     float *lens;
@@ -48,7 +58,7 @@ struct LocalSearchArgs {
 
 struct StatsArgs {
     int n, n_ants, T, nloc, log2_nloc, ras_ranks, record_cap;
-    int do_elites;         // 0 in the bootstrap of init_aco (g_aco.cpp:87)
+    int do_elites;         // unused on the device (passed per launch)
     int *solutions;
     float *lens;
     int *elites;           // ras_ranks
@@ -63,49 +73,53 @@ struct StatsArgs {
 };
 
 struct UpdateArgs {
-    int n, ld, q;            // q = float4 chunks per row
-    unsigned long long qinv; // ceil(2^40 / q): row = (u * qinv) >> 40
+    int n, ld;
     int ras_ranks;
     float evap;              // 1.0f - rho
-    float alpha;
-    int alpha_int;           // alpha as an integer exponent in [0, 8], or -1
+    float alpha, beta;
+    int alpha_int, beta_int; // exponents as integers in [0, 8], or -1
+    float rho;
     float *tau;
     float *total;
-    const float *heur;
+    float *heur;
+    const float *dist;
     const int *succ;
     const uint32_t *depmask;
     const float *d_tau;
+    const float *bsf_len;    // lens[A] (trail_0 = 1/(rho * bsf))
+    float *chc;              // n x Kp, or null (no candidate table)
+    const uint16_t *nn16;    // n x Kp
+    int K, Kp;
 };
 
-struct InitArgs {
-    int n, ld;
-    float trail;             // used when from_bsf == 0
-    int from_bsf;            // trail = 1/(rho * lens[A]) (g_aco.cpp:89)
-    float rho, alpha;
-    int alpha_int;
-    const float *bsf_len;
-    float *tau;
-    float *total;
-    const float *heur;
-};
+// Per-row pass modes of the row kernel.
+enum RowMode { ROW_HEUR = 0, ROW_INIT_TRAIL = 1, ROW_INIT_BSF = 2, ROW_UPDATE = 3, ROW_GATHER = 4 };
 
-// Launchers (stream-ordered; return cudaGetLastError()).
-cudaError_t launch_heur(const float *dist, float *heur, int n, int ld, float beta, int beta_int, cudaStream_t st);
-cudaError_t launch_pheromone_init(const InitArgs &a, cudaStream_t st);
+// Launchers (stream-ordered; return cudaGetLastError()).  `d_*args` point to
+// arrays of argument blocks in device memory, one per instance.
 cudaError_t launch_construct_parity(const ConstructArgs &a, int warps_per_ant, int ants_per_block, bool stage_total,
                                     cudaStream_t st);
-cudaError_t launch_construct_nn(const ConstructArgs &a, int ants_per_block, bool stage_total, bool packed,
-                                cudaStream_t st);
-cudaError_t launch_local_search(const LocalSearchArgs &a, int ants_per_block, bool stage_nn, cudaStream_t st);
-cudaError_t launch_stats(const StatsArgs &a, cudaStream_t st);
-cudaError_t launch_pheromone_update(const UpdateArgs &a, int sm_count, cudaStream_t st);
+// Throughput construct, persistent: CTAs pull work items {instance, first ant}
+// from *d_queue (reset to 0 by the caller before the launch).
+cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue,
+                                int ants_per_cta, size_t smem, int sm_count, bool finite_maxd, cudaStream_t st);
+// 2-opt: one CTA of `warps` warps per ant; d_ant_inst[g] = instance of global ant g,
+// d_ant_base[b] = first global ant of instance b.
+cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
+                                int total_ants, int warps, size_t smem, cudaStream_t st);
+cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st);
+// Row passes (heuristic matrix, pheromone init, fused update, candidate gather):
+// one warp per row over all instances; d_row_base[b] = first global row of instance b.
+cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, int n_inst, int total_rows, int mode,
+                        float trail, int ld_max, int sm_count, cudaStream_t st);
 cudaError_t launch_t0(unsigned long long *t0, cudaStream_t st);
 
-// Shared-memory bytes the launchers request (the host picks configurations
-// that fit the 227 KB per-CTA limit).
+// Shared-memory bytes of the launches (the host picks configurations that fit
+// the 227 KB per-CTA limit).
 size_t construct_parity_smem(int n, int nloc, int kmax, int warps_per_ant, int ants_per_block, bool stage_total,
                              bool finite_maxd);
-size_t construct_nn_smem(int n, int K, int Kp, int ants_per_block, bool stage_total, bool packed);
-size_t local_search_smem(int n, int nn_ls, int rmax, int ants_per_block, bool stage_nn);
+size_t construct_nn_smem(int n, int K, int Kp, int ants_per_cta, bool stage_total, bool packed);
+size_t local_search_smem(int n, int warps);
+size_t rows_smem(int ld_max);
 
 } // namespace aco

@@ -323,9 +323,13 @@ __device__ int two_opt_route_generic(Route &c, int pass_limit)
     return ACO_OK;
 }
 
-__global__ void __launch_bounds__(1024) local_search_kernel(LocalSearchArgs a)
+__global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArgs *args, const int *ant_inst,
+                                                             const int *ant_base)
 {
     extern __shared__ __align__(128) unsigned char smem[];
+    const int b = __ldg(ant_inst + blockIdx.x);
+    const LocalSearchArgs a = args[b];
+    const int ant = blockIdx.x - __ldg(ant_base + b);
     const int n = a.n, T = a.T;
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -343,7 +347,6 @@ __global__ void __launch_bounds__(1024) local_search_kernel(LocalSearchArgs a)
     uint16_t *rnode = reinterpret_cast<uint16_t *>(smem + L.rnodes) + (size_t)warp * kRL;
     __shared__ int s_routes, s_next;
 
-    const int ant = blockIdx.x;
     int *gtour = a.solutions + (size_t)ant * T;
     const int size = gtour[T - 1];
     if (size < 2) return; // a failed construction has nothing to improve (uniform over the CTA)
@@ -452,17 +455,14 @@ __global__ void __launch_bounds__(1024) local_search_kernel(LocalSearchArgs a)
 
 } // namespace
 
-size_t local_search_smem(int n, int /*nn_ls*/, int /*rmax*/, int warps, bool /*stage_nn*/)
-{
-    return ls_layout(n, 2 * n, warps).bytes;
-}
+size_t local_search_smem(int n, int warps) { return ls_layout(n, 2 * n, warps).bytes; }
 
-cudaError_t launch_local_search(const LocalSearchArgs &a, int warps, bool /*stage_nn*/, cudaStream_t st)
+cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
+                                int total_ants, int warps, size_t smem, cudaStream_t st)
 {
-    const size_t bytes = ls_layout(a.n, a.T, warps).bytes;
-    cudaError_t e = cudaFuncSetAttribute(local_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaError_t e = cudaFuncSetAttribute(local_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    local_search_kernel<<<a.n_ants, warps * 32, bytes, st>>>(a);
+    local_search_kernel<<<total_ants, warps * 32, smem, st>>>(d_args, d_ant_inst, d_ant_base);
     return cudaGetLastError();
 }
 

@@ -66,7 +66,7 @@ typedef struct aco_instance {
 /* Parameters: set_default_parameters (problem.cpp:186-220) plus the values the
  * reference hard-codes or takes from the clock. */
 typedef struct aco_params {
-    int n_ants;           /* n_ants (default n, problem.cpp:189) */
+    int n_ants;           /* n_ants (default n, problem.cpp:189); at most 57344 */
     float alpha;          /* 1.0 (kernel.cl:10, problem.cpp:207) */
     float beta;           /* 2.0 (kernel.cl:11) */
     float rho;            /* 0.1 (kernel.cl:9) */
@@ -187,6 +187,29 @@ int aco_time_phases(aco_solver *s, int n_iter, float *ms4);
  * construct, and whether matrices are staged in shared memory (bit 0: total_info
  * in construct, bit 1: NN lists in 2-opt). */
 int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *staging_flags);
+
+/* ---- batches: many independent instances in the same launches --------------
+ * No reference counterpart (the reference solves one instance per process).
+ * ACO_MODE_THROUGHPUT only; every instance has n <= 1024 nodes and its own
+ * device state (pheromone, tours, best-so-far, records); instance b uses the
+ * seeds of rnd_seed + b.  Lists deeper than an instance allows are clamped to
+ * n-2 for it.  One iteration is four launches for the whole batch: a persistent
+ * construct kernel over a device work queue of (instance, ant group) items,
+ * 2-opt (one CTA per ant), statistics (one CTA per instance) and the row pass
+ * over every instance's matrices; replayed as one CUDA graph. */
+typedef struct aco_batch aco_batch;
+int aco_batch_create(const aco_instance *insts, int count, const aco_params *params, aco_batch **out);
+int aco_batch_init(aco_batch *b);
+int aco_batch_iterate(aco_batch *b, int n_iter);
+int aco_batch_enqueue_iterations(aco_batch *b, int n_iter);
+int aco_batch_status(aco_batch *b);
+int aco_batch_size(aco_batch *b, int *count, int *total_ants);
+int aco_batch_get_best(aco_batch *b, int idx, int *tour, int cap, int *tour_size, float *length);
+int aco_batch_get_solutions(aco_batch *b, int idx, int *solutions, size_t cap_ints, float *lens, size_t cap_lens);
+int aco_batch_get_pheromone(aco_batch *b, int idx, float *tau, float *total_info, size_t cap);
+int aco_batch_time_phases(aco_batch *b, int n_iter, float *ms4);
+void *aco_batch_get_stream(aco_batch *b);
+void aco_batch_destroy(aco_batch *b);
 
 /* ---- pheromone update without allocation ---------------------------------
  * No counterpart in the reference.  For callers that cannot let this library
