@@ -36,6 +36,8 @@ sys.path.insert(0, ROOT)
 
 N_CUST, ANTS, NN_ANTS, NN_LS, NLOC = 200, 200, 25, 25, 256
 SEED_INSTANCE, SEED_TIME, RND_SEED = 2026, 1796300000, 4242
+BATCH_COUNT, BATCH_ANTS, BATCH_SEED = 512, 128, 512
+KERNELS = ["construct_nn_kernel", "local_search_kernel", "stats_kernel", "rows_kernel"]
 METRIC = "ant-tours/sec (construct+2-opt+update)"
 UNIT = "ant-tours/s"
 WORKLOAD = ("single CVRP instance, 200 customers (50% uniform, 50% 8 Gaussian clusters), 200 ants, "
@@ -194,7 +196,7 @@ def run_ours(args, ws, rank, local):
 
     # per-kernel shares (device time, phase by phase, same workload and stream)
     phase_ms = S.time_phases(max(5, args.steps // 2))
-    names = ["construct_nn_kernel", "local_search_kernel", "stats_kernel", "pheromone_update_kernel"]
+    names = KERNELS
     share = phase_ms / phase_ms.sum()
     dom = int(np.argmax(phase_ms))
     n_phase = max(5, args.steps // 2)
@@ -210,7 +212,7 @@ def run_ours(args, ws, rank, local):
         "construct_nn_kernel": ANTS * steps_per_tour * NN_ANTS * 12,   # neighbour id + choice_info + distance
         "local_search_kernel": ANTS * 2 * (2 * n) * 4 * 4,              # tour read/write + edge lengths, 4 B each
         "stats_kernel": (ANTS + 1) * 4 + 6 * (2 * n) * 4,
-        "pheromone_update_kernel": 16 * n * n,                        # read tau, heur; write tau, total
+        "rows_kernel": 16 * n * n,                                     # read tau, heur; write tau, total
     }
     peak, peak_kind = load_peaks()
     dk = names[dom]
@@ -230,9 +232,11 @@ def run_ours(args, ws, rank, local):
                    "mode": "throughput", "ras_ranks": 6, "parallelism": f"replicas x{ws}",
                    "l2": "flushed before every timed iteration (256 MiB write)", "instance_seed": SEED_INSTANCE},
         "clocks": clk.summary(), "roofline": roofline,
-        "gpu_launches": args.steps * 4,
+        "gpu_launches": args.steps * 4,  # construct, 2-opt, statistics, row pass per iteration
         "best_length": float(best_len),
     }
+    if not args.no_batched:
+        result["batched"] = run_batched(args, ws, rank, local, peak, peak_kind)
     # end to end through the public API with host buffers
     if rank == 0 or ws > 1:
         result["e2e"] = run_e2e(args, rank, local)
@@ -247,6 +251,76 @@ def run_ours(args, ws, rank, local):
         if ws == 1 and not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(seconds=args.cpu_seconds)
         print(json.dumps(result, default=float))
+
+
+def run_batched(args, ws, rank, local, peak, peak_kind):
+    """Batched workload: BATCH_COUNT independent instances, customer count
+    uniform in [100, 1000] (mixed and large generators alternately), 128 ants
+    each, all served by the same four launches per iteration.  Instances are
+    sharded over ranks (rank r takes every ws-th instance; no collective).
+    Reports ant-tours/s over the whole batch and the roofline of the fused
+    pheromone pass, whose matrices (16 bytes per element over all instances)
+    far exceed L2."""
+    import torch
+    from cvrp_aco_ocl_b200 import MODE_THROUGHPUT, Batch, Problem, default_params
+    from cvrp_aco_ocl_b200 import instances as I
+
+    insts = I.gen_batch(BATCH_SEED, BATCH_COUNT, 100, 1000)[rank::ws]
+    probs = [Problem.from_instance(x) for x in insts]
+    p = default_params(1001)
+    p.mode, p.n_ants, p.nn_ants, p.nn_ls, p.nloc = MODE_THROUGHPUT, BATCH_ANTS, NN_ANTS, NN_LS, NLOC
+    p.seed_time, p.rnd_seed, p.device, p.ls_flag = SEED_TIME, RND_SEED, local, 1
+    t0 = time.perf_counter()
+    B = Batch(probs, p)
+    B.init()
+    t_setup = time.perf_counter() - t0
+    count, total_ants = B.size()
+    for _ in range(max(3, args.batch_warmup)):
+        B.enqueue(1)
+    if B.status() != 0:
+        raise RuntimeError("batched warm-up failed")
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.ExternalStream(B.stream(), device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.batch_steps)]
+    torch.cuda.synchronize()
+    for e0, e1 in evs:  # inputs (about 3 GB of matrices) exceed L2: no flush needed
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        B.enqueue(1)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+    torch.cuda.synchronize()
+    if B.status() != 0:
+        raise RuntimeError("batched run failed")
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    tot = torch.tensor([float(total_ants)], device=dev, dtype=torch.float64)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    ms_max = float(t.item())
+    phase = B.time_phases(args.batch_steps)
+    B.close()
+    n_all = [pr.num_node for pr in probs]
+    row_bytes = sum(16 * n * n for n in n_all)
+    row_ms = float(phase[3]) / args.batch_steps
+    achieved = row_bytes / (row_ms / 1e3) / 1e9
+    return {
+        "workload": f"{BATCH_COUNT} independent instances, 100-1000 customers (seeded, mixed/large generators), "
+                    f"{BATCH_ANTS} ants each, {NN_ANTS}-NN lists, 2-opt on {NN_LS}-NN lists",
+        "value": float(tot.item()) * args.batch_steps / (ms_max / 1e3), "unit": UNIT,
+        "ms_per_step": ms_max / args.batch_steps, "steps": args.batch_steps, "instances_this_rank": count,
+        "ants_this_rank": total_ants, "setup_s": t_setup,
+        "gpu_launches": args.batch_steps * 4,
+        "kernel_share": {k: float(v) for k, v in zip(KERNELS, phase / phase.sum())},
+        "roofline": {"bound": "hbm", "kernel": "rows_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": profile_traffic("rows_kernel@batch"),
+                     "algorithmic_bytes_per_launch": row_bytes, "launch_ms": row_ms,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                     "fallback 6.65 TB/s"},
+    }
 
 
 def run_e2e(args, rank, local):
@@ -341,6 +415,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload section")
+    ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--batch-warmup", type=int, default=3)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     ws, rank, local = dist_env()

@@ -390,7 +390,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
 
 int Colony::run_rows(int mode, float trail)
 {
-    CK(launch_rows(uargs_d_, row_base_d_, (int)inst.size(), total_rows, mode, trail, ld_max, sm_count, st));
+    CK(launch_rows(uargs_d_, row_base_d_, (int)inst.size(), total_rows, mode, trail, sm_count, st));
     return ACO_OK;
 }
 

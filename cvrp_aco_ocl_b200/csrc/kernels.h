@@ -111,7 +111,7 @@ cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, siz
 // Row passes (heuristic matrix, pheromone init, fused update, candidate gather):
 // one warp per row over all instances; d_row_base[b] = first global row of instance b.
 cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, int n_inst, int total_rows, int mode,
-                        float trail, int ld_max, int sm_count, cudaStream_t st);
+                        float trail, int sm_count, cudaStream_t st);
 cudaError_t launch_t0(unsigned long long *t0, cudaStream_t st);
 
 // Shared-memory bytes of the launches (the host picks configurations that fit
@@ -120,6 +120,5 @@ size_t construct_parity_smem(int n, int nloc, int kmax, int warps_per_ant, int a
                              bool finite_maxd);
 size_t construct_nn_smem(int n, int K, int Kp, int ants_per_cta, bool stage_total, bool packed);
 size_t local_search_smem(int n, int warps);
-size_t rows_smem(int ld_max);
 
 } // namespace aco

@@ -13,8 +13,9 @@
 // compute_total_info (:782-789) as one pass: one warp per matrix row, float4
 // loads and stores; it reads tau and heur (= eta^beta, precomputed once) and
 // writes tau and total_info -- 16 bytes of HBM traffic per element -- and, in
-// throughput mode, the total_info of the row's candidates (staged in shared
-// memory) into the compact candidate table the construct kernel loads by TMA.
+// throughput mode, the total_info of the row's candidates (re-read from L2
+// after the row is written) into the compact candidate table the construct
+// kernel loads by TMA.
 #include <cuda_runtime.h>
 
 #include "aco_device.cuh"
@@ -140,22 +141,142 @@ __global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, int 
     if (tid == 0) *a.iteration = iter + 1; // main.cpp:86 (Problem::iteration++)
 }
 
+// Deposit of elite ranks into one float4 of row i (columns c4..c4+3), in
+// elite order 0, 1, ..., R-1 -- the order the oracle applies the deposit in.
+__device__ __forceinline__ void deposit4(const UpdateArgs &a, int i, int c4, const int (&sr)[8], const float (&dr)[8],
+                                         float &v0, float &v1, float &v2, float &v3)
+{
+    const int R = a.ras_ranks, n = a.n;
+    if (i != 0) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const unsigned d = (unsigned)(sr[r] - c4);
+            if (r < R && d < 4u) {
+                if (d == 0) v0 = __fadd_rn(v0, dr[r]);
+                else if (d == 1) v1 = __fadd_rn(v1, dr[r]);
+                else if (d == 2) v2 = __fadd_rn(v2, dr[r]);
+                else v3 = __fadd_rn(v3, dr[r]);
+            }
+        }
+        for (int r = 8; r < R; r++) { // more than 8 ranks: read the rest directly
+            const unsigned d = (unsigned)(__ldg(a.succ + (size_t)r * n + i) - c4);
+            if (d < 4u) {
+                const float dt = __ldg(a.d_tau + r);
+                if (d == 0) v0 = __fadd_rn(v0, dt);
+                else if (d == 1) v1 = __fadd_rn(v1, dt);
+                else if (d == 2) v2 = __fadd_rn(v2, dt);
+                else v3 = __fadd_rn(v3, dt);
+            }
+        }
+    } else { // depot row: depot -> customer edges from the per-column masks
+        const uint32_t m0 = c4 + 0 < n ? __ldg(a.depmask + c4 + 0) : 0u;
+        const uint32_t m1 = c4 + 1 < n ? __ldg(a.depmask + c4 + 1) : 0u;
+        const uint32_t m2 = c4 + 2 < n ? __ldg(a.depmask + c4 + 2) : 0u;
+        const uint32_t m3 = c4 + 3 < n ? __ldg(a.depmask + c4 + 3) : 0u;
+        for (int r = 0; r < R; r++) {
+            const float dt = __ldg(a.d_tau + r);
+            if ((m0 >> r) & 1u) v0 = __fadd_rn(v0, dt);
+            if ((m1 >> r) & 1u) v1 = __fadd_rn(v1, dt);
+            if ((m2 >> r) & 1u) v2 = __fadd_rn(v2, dt);
+            if ((m3 >> r) & 1u) v3 = __fadd_rn(v3, dt);
+        }
+    }
+}
+
+// Float4 per lane per chunk of the evaporation pass: every load of a chunk is
+// issued before its arithmetic, so a lane keeps four float4 of each input
+// matrix in flight.
+constexpr int kU = 4;
+
+// Evaporation + total_info over one customer row, U float4 per lane per chunk
+// (A1: alpha == 1, so tau^alpha is tau itself).  The deposit columns are fixed
+// up afterwards (row_pass).
+template <int U, bool A1>
+__device__ __forceinline__ void evaporate_row(const UpdateArgs &a, int lane, int q4, float4 *tau4,
+                                              const float4 *heur4, float4 *tot4)
+{
+    const float evap = a.evap;
+    float4 *tp = tau4 + lane, *op = tot4 + lane;
+    const float4 *hp = heur4 + lane;
+    for (int left = q4 - lane; left > 0; left -= 32 * U, tp += 32 * U, op += 32 * U, hp += 32 * U) {
+        float4 t[U], h[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (32 * u < left) {
+                t[u] = __ldcs(tp + 32 * u); // read once per pass: evict first
+                h[u] = __ldcs(hp + 32 * u);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (32 * u < left) {
+                float4 o, tot;
+                o.x = __fmul_rn(evap, t[u].x);
+                o.y = __fmul_rn(evap, t[u].y);
+                o.z = __fmul_rn(evap, t[u].z);
+                o.w = __fmul_rn(evap, t[u].w);
+                if (A1) {
+                    tot.x = __fmul_rn(o.x, h[u].x);
+                    tot.y = __fmul_rn(o.y, h[u].y);
+                    tot.z = __fmul_rn(o.z, h[u].z);
+                    tot.w = __fmul_rn(o.w, h[u].w);
+                } else {
+                    tot.x = __fmul_rn(pow_rule(o.x, a.alpha, a.alpha_int), h[u].x);
+                    tot.y = __fmul_rn(pow_rule(o.y, a.alpha, a.alpha_int), h[u].y);
+                    tot.z = __fmul_rn(pow_rule(o.z, a.alpha, a.alpha_int), h[u].z);
+                    tot.w = __fmul_rn(pow_rule(o.w, a.alpha, a.alpha_int), h[u].w);
+                }
+                tp[32 * u] = o;
+                op[32 * u] = tot;
+            }
+        }
+    }
+}
+
+// Depot row: every column may receive deposits (depot -> customer edges of
+// every route of every elite), so each float4 takes the mask check.
+__device__ __forceinline__ void update_depot_row(const UpdateArgs &a, int lane, int q4, float4 *tau4,
+                                                 const float4 *heur4, float4 *tot4)
+{
+    const int sr[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+    const float dr[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int q = lane; q < q4; q += 32) {
+        const float4 t = tau4[q], h = heur4[q];
+        float v0 = __fmul_rn(a.evap, t.x), v1 = __fmul_rn(a.evap, t.y);
+        float v2 = __fmul_rn(a.evap, t.z), v3 = __fmul_rn(a.evap, t.w);
+        deposit4(a, 0, 4 * q, sr, dr, v0, v1, v2, v3);
+        float4 o, tot;
+        o.x = v0; o.y = v1; o.z = v2; o.w = v3;
+        tot.x = __fmul_rn(pow_rule(v0, a.alpha, a.alpha_int), h.x);
+        tot.y = __fmul_rn(pow_rule(v1, a.alpha, a.alpha_int), h.y);
+        tot.z = __fmul_rn(pow_rule(v2, a.alpha, a.alpha_int), h.z);
+        tot.w = __fmul_rn(pow_rule(v3, a.alpha, a.alpha_int), h.w);
+        tau4[q] = o;
+        tot4[q] = tot;
+    }
+}
+
 // One warp, row i of instance a.  Columns are walked as float4 (ld is a
-// multiple of 32); columns n..ld-1 stay zero.
-__device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, float trail, float *srow, int lane)
+// multiple of 32; columns n..ld-1 stay zero).
+__device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, float trail, int lane)
 {
     const int n = a.n, q4 = (n + 3) >> 2;
     const size_t off = (size_t)i * a.ld;
+    const float4 *heur4 = reinterpret_cast<const float4 *>(a.heur + off);
+    float4 *tau4 = reinterpret_cast<float4 *>(a.tau + off);
+    float4 *tot4 = reinterpret_cast<float4 *>(a.total + off);
     if (mode == ROW_HEUR) {
+        const float4 *dist4 = reinterpret_cast<const float4 *>(a.dist + off);
+        float4 *h4 = reinterpret_cast<float4 *>(a.heur + off);
         for (int q = lane; q < q4; q += 32) {
-            const float4 d = *reinterpret_cast<const float4 *>(a.dist + off + 4 * q);
+            const float4 d = dist4[q];
             const int c = 4 * q;
             float4 h;
             h.x = c + 0 < n ? pow_rule(__fdiv_rn(1.0f, __fadd_rn(d.x, 0.1f)), a.beta, a.beta_int) : 0.f;
             h.y = c + 1 < n ? pow_rule(__fdiv_rn(1.0f, __fadd_rn(d.y, 0.1f)), a.beta, a.beta_int) : 0.f;
             h.z = c + 2 < n ? pow_rule(__fdiv_rn(1.0f, __fadd_rn(d.z, 0.1f)), a.beta, a.beta_int) : 0.f;
             h.w = c + 3 < n ? pow_rule(__fdiv_rn(1.0f, __fadd_rn(d.w, 0.1f)), a.beta, a.beta_int) : 0.f;
-            *reinterpret_cast<float4 *>(a.heur + off + 4 * q) = h;
+            h4[q] = h;
         }
         return;
     }
@@ -163,102 +284,55 @@ __device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, f
         const float tr = mode == ROW_INIT_BSF ? __fdiv_rn(1.0f, __fmul_rn(a.rho, *a.bsf_len)) : trail;
         const float pa = pow_rule(tr, a.alpha, a.alpha_int);
         for (int q = lane; q < q4; q += 32) {
-            const float4 h = *reinterpret_cast<const float4 *>(a.heur + off + 4 * q);
+            const float4 h = heur4[q];
             const int c = 4 * q;
             float4 t, o;
             t.x = c + 0 < n ? tr : 0.f; o.x = c + 0 < n ? __fmul_rn(pa, h.x) : 0.f;
             t.y = c + 1 < n ? tr : 0.f; o.y = c + 1 < n ? __fmul_rn(pa, h.y) : 0.f;
             t.z = c + 2 < n ? tr : 0.f; o.z = c + 2 < n ? __fmul_rn(pa, h.z) : 0.f;
             t.w = c + 3 < n ? tr : 0.f; o.w = c + 3 < n ? __fmul_rn(pa, h.w) : 0.f;
-            *reinterpret_cast<float4 *>(a.tau + off + 4 * q) = t;
-            *reinterpret_cast<float4 *>(a.total + off + 4 * q) = o;
-            if (a.chc) *reinterpret_cast<float4 *>(srow + 4 * q) = o;
+            tau4[q] = t;
+            tot4[q] = o;
         }
     } else if (mode == ROW_UPDATE) {
-        // deposit columns of this row: the successor of customer i in each elite
-        // tour, read once and broadcast (elite order kept when adding)
-        const int R = a.ras_ranks;
-        int mys = -1;
-        float myd = 0.f;
-        if (lane < R && i != 0) {
-            mys = __ldg(a.succ + (size_t)lane * n + i);
-            myd = __ldg(a.d_tau + lane);
-        }
-        int sr[8];
-        float dr[8];
-#pragma unroll
-        for (int r = 0; r < 8; r++) {
-            sr[r] = __shfl_sync(FULL, mys, r);
-            dr[r] = __shfl_sync(FULL, myd, r);
-        }
-        for (int q = lane; q < q4; q += 32) {
-            const float4 t = *reinterpret_cast<const float4 *>(a.tau + off + 4 * q);
-            const float4 h = __ldg(reinterpret_cast<const float4 *>(a.heur + off + 4 * q));
-            float v0 = __fmul_rn(a.evap, t.x), v1 = __fmul_rn(a.evap, t.y);
-            float v2 = __fmul_rn(a.evap, t.z), v3 = __fmul_rn(a.evap, t.w);
-            const int c4 = 4 * q;
-            if (i != 0) {
-#pragma unroll
-                for (int r = 0; r < 8; r++) {
-                    const unsigned d = (unsigned)(sr[r] - c4);
-                    if (r < R && d < 4u) {
-                        if (d == 0) v0 = __fadd_rn(v0, dr[r]);
-                        else if (d == 1) v1 = __fadd_rn(v1, dr[r]);
-                        else if (d == 2) v2 = __fadd_rn(v2, dr[r]);
-                        else v3 = __fadd_rn(v3, dr[r]);
-                    }
-                }
-                for (int r = 8; r < R; r++) { // more than 8 ranks: read the rest directly
-                    const unsigned d = (unsigned)(__ldg(a.succ + (size_t)r * n + i) - c4);
-                    if (d < 4u) {
-                        const float dt = __ldg(a.d_tau + r);
-                        if (d == 0) v0 = __fadd_rn(v0, dt);
-                        else if (d == 1) v1 = __fadd_rn(v1, dt);
-                        else if (d == 2) v2 = __fadd_rn(v2, dt);
-                        else v3 = __fadd_rn(v3, dt);
-                    }
-                }
-            } else { // depot row: depot -> customer edges from the per-column masks
-                const uint32_t m0 = c4 + 0 < n ? __ldg(a.depmask + c4 + 0) : 0u;
-                const uint32_t m1 = c4 + 1 < n ? __ldg(a.depmask + c4 + 1) : 0u;
-                const uint32_t m2 = c4 + 2 < n ? __ldg(a.depmask + c4 + 2) : 0u;
-                const uint32_t m3 = c4 + 3 < n ? __ldg(a.depmask + c4 + 3) : 0u;
-                for (int r = 0; r < R; r++) {
-                    const float dt = __ldg(a.d_tau + r);
-                    if ((m0 >> r) & 1u) v0 = __fadd_rn(v0, dt);
-                    if ((m1 >> r) & 1u) v1 = __fadd_rn(v1, dt);
-                    if ((m2 >> r) & 1u) v2 = __fadd_rn(v2, dt);
-                    if ((m3 >> r) & 1u) v3 = __fadd_rn(v3, dt);
-                }
+        if (i == 0) {
+            update_depot_row(a, lane, q4, tau4, heur4, tot4);
+        } else {
+            if (a.alpha_int == 1) evaporate_row<kU, true>(a, lane, q4, tau4, heur4, tot4);
+            else evaporate_row<1, false>(a, lane, q4, tau4, heur4, tot4);
+            // deposit (kernel.cl:747-776): lane r < R owns the successor of
+            // customer i in elite r's tour.  It re-reads the evaporated value
+            // this warp just wrote and adds every elite's deposit on that edge
+            // in elite order, so lanes of elites sharing the edge write the same
+            // value; total_info of the column is recomputed from the result.
+            const int R = a.ras_ranks;
+            int c = -1;
+            if (lane < R) c = __ldg(a.succ + (size_t)lane * n + i);
+            __syncwarp();
+            if (c >= 0) {
+                float v = a.tau[off + c];
+                for (int r = 0; r < R; r++)
+                    if (__ldg(a.succ + (size_t)r * n + i) == c) v = __fadd_rn(v, __ldg(a.d_tau + r));
+                a.total[off + c] = __fmul_rn(pow_rule(v, a.alpha, a.alpha_int), a.heur[off + c]);
+                a.tau[off + c] = v;
             }
-            float4 o, tot;
-            o.x = v0; o.y = v1; o.z = v2; o.w = v3;
-            tot.x = __fmul_rn(pow_rule(v0, a.alpha, a.alpha_int), h.x);
-            tot.y = __fmul_rn(pow_rule(v1, a.alpha, a.alpha_int), h.y);
-            tot.z = __fmul_rn(pow_rule(v2, a.alpha, a.alpha_int), h.z);
-            tot.w = __fmul_rn(pow_rule(v3, a.alpha, a.alpha_int), h.w);
-            *reinterpret_cast<float4 *>(a.tau + off + 4 * q) = o;
-            *reinterpret_cast<float4 *>(a.total + off + 4 * q) = tot;
-            if (a.chc) *reinterpret_cast<float4 *>(srow + 4 * q) = tot;
         }
-    } else if (mode == ROW_GATHER) {
-        if (a.chc)
-            for (int q = lane; q < q4; q += 32)
-                *reinterpret_cast<float4 *>(srow + 4 * q) = *reinterpret_cast<const float4 *>(a.total + off + 4 * q);
     }
     if (a.chc) { // compact candidate table: chc[i][j] = total[i][nn[i][j]]
+        // the row was written by this warp; __syncwarp orders those stores before
+        // the re-reads below (they hit L2, the lines were just written)
         __syncwarp();
-        for (int j = lane; j < a.K; j += 32) a.chc[(size_t)i * a.Kp + j] = srow[a.nn16[(size_t)i * a.Kp + j]];
-        __syncwarp();
+        for (int j = lane; j < a.K; j += 32)
+            a.chc[(size_t)i * a.Kp + j] = a.total[off + a.nn16[(size_t)i * a.Kp + j]];
     }
 }
 
-__global__ void __launch_bounds__(256) rows_kernel(const UpdateArgs *args, const int *row_base, int n_inst,
-                                                   int total_rows, int mode, float trail, int ld_max)
+template <int MODE>
+__global__ void __launch_bounds__(256, 4) rows_kernel(const UpdateArgs *args, const int *row_base, int n_inst,
+                                                      int total_rows, float trail)
 {
-    extern __shared__ __align__(16) float s_rows[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    float *srow = s_rows + (size_t)wib * ld_max;
+    constexpr int mode = MODE;
+    const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     int b = 0;
@@ -272,7 +346,7 @@ __global__ void __launch_bounds__(256) rows_kernel(const UpdateArgs *args, const
             }
             b = lo;
         }
-        row_pass(args[b], g - __ldg(row_base + b), mode, trail, srow, lane);
+        row_pass(args[b], g - __ldg(row_base + b), mode, trail, lane);
     }
 }
 
@@ -290,21 +364,26 @@ cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, siz
     return cudaGetLastError();
 }
 
-size_t rows_smem(int ld_max) { return (size_t)8 * ld_max * sizeof(float); }
-
 cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, int n_inst, int total_rows, int mode,
-                        float trail, int ld_max, int sm_count, cudaStream_t st)
+                        float trail, int sm_count, cudaStream_t st)
 {
-    const size_t smem = rows_smem(ld_max);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
     int blocks = (total_rows + 7) / 8; // 8 warps (rows) per CTA
-    const int cap = sm_count * 8;      // grid-stride beyond 8 CTAs per SM
+    const int cap = sm_count * 4;      // grid-stride beyond 4 CTAs (32 warps) per SM
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    rows_kernel<<<blocks, 256, smem, st>>>(d_args, d_row_base, n_inst, total_rows, mode, trail, ld_max);
+    switch (mode) {
+    case ROW_HEUR: rows_kernel<ROW_HEUR><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail); break;
+    case ROW_INIT_TRAIL:
+        rows_kernel<ROW_INIT_TRAIL><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        break;
+    case ROW_INIT_BSF:
+        rows_kernel<ROW_INIT_BSF><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        break;
+    case ROW_UPDATE:
+        rows_kernel<ROW_UPDATE><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        break;
+    default: rows_kernel<ROW_GATHER><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail); break;
+    }
     return cudaGetLastError();
 }
 

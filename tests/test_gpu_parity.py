@@ -254,3 +254,28 @@ def test_two_solvers_independent(gpu):
         S1.iterate(1); S2.iterate(2); O1.run_iteration(); O2.run_iteration(); O2.run_iteration()
         compare_state(S1, O1)
         compare_state(S2, O2)
+
+
+@pytest.mark.parametrize("mode", [MODE_PARITY, MODE_THROUGHPUT])
+def test_integer_exponents_and_many_ranks(gpu, mode):
+    """alpha=2, beta=3, rho=0.2 and 10 elite ranks: the general exponent path of
+    the row pass and the deposit of ranks beyond the eighth."""
+    inst = I.gen_mixed(61, 150)
+    n, A, nloc, T0, rs0 = inst.n, 48, 256, 1796300000, 313
+    prob = problem_of(inst.x, inst.y, inst.demand, inst.capacity)
+    p = params_for(n, A, nloc, T0, rs0, True, 20, mode=mode, alpha=2.0, beta=3.0, rho=0.2, ras_ranks=10)
+    if mode == MODE_THROUGHPUT:
+        p.nn_ants = 20
+    dist = oracle.compute_distances(inst.x, inst.y)
+    nn = oracle.compute_nn_lists(dist, 20, 20)
+    seeds, _ = oracle.make_seeds(T0, rs0, A, nloc)
+    O = oracle.Oracle(dist, inst.demand, inst.capacity, A, nloc, nn, seeds, ls_flag=True, alpha=2.0, beta=3.0,
+                      rho=0.2, ras_ranks=10, nn_ants_list=nn if mode == MODE_THROUGHPUT else None, n_threads=8)
+    thr = mode == MODE_THROUGHPUT
+    with Solver(prob, p) as S:
+        S.init(); O.init_aco(throughput=thr)
+        compare_state(S, O)
+        for _ in range(3):
+            S.iterate(1); O.run_iteration(throughput=thr)
+            compare_state(S, O)
+        assert np.array_equal(S.elites(), O.elites)
