@@ -265,7 +265,8 @@ def run_batched(args, ws, rank, local, peak, peak_kind):
     from cvrp_aco_ocl_b200 import MODE_THROUGHPUT, Batch, Problem, default_params
     from cvrp_aco_ocl_b200 import instances as I
 
-    insts = I.gen_batch(BATCH_SEED, BATCH_COUNT, 100, 1000)[rank::ws]
+    count_all = args.batch_count
+    insts = I.gen_batch(BATCH_SEED, count_all, 100, 1000)[rank::ws]
     probs = [Problem.from_instance(x) for x in insts]
     p = default_params(1001)
     p.mode, p.n_ants, p.nn_ants, p.nn_ls, p.nloc = MODE_THROUGHPUT, BATCH_ANTS, NN_ANTS, NN_LS, NLOC
@@ -308,7 +309,7 @@ def run_batched(args, ws, rank, local, peak, peak_kind):
     row_ms = float(phase[3]) / args.batch_steps
     achieved = row_bytes / (row_ms / 1e3) / 1e9
     return {
-        "workload": f"{BATCH_COUNT} independent instances, 100-1000 customers (seeded, mixed/large generators), "
+        "workload": f"{count_all} independent instances, 100-1000 customers (seeded, mixed/large generators), "
                     f"{BATCH_ANTS} ants each, {NN_ANTS}-NN lists, 2-opt on {NN_LS}-NN lists",
         "value": float(tot.item()) * args.batch_steps / (ms_max / 1e3), "unit": UNIT,
         "ms_per_step": ms_max / args.batch_steps, "steps": args.batch_steps, "instances_this_rank": count,
@@ -417,12 +418,23 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload section")
     ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--batch-count", type=int, default=BATCH_COUNT,
+                    help="instances of the batched section (smaller counts for profiling captures)")
+    ap.add_argument("--only-batched", action="store_true",
+                    help="run the batched section alone and print it as the line")
     ap.add_argument("--batch-warmup", type=int, default=3)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     ws, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, ws, rank)
+        return
+    if args.only_batched:
+        import torch
+        torch.cuda.set_device(local)
+        peak, peak_kind = load_peaks()
+        line = run_batched(args, 1, 0, local, peak, peak_kind)
+        print(json.dumps(line, default=float))
         return
     run_ours(args, ws, rank, local)
 

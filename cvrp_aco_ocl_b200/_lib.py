@@ -34,7 +34,7 @@ EXPORTED = [
     "aco_pheromone_update_noalloc", "aco_batch_create", "aco_batch_init", "aco_batch_iterate",
     "aco_batch_enqueue_iterations", "aco_batch_status", "aco_batch_size", "aco_batch_get_best",
     "aco_batch_get_solutions", "aco_batch_get_pheromone", "aco_batch_time_phases", "aco_batch_get_stream",
-    "aco_batch_destroy",
+    "aco_batch_destroy", "aco_autotune", "aco_batch_autotune",
 ]
 
 
@@ -59,7 +59,8 @@ class AcoParams(ctypes.Structure):
         ("mode", ctypes.c_int), ("nloc", ctypes.c_int), ("seed_time", ctypes.c_int), ("rnd_seed", ctypes.c_int),
         ("max_iteration", ctypes.c_int), ("max_runtime", ctypes.c_float), ("ls_pass_limit", ctypes.c_int),
         ("record_cap", ctypes.c_int), ("device", ctypes.c_int), ("use_graph", ctypes.c_int),
-        ("ants_per_block", ctypes.c_int), ("warps_per_ant", ctypes.c_int),
+        ("ants_per_block", ctypes.c_int), ("warps_per_ant", ctypes.c_int), ("ls_warps", ctypes.c_int),
+        ("stage_matrix", ctypes.c_int),
     ]
 
 
@@ -126,6 +127,10 @@ def lib() -> ctypes.CDLL:
         L.aco_batch_get_stream.restype = vp
         L.aco_batch_destroy.argtypes = [vp]
         L.aco_batch_destroy.restype = None
+        L.aco_autotune.argtypes = [ctypes.POINTER(AcoInstance), ctypes.POINTER(AcoParams), ip,
+                                   ctypes.POINTER(AcoParams), ctypes.POINTER(fp)]
+        L.aco_batch_autotune.argtypes = [ctypes.POINTER(AcoInstance), ip, ctypes.POINTER(AcoParams), ip,
+                                         ctypes.POINTER(AcoParams), ctypes.POINTER(fp)]
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
         _lib = L
     return _lib

@@ -179,11 +179,13 @@ def default_params(n: int) -> AcoParams:
 class Solver:
     """One solver handle: device state of one instance on one GPU."""
 
-    def __init__(self, problem: Problem, params: Optional[AcoParams] = None, **overrides):
+    def __init__(self, problem: Problem, params: Optional[AcoParams] = None, tune_table=None, **overrides):
         self.problem = problem
         p = params if params is not None else default_params(problem.num_node)
         for k, v in overrides.items():
             setattr(p, k, v)
+        if tune_table is not None:  # fills the launch-shape fields left at 0
+            tune_table.apply(p, problem.num_node)
         self.params = p
         ci, keep = problem.c_instance()
         h = ctypes.c_void_p()
@@ -328,13 +330,16 @@ class Batch:
     ``rnd_seed + b`` runs on it; the batch only shares launches, the work
     queue of the construct kernel and one device arena."""
 
-    def __init__(self, problems: List[Problem], params: Optional[AcoParams] = None, **overrides):
+    def __init__(self, problems: List[Problem], params: Optional[AcoParams] = None, tune_table=None, **overrides):
         self.problems = list(problems)
         if params is None:
             params = default_params(max(p.num_node for p in self.problems))
             params.mode = _lib.MODE_THROUGHPUT
         for k, v in overrides.items():
             setattr(params, k, v)
+        if tune_table is not None:  # one launch shape for the batch: the entry of the median size
+            sizes = sorted(p.num_node for p in self.problems)
+            tune_table.apply(params, sizes[len(sizes) // 2])
         self.params = params
         cis, self._keep = [], []
         for p in self.problems:

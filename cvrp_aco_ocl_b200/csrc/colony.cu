@@ -233,6 +233,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         cp_wpa = wpa;
         const int per_block = std::max(1, std::min(8, (ih.A + sm_count - 1) / sm_count));
         cp_apc = p.ants_per_block > 0 ? p.ants_per_block : std::max(1, per_block / wpa);
+        if (cp_apc * cp_wpa > 16) return ACO_ERR_INVALID; // 512 threads per CTA at most
         cp_stage = construct_parity_smem(ih.n, ih.nloc, ih.kmax, wpa, cp_apc, true, fin_any) <= kSmemBudget;
     } else {
         // ants per work item: enough CTAs to cover the SMs for one instance,
@@ -249,7 +250,8 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
                 bool packable = true;
                 for (int i = 0; i < ih.n; i++)
                     if (ih.demand[i] < 0 || ih.demand[i] > 0xFFFF) packable = false;
-                ih.smat = ih.n <= 1024 && packable && construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, true, true) <= kSmemBudget;
+                ih.smat = p.stage_matrix >= 0 && ih.n <= 1024 && packable &&
+                          construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, true, true) <= kSmemBudget;
                 ih.packed = packable && construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, ih.smat, true) <= kSmemBudget;
                 const size_t need = construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, ih.smat, ih.packed);
                 if (need > kSmemBudget) fits = false;
@@ -261,7 +263,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
             }
         }
     }
-    ls_warps = (int)std::max<long long>(1, std::min<long long>(32, max_routes + 2));
+    ls_warps = p.ls_warps > 0 ? p.ls_warps : (int)std::max<long long>(1, std::min<long long>(32, max_routes + 2));
     ls_smem = 0;
     for (const InstHost &ih : inst) ls_smem = std::max(ls_smem, local_search_smem(ih.n, ls_warps));
     while (ls_warps > 1 && ls_smem > kSmemBudget) {

@@ -59,6 +59,8 @@ int check_params(const aco_params &p, int n)
                                  (p.warps_per_ant & (p.warps_per_ant - 1)) || 32 * p.warps_per_ant > p.nloc))
         return ACO_ERR_INVALID;
     if (p.ants_per_block < 0 || p.ants_per_block > 16) return ACO_ERR_INVALID;
+    if (p.ls_warps < 0 || p.ls_warps > 32) return ACO_ERR_INVALID;
+    if (p.stage_matrix < -1 || p.stage_matrix > 0) return ACO_ERR_INVALID;
     if (!(p.rho > 0.0f && p.rho <= 1.0f)) return ACO_ERR_INVALID;
     if (p.n_ants > 56 * 1024) return ACO_ERR_INVALID; // the statistics kernel holds n_ants lengths in shared memory
     return ACO_OK;
@@ -611,3 +613,117 @@ int aco_batch_time_phases(aco_batch *b, int n_iter, float *ms4)
 void *aco_batch_get_stream(aco_batch *b) { return b ? (void *)b->c.st : nullptr; }
 
 } // extern "C"
+
+/* ---- autotuner ------------------------------------------------------------ */
+
+namespace {
+
+// Per-kernel times (ms per iteration) of one configuration on a fresh colony.
+int time_config(const InstanceSpec *specs, int count, const aco_params &p, int iters, float *ph4)
+{
+    Colony c;
+    int rc = c.create(specs, count, p);
+    if (rc == ACO_OK) rc = c.init();
+    if (rc == ACO_OK) rc = c.enqueue(2);
+    if (rc == ACO_OK) rc = c.sync_status();
+    if (rc == ACO_OK) rc = c.time_phases(iters, ph4);
+    if (rc != ACO_OK) return rc;
+    for (int k = 0; k < 4; k++) ph4[k] /= (float)iters;
+    return ACO_OK;
+}
+
+int autotune(const InstanceSpec *specs, int count, const aco_params &p0, int iters, aco_params *out, float *ms_out)
+{
+    if (iters < 1 || !out) return ACO_ERR_INVALID;
+    const bool thr = p0.mode == ACO_MODE_THROUGHPUT;
+    aco_params best = p0;
+    float best_ph[4] = {0, 0, 0, 0};
+    float best_c = INFINITY;
+    bool any = false;
+    // construct: ants per CTA x (warps per ant | matrix staging)
+    std::vector<std::pair<int, int>> cands;
+    if (thr) {
+        for (int apc : {1, 2, 4, 8, 16})
+            for (int stage : {0, -1}) cands.push_back({apc, stage});
+    } else {
+        for (int wpa : {1, 2, 4, 8})
+            for (int apc : {1, 2, 4, 8})
+                if (wpa * apc <= 16 && 32 * wpa <= p0.nloc) cands.push_back({apc, wpa});
+    }
+    for (const auto &cd : cands) {
+        aco_params q = p0;
+        q.ants_per_block = cd.first;
+        if (thr) q.stage_matrix = cd.second;
+        else q.warps_per_ant = cd.second;
+        if (q.ls_warps == 0 && best.ls_warps != 0) q.ls_warps = best.ls_warps;
+        float ph[4];
+        if (time_config(specs, count, q, iters, ph) != ACO_OK) continue; // e.g. shared memory does not fit
+        if (ph[0] < best_c) {
+            best_c = ph[0];
+            best = q;
+            std::memcpy(best_ph, ph, sizeof(ph));
+            any = true;
+        }
+    }
+    if (!any) return ACO_ERR_INVALID;
+    // 2-opt CTA width with the chosen construct
+    if (p0.ls_flag && p0.ls_warps == 0) {
+        float best_l = best_ph[1];
+        int best_w = 0;
+        for (int w : {4, 8, 16, 32}) {
+            aco_params q = best;
+            q.ls_warps = w;
+            float ph[4];
+            if (time_config(specs, count, q, iters, ph) != ACO_OK) continue;
+            if (ph[1] < best_l) {
+                best_l = ph[1];
+                best_w = w;
+                std::memcpy(best_ph, ph, sizeof(ph));
+                best_ph[0] = best_c;
+            }
+        }
+        best.ls_warps = best_w;
+    }
+    *out = best;
+    if (ms_out) *ms_out = best_ph[0] + best_ph[1] + best_ph[2] + best_ph[3];
+    return ACO_OK;
+}
+
+} // namespace
+
+int aco_autotune(const aco_instance *inst, const aco_params *params, int iters, aco_params *out, float *ms_out)
+{
+    if (!inst || !out || !spec_ok(*inst)) return ACO_ERR_INVALID;
+    const int n = inst->n;
+    aco_params p;
+    if (params) p = *params;
+    else aco_params_default(&p, n);
+    if (p.n_ants <= 0) p.n_ants = n;
+    if (p.record_cap <= 0) p.record_cap = 4096;
+    int rc = check_params(p, n);
+    if (rc != ACO_OK) return rc;
+    const InstanceSpec sp = spec_of(*inst);
+    return autotune(&sp, 1, p, iters, out, ms_out);
+}
+
+int aco_batch_autotune(const aco_instance *insts, int count, const aco_params *params, int iters, aco_params *out,
+                       float *ms_out)
+{
+    if (!insts || !params || !out || count < 1 || count > 65535) return ACO_ERR_INVALID;
+    if (params->mode != ACO_MODE_THROUGHPUT || params->n_ants <= 0) return ACO_ERR_INVALID;
+    std::vector<InstanceSpec> specs(count);
+    int n_min = INT_MAX;
+    for (int b = 0; b < count; b++) {
+        if (!spec_ok(insts[b]) || insts[b].n > 1024) return ACO_ERR_INVALID;
+        n_min = std::min(n_min, insts[b].n);
+        specs[b] = spec_of(insts[b]);
+    }
+    aco_params pc = *params;
+    pc.nn_ls = std::min(pc.nn_ls, n_min - 2);
+    pc.nn_ants = std::min(pc.nn_ants, n_min - 2);
+    const int rc = check_params(pc, n_min);
+    if (rc != ACO_OK) return rc;
+    aco_params p = *params;
+    if (p.record_cap <= 0) p.record_cap = 4096;
+    return autotune(specs.data(), count, p, iters, out, ms_out);
+}

@@ -87,6 +87,9 @@ typedef struct aco_params {
     int use_graph;        /* 1 = replay one CUDA graph per iteration (default 1) */
     int ants_per_block;   /* 0 = autotuned; else ants per CTA of the construct kernel */
     int warps_per_ant;    /* 0 = autotuned; else warps per ant of the parity construct kernel (1,2,4,8) */
+    int ls_warps;         /* 0 = autotuned; else warps per 2-opt CTA (1..32, one route per warp at a time) */
+    int stage_matrix;     /* throughput construct: 0 = stage the whole total_info matrix in shared memory when
+                             it fits (used by the no-candidate fallback); -1 = never, rows are read through L2 */
 } aco_params;
 
 /* One best-so-far record {iteration, length, seconds since init} (problem.h:62-66). */
@@ -187,6 +190,22 @@ int aco_time_phases(aco_solver *s, int n_iter, float *ms4);
  * construct, and whether matrices are staged in shared memory (bit 0: total_info
  * in construct, bit 1: NN lists in 2-opt). */
 int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *staging_flags);
+
+/* ---- autotuner (no reference counterpart) -----------------------------------
+ * Times launch configurations on the instance(s) and returns the fastest in
+ * *out (a copy of *p with ants_per_block, ls_warps, stage_matrix -- and
+ * warps_per_ant in ACO_MODE_PARITY -- set explicitly).  Every configuration
+ * computes the same tours, lengths and pheromone bit for bit; only speed
+ * differs.  Each candidate runs on a fresh solver from the same seeds:
+ * aco_init, 2 warm-up iterations, then `iters` timed iterations (per-kernel
+ * CUDA events).  The construct candidates (ants per CTA x staging) are timed
+ * first with the default 2-opt shape, then the 2-opt CTA widths with the best
+ * construct.  ms_out (optional) = the chosen configuration's time per
+ * iteration.  The candidate-list length (nn_ants) changes the search itself,
+ * not only its speed, so it is not chosen here. */
+int aco_autotune(const aco_instance *inst, const aco_params *p, int iters, aco_params *out, float *ms_out);
+int aco_batch_autotune(const aco_instance *insts, int count, const aco_params *p, int iters, aco_params *out,
+                       float *ms_out);
 
 /* ---- batches: many independent instances in the same launches --------------
  * No reference counterpart (the reference solves one instance per process).
