@@ -34,7 +34,8 @@ EXPORTED = [
     "aco_pheromone_update_noalloc", "aco_batch_create", "aco_batch_init", "aco_batch_iterate",
     "aco_batch_enqueue_iterations", "aco_batch_status", "aco_batch_size", "aco_batch_get_best",
     "aco_batch_get_solutions", "aco_batch_get_pheromone", "aco_batch_time_phases", "aco_batch_get_stream",
-    "aco_batch_destroy", "aco_autotune", "aco_batch_autotune",
+    "aco_batch_destroy", "aco_autotune", "aco_batch_autotune", "aco_mpnn_param_count", "aco_mpnn_workspace_bytes",
+    "aco_mpnn_forward", "aco_mpnn_grad", "aco_mpnn_adam", "aco_mpnn_status", "aco_set_prior", "aco_batch_set_prior",
 ]
 
 
@@ -131,6 +132,15 @@ def lib() -> ctypes.CDLL:
                                    ctypes.POINTER(AcoParams), ctypes.POINTER(fp)]
         L.aco_batch_autotune.argtypes = [ctypes.POINTER(AcoInstance), ip, ctypes.POINTER(AcoParams), ip,
                                          ctypes.POINTER(AcoParams), ctypes.POINTER(fp)]
+        sz = ctypes.c_size_t
+        L.aco_mpnn_param_count.argtypes = [ip]
+        L.aco_mpnn_workspace_bytes.argtypes = [ip, ip, ip, ctypes.POINTER(sz)]
+        L.aco_mpnn_forward.argtypes = [ip, ip, ip, vp, vp, vp, vp, vp, sz, vp, vp]
+        L.aco_mpnn_grad.argtypes = [ip, ip, ip, vp, vp, vp, vp, vp, fp, vp, sz, vp, vp, vp, vp]
+        L.aco_mpnn_adam.argtypes = [ip, vp, vp, vp, vp, fp, fp, fp, fp, ip, vp]
+        L.aco_mpnn_status.argtypes = [vp, vp]
+        L.aco_set_prior.argtypes = [vp, vp, ip]
+        L.aco_batch_set_prior.argtypes = [vp, ip, vp, ip]
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
         _lib = L
     return _lib

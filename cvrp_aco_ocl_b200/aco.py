@@ -288,6 +288,16 @@ class Solver:
                   "aco_get_bsf_records")
         return [(arr[i].iter, arr[i].length, arr[i].time) for i in range(k)]
 
+    def set_prior(self, prior=None):
+        """heur = eta^beta * prior (n x n, finite, >= 0); None restores eta^beta."""
+        if prior is None:
+            check(lib().aco_set_prior(self.h, None, 0), "aco_set_prior")
+            return
+        pr = np.ascontiguousarray(prior, np.float32)
+        if pr.shape != (self.n, self.n):
+            raise ValueError(f"prior must be {self.n} x {self.n}")
+        check(lib().aco_set_prior(self.h, ptr(pr), self.n), "aco_set_prior")
+
     def set_state(self, tau=None, total=None, solutions=None, lens=None, seeds=None):
         def c(a, dt):
             return None if a is None else np.ascontiguousarray(a, dt)
@@ -402,6 +412,17 @@ class Batch:
         ms = np.zeros(4, np.float32)
         check(lib().aco_batch_time_phases(self.h, n_iter, ptr(ms)), "aco_batch_time_phases")
         return ms
+
+    def set_prior(self, b: int, prior=None):
+        """Prior of instance b (see Solver.set_prior)."""
+        if prior is None:
+            check(lib().aco_batch_set_prior(self.h, b, None, 0), "aco_batch_set_prior")
+            return
+        n = self.problems[b].num_node
+        pr = np.ascontiguousarray(prior, np.float32)
+        if pr.shape != (n, n):
+            raise ValueError(f"prior must be {n} x {n}")
+        check(lib().aco_batch_set_prior(self.h, b, ptr(pr), n), "aco_batch_set_prior")
 
     def close(self):
         if self.h:

@@ -171,7 +171,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         ld_max = std::max(ld_max, ih.ld);
     }
     const size_t o_ant_inst = take((size_t)total_ants * 4), o_ant_base = take((size_t)(count + 1) * 4);
-    const size_t o_row_base = take((size_t)(count + 1) * 4);
+    const size_t o_row_base = take((size_t)(count + 1) * 4), o_zero_base = take(16);
     const size_t o_cargs = take(sizeof(ConstructArgs) * count), o_largs = take(sizeof(LocalSearchArgs) * count);
     const size_t o_sargs = take(sizeof(StatsArgs) * count), o_uargs = take(sizeof(UpdateArgs) * count);
     // construct work items {instance, first ant}, larger instances first
@@ -205,6 +205,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     ant_inst_d_ = (int *)(base + o_ant_inst);
     ant_base_d_ = (int *)(base + o_ant_base);
     row_base_d_ = (int *)(base + o_row_base);
+    zero_base_d_ = (int *)(base + o_zero_base); // {0}: row base of a one-instance launch
     cargs_d_ = (ConstructArgs *)(base + o_cargs);
     largs_d_ = (LocalSearchArgs *)(base + o_largs);
     sargs_d_ = (StatsArgs *)(base + o_sargs);
@@ -394,6 +395,39 @@ int Colony::run_rows(int mode, float trail)
 {
     CK(launch_rows(uargs_d_, row_base_d_, (int)inst.size(), total_rows, mode, trail, sm_count, st));
     return ACO_OK;
+}
+
+int Colony::run_rows_one(int b, int mode)
+{
+    CK(launch_rows(uargs_d_ + b, zero_base_d_, 1, inst[b].n, mode, 0.f, sm_count, st));
+    return ACO_OK;
+}
+
+int Colony::set_prior(int b, const float *prior, int ld)
+{
+    if (b < 0 || b >= (int)inst.size()) return ACO_ERR_INVALID;
+    InstHost &ih = inst[b];
+    const int n = ih.n;
+    if (prior) {
+        if (ld < n) return ACO_ERR_INVALID;
+        for (int i = 0; i < n; i++) // weights must stay usable by the roulette
+            for (int j = 0; j < n; j++) {
+                const float v = prior[(size_t)i * ld + j];
+                if (!(v >= 0.0f) || std::isinf(v)) return ACO_ERR_INVALID;
+            }
+    }
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    if (prior) {
+        CK(cudaMemcpy2DAsync(ih.heur_d, (size_t)ih.ld * 4, prior, (size_t)ld * 4, (size_t)n * 4, n,
+                             cudaMemcpyHostToDevice, st));
+        rc = run_rows_one(b, ROW_PRIOR);
+    } else {
+        rc = run_rows_one(b, ROW_HEUR);
+    }
+    if (rc == ACO_OK && initialized) rc = run_rows_one(b, ROW_TOTAL);
+    if (rc != ACO_OK) return rc;
+    return sync_status();
 }
 
 int Colony::construct()

@@ -60,6 +60,9 @@ public:
     int update();
     int pheromone_init(float trail, bool from_bsf);
     int gather_candidates();     // refresh the compact candidate table from total_info
+    // heur = eta^beta * prior for instance b (prior: n x n host array, row stride ld;
+    // null restores eta^beta); total_info follows when the colony is initialised
+    int set_prior(int b, const float *prior, int ld);
     int time_phases(int n_iter, float *ms4);
     int set_device() const;
 
@@ -86,12 +89,13 @@ private:
     int run_phases();
     int ensure_graph();
     int run_rows(int mode, float trail);
+    int run_rows_one(int b, int mode);
     std::vector<void *> allocs_;
     void *arena_ = nullptr;
     unsigned long long *t0_d_ = nullptr;
     int2 *items_d_ = nullptr;
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
-    int *row_base_d_ = nullptr;
+    int *row_base_d_ = nullptr, *zero_base_d_ = nullptr;
     ConstructArgs *cargs_d_ = nullptr;
     LocalSearchArgs *largs_d_ = nullptr;
     StatsArgs *sargs_d_ = nullptr;

@@ -93,7 +93,15 @@ struct UpdateArgs {
 };
 
 // Per-row pass modes of the row kernel.
-enum RowMode { ROW_HEUR = 0, ROW_INIT_TRAIL = 1, ROW_INIT_BSF = 2, ROW_UPDATE = 3, ROW_GATHER = 4 };
+enum RowMode {
+    ROW_HEUR = 0,       // heur = eta^beta
+    ROW_INIT_TRAIL = 1, // tau = trail, total = trail^alpha * heur
+    ROW_INIT_BSF = 2,   // same with trail = 1 / (rho * best-so-far length)
+    ROW_UPDATE = 3,     // evaporation + deposit + total_info
+    ROW_GATHER = 4,     // candidate table from total_info
+    ROW_PRIOR = 5,      // heur = eta^beta * (prior held in heur on entry)
+    ROW_TOTAL = 6,      // total = tau^alpha * heur
+};
 
 // Launchers (stream-ordered; return cudaGetLastError()).  `d_*args` point to
 // arrays of argument blocks in device memory, one per instance.

@@ -265,7 +265,8 @@ __device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, f
     const float4 *heur4 = reinterpret_cast<const float4 *>(a.heur + off);
     float4 *tau4 = reinterpret_cast<float4 *>(a.tau + off);
     float4 *tot4 = reinterpret_cast<float4 *>(a.total + off);
-    if (mode == ROW_HEUR) {
+    if (mode == ROW_HEUR || mode == ROW_PRIOR) {
+        // eta^beta; ROW_PRIOR multiplies it by the prior the heuristic matrix holds on entry
         const float4 *dist4 = reinterpret_cast<const float4 *>(a.dist + off);
         float4 *h4 = reinterpret_cast<float4 *>(a.heur + off);
         for (int q = lane; q < q4; q += 32) {
@@ -276,9 +277,27 @@ __device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, f
             h.y = c + 1 < n ? pow_rule(__fdiv_rn(1.0f, __fadd_rn(d.y, 0.1f)), a.beta, a.beta_int) : 0.f;
             h.z = c + 2 < n ? pow_rule(__fdiv_rn(1.0f, __fadd_rn(d.z, 0.1f)), a.beta, a.beta_int) : 0.f;
             h.w = c + 3 < n ? pow_rule(__fdiv_rn(1.0f, __fadd_rn(d.w, 0.1f)), a.beta, a.beta_int) : 0.f;
+            if (mode == ROW_PRIOR) {
+                const float4 pr = h4[q];
+                h.x = __fmul_rn(h.x, pr.x);
+                h.y = __fmul_rn(h.y, pr.y);
+                h.z = __fmul_rn(h.z, pr.z);
+                h.w = __fmul_rn(h.w, pr.w);
+            }
             h4[q] = h;
         }
         return;
+    }
+    if (mode == ROW_TOTAL) { // compute_total_info (kernel.cl:782-789) from the current tau and heur
+        for (int q = lane; q < q4; q += 32) {
+            const float4 t = tau4[q], h = heur4[q];
+            float4 o;
+            o.x = __fmul_rn(pow_rule(t.x, a.alpha, a.alpha_int), h.x);
+            o.y = __fmul_rn(pow_rule(t.y, a.alpha, a.alpha_int), h.y);
+            o.z = __fmul_rn(pow_rule(t.z, a.alpha, a.alpha_int), h.z);
+            o.w = __fmul_rn(pow_rule(t.w, a.alpha, a.alpha_int), h.w);
+            tot4[q] = o;
+        }
     }
     if (mode == ROW_INIT_TRAIL || mode == ROW_INIT_BSF) { // pheromone_init (kernel.cl:672-679)
         const float tr = mode == ROW_INIT_BSF ? __fdiv_rn(1.0f, __fmul_rn(a.rho, *a.bsf_len)) : trail;
@@ -381,6 +400,12 @@ cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, int n_i
         break;
     case ROW_UPDATE:
         rows_kernel<ROW_UPDATE><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        break;
+    case ROW_PRIOR:
+        rows_kernel<ROW_PRIOR><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        break;
+    case ROW_TOTAL:
+        rows_kernel<ROW_TOTAL><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
         break;
     default: rows_kernel<ROW_GATHER><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail); break;
     }

@@ -518,6 +518,12 @@ int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *
     return ACO_OK;
 }
 
+int aco_set_prior(aco_solver *s, const float *prior, int ld)
+{
+    if (!s) return ACO_ERR_INVALID;
+    return s->c.set_prior(0, prior, ld);
+}
+
 /* ---- batches ------------------------------------------------------------ */
 
 int aco_batch_create(const aco_instance *insts, int count, const aco_params *params, aco_batch **out)
@@ -608,6 +614,12 @@ int aco_batch_time_phases(aco_batch *b, int n_iter, float *ms4)
 {
     if (!b || !ms4 || n_iter <= 0) return ACO_ERR_INVALID;
     return b->c.time_phases(n_iter, ms4);
+}
+
+int aco_batch_set_prior(aco_batch *b, int idx, const float *prior, int ld)
+{
+    if (!b) return ACO_ERR_INVALID;
+    return b->c.set_prior(idx, prior, ld);
 }
 
 void *aco_batch_get_stream(aco_batch *b) { return b ? (void *)b->c.st : nullptr; }

@@ -230,6 +230,45 @@ int aco_batch_time_phases(aco_batch *b, int n_iter, float *ms4);
 void *aco_batch_get_stream(aco_batch *b);
 void aco_batch_destroy(aco_batch *b);
 
+/* ---- learned prior: edge-scoring network (no reference counterpart) -------
+ * A message-passing network on the k-nearest-customer graph of an instance
+ * scores every edge (i, j); sigmoid(score) multiplies eta^beta as a sampling
+ * prior (aco_set_prior).  Hidden width 64, BF16 tensor-core products with FP32
+ * accumulation, FP32 master parameters (aco_mpnn_param_count floats, packed
+ * in the order embeddings, layers (W, b, A, a), head (W_h, b_h, w_o, b_o)).
+ * Graph arrays hold node i's k out-edges at rows i*k .. i*k+k-1; several
+ * graphs are batched by concatenating their nodes (nbr holds global ids).
+ * All pointers below are device pointers; stream may be NULL.  The calls only
+ * enqueue work; aco_mpnn_status synchronises and returns the sticky status. */
+#define ACO_MPNN_HIDDEN 64
+#define ACO_MPNN_NODE_FEATURES 5 /* x, y (bounding-box normalised), demand/capacity, is_depot, d(i, depot) */
+int aco_mpnn_param_count(int layers);
+int aco_mpnn_workspace_bytes(int n_nodes, int k, int layers, size_t *bytes);
+/* scores[n_nodes*k]: edge logits. */
+int aco_mpnn_forward(int n_nodes, int k, int layers, const float *params, const float *node_feat,
+                     const float *edge_feat, const int *nbr, void *workspace, size_t ws_bytes, float *scores,
+                     void *stream);
+/* Forward + backward of the mean weighted binary cross-entropy against labels
+ * (1 = the edge is on the target route): grad (param_count floats) and *loss
+ * are overwritten; scores (optional) receives the logits. */
+int aco_mpnn_grad(int n_nodes, int k, int layers, const float *params, const float *node_feat, const float *edge_feat,
+                  const int *nbr, const float *labels, float pos_weight, void *workspace, size_t ws_bytes, float *grad,
+                  float *loss, float *scores, void *stream);
+/* One Adam step (bias-corrected, step >= 1) on count parameters. */
+int aco_mpnn_adam(int count, float *params, const float *grad, float *m, float *v, float lr, float beta1, float beta2,
+                  float eps, int step, void *stream);
+int aco_mpnn_status(void *workspace, void *stream);
+
+/* Sampling prior: heur = eta^beta * prior (prior: n x n host array, row stride
+ * ld >= n, finite and >= 0), so that total_info = tau^alpha * eta^beta * prior.
+ * Tours stay feasible and lengths exact: only the choice weights change.  Call
+ * before aco_init (the bootstrap construct uses it) or between iterations
+ * (total_info is recomputed from the current tau).  prior = NULL restores plain
+ * eta^beta, the fallback.  A non-uniform prior departs from the reference's
+ * choice rule: use it with ACO_MODE_THROUGHPUT. */
+int aco_set_prior(aco_solver *s, const float *prior, int ld);
+int aco_batch_set_prior(aco_batch *b, int idx, const float *prior, int ld);
+
 /* ---- pheromone update without allocation ---------------------------------
  * No counterpart in the reference.  For callers that cannot let this library
  * allocate device memory: hosts whose memory manager owns all device memory,
