@@ -254,7 +254,13 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
                 ih.smat = p.stage_matrix >= 0 && ih.n <= 1024 && packable &&
                           construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, true, true) <= kSmemBudget;
                 ih.packed = packable && construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, ih.smat, true) <= kSmemBudget;
-                const size_t need = construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, ih.smat, ih.packed);
+                ih.gtab = false;
+                size_t need = construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, ih.smat, ih.packed);
+                if (need > kSmemBudget) { // the candidate table stays in global memory (read through L2)
+                    ih.gtab = true;
+                    ih.packed = packable;
+                    need = construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, false, ih.packed, true);
+                }
                 if (need > kSmemBudget) fits = false;
                 cn_smem = std::max(cn_smem, need);
             }
@@ -353,7 +359,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         c.capacity = ih.capacity; c.max_dist = ih.max_dist; c.serv_time = ih.serv_time;
         c.total = ih.total_d; c.dist = ih.dist_d; c.demand = ih.dem_d; c.tiekey = ih.key_d; c.jump = ih.jump_d;
         c.adv = ih.adv_d; c.nn16 = ih.nn16_d; c.cand32 = ih.cand32_d; c.chc = ih.chc_d; c.K = ih.K; c.Kp = ih.Kp;
-        c.smat = ih.smat ? 1 : 0; c.packed = ih.packed ? 1 : 0;
+        c.smat = ih.smat ? 1 : 0; c.packed = ih.packed ? 1 : 0; c.gtab = ih.gtab ? 1 : 0;
         c.seeds = ih.seeds_d; c.solutions = ih.sol_d; c.lens = ih.lens_d; c.status = status_d;
         LocalSearchArgs &l = largs[b];
         l = LocalSearchArgs{};

@@ -29,7 +29,7 @@ struct InstHost {
     int n = 0, ld = 0, n4 = 0, A = 0, T = 0, K = 0, Kp = 8, nn_ls = 0, R = 0, nloc = 0, lg = 0, kmax = 0;
     int capacity = 0;
     float max_dist = 0, serv_time = 0;
-    bool smat = false, packed = false;
+    bool smat = false, packed = false, gtab = false;
     std::vector<float> dist; // n*n
     std::vector<int> demand;
     std::vector<int> nn;     // n x depth

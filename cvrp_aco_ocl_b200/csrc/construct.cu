@@ -236,7 +236,9 @@ struct NNLayout {
     size_t bar, dem, d0, cand, chc, vis, tour, mat, bytes;
 };
 
-__host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, bool smat, bool packed)
+// gtab: the candidate table is read from global memory (L2) instead of being
+// staged (instances whose table does not fit next to the per-ant buffers).
+__host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, bool smat, bool packed, bool gtab)
 {
     const size_t n4 = (size_t)((n + 3) & ~3);
     const size_t words = (size_t)((n + 31) / 32);
@@ -245,8 +247,8 @@ __host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, boo
     L.bar = o; o = al128(o + 16);
     L.dem = o; o = al128(o + n4 * 4);
     L.d0 = o; o = al128(o + n4 * 4);
-    L.cand = o; o = al128(o + (size_t)n * Kp * (packed ? 4 : 2));
-    L.chc = o; o = al128(o + (size_t)n * Kp * 4);
+    L.cand = o; if (!gtab) o = al128(o + (size_t)n * Kp * (packed ? 4 : 2));
+    L.chc = o; if (!gtab) o = al128(o + (size_t)n * Kp * 4);
     L.vis = o; o = al128(o + (size_t)apc * words * 4);
     L.tour = o; o = al128(o + (size_t)apc * 2 * n * 2);
     L.mat = o;
@@ -258,19 +260,20 @@ __host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, boo
 
 // One work item: ants [ant0, ant0 + apc) of instance a.  Returns false if the
 // staging copies did not arrive in time (uniform over the CTA).
-template <bool FIN, bool SMAT, bool PACKED, bool REGVIS>
+template <bool FIN, bool SMAT, bool PACKED, bool REGVIS, bool GTAB = false>
 __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int apc, int ant0, unsigned char *smem, uint32_t phase,
                                   uint32_t pw)
 {
     const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp, T = a.T;
     const int n4 = (n + 3) & ~3;
-    const NNLayout L = nn_layout(n, K, Kp, apc, SMAT, PACKED);
+    const NNLayout L = nn_layout(n, K, Kp, apc, SMAT, PACKED, GTAB);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar);
     int *s_dem = reinterpret_cast<int *>(smem + L.dem);
     float *s_d0 = reinterpret_cast<float *>(smem + L.d0);
-    uint32_t *s_cand = reinterpret_cast<uint32_t *>(smem + L.cand);
-    uint16_t *s_nn = reinterpret_cast<uint16_t *>(smem + L.cand);
-    float *s_chc = reinterpret_cast<float *>(smem + L.chc);
+    // candidate table: staged copy, or the global one itself (generic loads either way)
+    const uint32_t *s_cand = GTAB ? a.cand32 : reinterpret_cast<const uint32_t *>(smem + L.cand);
+    const uint16_t *s_nn = GTAB ? a.nn16 : reinterpret_cast<const uint16_t *>(smem + L.cand);
+    const float *s_chc = GTAB ? a.chc : reinterpret_cast<const float *>(smem + L.chc);
     uint32_t *s_vis = reinterpret_cast<uint32_t *>(smem + L.vis);
     uint16_t *s_tour = reinterpret_cast<uint16_t *>(smem + L.tour);
     float *s_mat = reinterpret_cast<float *>(smem + L.mat);
@@ -280,12 +283,14 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
 
     const uint32_t cand_bytes = (uint32_t)(n * Kp * (PACKED ? 4 : 2));
     if (threadIdx.x == 0) {
-        uint32_t bytes = (uint32_t)(n4 * 4) + cand_bytes + (uint32_t)(n * Kp * 4);
+        uint32_t bytes = (uint32_t)(n4 * 4) + (GTAB ? 0u : cand_bytes + (uint32_t)(n * Kp * 4));
         if (SMAT) bytes += (uint32_t)(n * n4 * 4);
         mbar_arrive_expect_tx(bar, bytes);
         tma_bulk_g2s(s_dem, a.demand, n4 * 4, bar);
-        tma_bulk_g2s(s_cand, PACKED ? (const void *)a.cand32 : (const void *)a.nn16, cand_bytes, bar);
-        tma_bulk_g2s(s_chc, a.chc, n * Kp * 4, bar);
+        if (!GTAB) {
+            tma_bulk_g2s(smem + L.cand, PACKED ? (const void *)a.cand32 : (const void *)a.nn16, cand_bytes, bar);
+            tma_bulk_g2s(smem + L.chc, a.chc, n * Kp * 4, bar);
+        }
     }
     if (SMAT)
         for (int r = threadIdx.x; r < n; r += blockDim.x)
@@ -465,7 +470,10 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *
         const ConstructArgs a = args[code.x];
         const int ant0 = code.y;
         bool ok;
-        if (a.n <= 1024) {
+        if (a.gtab) {
+            ok = a.packed ? construct_nn_item<FIN, false, true, false, true>(a, apc, ant0, smem, phase, pw)
+                          : construct_nn_item<FIN, false, false, false, true>(a, apc, ant0, smem, phase, pw);
+        } else if (a.n <= 1024) {
             if (a.smat) ok = a.packed ? construct_nn_item<FIN, true, true, true>(a, apc, ant0, smem, phase, pw)
                                       : construct_nn_item<FIN, true, false, true>(a, apc, ant0, smem, phase, pw);
             else ok = a.packed ? construct_nn_item<FIN, false, true, true>(a, apc, ant0, smem, phase, pw)
@@ -506,9 +514,9 @@ size_t construct_parity_smem(int n, int nloc, int kmax, int wpa, int apc, bool s
     return parity_layout(n, nloc, kmax, wpa, apc, stage_total).bytes;
 }
 
-size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool packed)
+size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool packed, bool global_table)
 {
-    return nn_layout(n, K, Kp, apc, stage_total, packed).bytes;
+    return nn_layout(n, K, Kp, apc, stage_total, packed, global_table).bytes;
 }
 
 cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue, int apc,

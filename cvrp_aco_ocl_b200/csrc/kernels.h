@@ -41,6 +41,7 @@ struct ConstructArgs {
     int K, Kp;             // candidate-list length and padded row length (multiple of 8)
     int smat;              // throughput construct: stage the whole total_info matrix
     int packed;            // throughput construct: use cand32 (else nn16 + demand lookups)
+    int gtab;              // throughput construct: read the candidate table from global memory (not staged)
     int *seeds;
     int *solutions;
     float *lens;
@@ -126,7 +127,8 @@ cudaError_t launch_t0(unsigned long long *t0, cudaStream_t st);
 // the 227 KB per-CTA limit).
 size_t construct_parity_smem(int n, int nloc, int kmax, int warps_per_ant, int ants_per_block, bool stage_total,
                              bool finite_maxd);
-size_t construct_nn_smem(int n, int K, int Kp, int ants_per_cta, bool stage_total, bool packed);
+size_t construct_nn_smem(int n, int K, int Kp, int ants_per_cta, bool stage_total, bool packed,
+                         bool global_table = false);
 size_t local_search_smem(int n, int warps);
 
 } // namespace aco

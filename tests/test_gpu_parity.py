@@ -279,3 +279,15 @@ def test_integer_exponents_and_many_ranks(gpu, mode):
             S.iterate(1); O.run_iteration(throughput=thr)
             compare_state(S, O)
         assert np.array_equal(S.elites(), O.elites)
+
+
+def test_throughput_candidate_table_in_global_memory(gpu):
+    """n=1201 with 25-candidate lists: the table does not fit in shared memory
+    and is read through L2; results stay bit-exact."""
+    inst = I.gen_large(17, 1200)
+    S, O = build_pair(inst, 32, 256, 1796300000, 8, True, 25, mode=MODE_THROUGHPUT, nn_ants=25)
+    with S:
+        S.init(); O.init_aco(throughput=True)
+        compare_state(S, O)
+        S.iterate(1); O.run_iteration(throughput=True)
+        compare_state(S, O)

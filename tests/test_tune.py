@@ -60,3 +60,13 @@ def test_apply_fills_only_unset_fields():
     q.mode = MODE_THROUGHPUT
     t.apply(q, 5000)  # no range holds n: unchanged
     assert (q.ants_per_block, q.ls_warps, q.stage_matrix) == (0, 0, 0)
+
+
+def test_shipped_prior_weights_match_the_network():
+    import numpy as np
+    from cvrp_aco_ocl_b200 import prior as PR
+    from cvrp_aco_ocl_b200._lib import lib
+    d = np.load(PR.DEFAULT_WEIGHTS)
+    assert int(d["layers"]) == PR.LAYERS
+    assert d["params"].size == lib().aco_mpnn_param_count(PR.LAYERS)
+    assert np.all(np.isfinite(d["params"]))
