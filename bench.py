@@ -257,7 +257,8 @@ def run_batched(args, ws, rank, local, peak, peak_kind):
     """Batched workload: BATCH_COUNT independent instances, customer count
     uniform in [100, 1000] (mixed and large generators alternately), 128 ants
     each, all served by the same four launches per iteration.  Instances are
-    sharded over ranks (rank r takes every ws-th instance; no collective).
+    sharded over ranks by estimated cost (cvrp_aco_ocl_b200.shard; no
+    collective on the data path).
     Reports ant-tours/s over the whole batch and the roofline of the fused
     pheromone pass, whose matrices (16 bytes per element over all instances)
     far exceed L2."""
@@ -265,8 +266,11 @@ def run_batched(args, ws, rank, local, peak, peak_kind):
     from cvrp_aco_ocl_b200 import MODE_THROUGHPUT, Batch, Problem, default_params
     from cvrp_aco_ocl_b200 import instances as I
 
+    from cvrp_aco_ocl_b200.shard import shard_of
+
     count_all = args.batch_count
-    insts = I.gen_batch(BATCH_SEED, count_all, 100, 1000)[rank::ws]
+    every = I.gen_batch(BATCH_SEED, count_all, 100, 1000)
+    insts = [every[i] for i in shard_of([x.n for x in every], BATCH_ANTS, ws, rank)]
     probs = [Problem.from_instance(x) for x in insts]
     p = default_params(1001)
     p.mode, p.n_ants, p.nn_ants, p.nn_ls, p.nloc = MODE_THROUGHPUT, BATCH_ANTS, NN_ANTS, NN_LS, NLOC
