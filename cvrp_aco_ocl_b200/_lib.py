@@ -36,6 +36,7 @@ EXPORTED = [
     "aco_batch_get_solutions", "aco_batch_get_pheromone", "aco_batch_time_phases", "aco_batch_get_stream",
     "aco_batch_destroy", "aco_autotune", "aco_batch_autotune", "aco_mpnn_param_count", "aco_mpnn_workspace_bytes",
     "aco_mpnn_forward", "aco_mpnn_grad", "aco_mpnn_adam", "aco_mpnn_status", "aco_set_prior", "aco_batch_set_prior",
+    "aco_last_cuda_error",
 ]
 
 
@@ -141,6 +142,8 @@ def lib() -> ctypes.CDLL:
         L.aco_mpnn_status.argtypes = [vp, vp]
         L.aco_set_prior.argtypes = [vp, vp, ip]
         L.aco_batch_set_prior.argtypes = [vp, ip, vp, ip]
+        L.aco_last_cuda_error.argtypes = []
+        L.aco_last_cuda_error.restype = ctypes.c_char_p
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
         _lib = L
     return _lib
@@ -148,6 +151,8 @@ def lib() -> ctypes.CDLL:
 
 def check(rc: int, where: str = "") -> None:
     if rc != ACO_OK:
+        if rc == -3:  # ACO_ERR_CUDA
+            where = f"{where} [{lib().aco_last_cuda_error().decode()}]"
         raise AcoError(rc, where)
 
 

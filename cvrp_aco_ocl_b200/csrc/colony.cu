@@ -8,6 +8,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <thread>
 
 #include "host.h"
@@ -17,12 +18,16 @@ namespace aco {
 #define CK(x)                                                                                                  \
     do {                                                                                                       \
         cudaError_t e_ = (x);                                                                                  \
-        if (e_ != cudaSuccess) return ACO_ERR_CUDA;                                                            \
+        if (e_ != cudaSuccess) {                                                                               \
+            aco::note_cuda_error(e_);                                                                          \
+            return ACO_ERR_CUDA;                                                                               \
+        }                                                                                                      \
     } while (0)
 
 namespace {
 
-constexpr size_t kSmemBudget = 227 * 1024;
+// 227 KB per CTA minus room for the kernels' static shared memory
+constexpr size_t kSmemBudget = 226 * 1024;
 
 int exp_as_int(float e)
 {
@@ -72,7 +77,82 @@ int prep_instance(const InstanceSpec &sp, const aco_params &p, InstHost &ih)
     return ACO_OK;
 }
 
+// Process-wide resources of one device, made once: its attributes, a memory
+// pool for the colonies' arenas (freed blocks stay cached in the pool, so a
+// new solver does not pay cudaMalloc's cost) and a block of pinned status
+// words handed out in 64-byte slots.
+struct DeviceRes {
+    std::once_flag once;
+    int rc = ACO_OK, sm = 0, major = 0;
+    cudaMemPool_t pool = nullptr;
+    int *pinned = nullptr;
+    std::mutex mu;
+    std::vector<int> free_slots;
+};
+
+constexpr int kMaxDevices = 64, kSlotInts = 16, kSlots = 256;
+DeviceRes g_res[kMaxDevices];
+
+DeviceRes *device_res(int dev)
+{
+    if (dev < 0 || dev >= kMaxDevices) return nullptr;
+    DeviceRes &r = g_res[dev];
+    std::call_once(r.once, [&]() {
+        int dc = 0;
+        if (cudaGetDeviceCount(&dc) != cudaSuccess || dev >= dc) { r.rc = ACO_ERR_NO_DEVICE; return; }
+        if (cudaDeviceGetAttribute(&r.major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&r.sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || r.major < 10) {
+            r.rc = ACO_ERR_NO_DEVICE;
+            return;
+        }
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(dev);
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        if (cudaMemPoolCreate(&r.pool, &props) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX; // never hand cached blocks back to the driver
+            cudaMemPoolSetAttribute(r.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        } else {
+            r.pool = nullptr;
+        }
+        if (cudaMallocHost(&r.pinned, sizeof(int) * kSlotInts * kSlots) == cudaSuccess) {
+            for (int i = kSlots - 1; i >= 0; i--) r.free_slots.push_back(i);
+        } else {
+            r.pinned = nullptr;
+        }
+        cudaSetDevice(prev);
+    });
+    return &r;
+}
+
+int *take_pinned_slot(DeviceRes &r)
+{
+    std::lock_guard<std::mutex> lk(r.mu);
+    if (!r.pinned || r.free_slots.empty()) return nullptr;
+    const int i = r.free_slots.back();
+    r.free_slots.pop_back();
+    return r.pinned + (size_t)i * kSlotInts;
+}
+
+bool give_pinned_slot(DeviceRes &r, int *p)
+{
+    if (!r.pinned || p < r.pinned || p >= r.pinned + kSlotInts * kSlots) return false;
+    std::lock_guard<std::mutex> lk(r.mu);
+    r.free_slots.push_back((int)((p - r.pinned) / kSlotInts));
+    return true;
+}
+
 } // namespace
+
+namespace {
+thread_local cudaError_t t_last_error = cudaSuccess;
+}
+
+void note_cuda_error(cudaError_t e) { t_last_error = e; }
+cudaError_t last_cuda_error() { return t_last_error; }
 
 Colony::~Colony()
 {
@@ -80,8 +160,13 @@ Colony::~Colony()
     if (st) cudaStreamSynchronize(st);
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
-    for (void *q : allocs_) cudaFree(q);
-    if (h_pin) cudaFreeHost(h_pin);
+    for (void *q : allocs_) {
+        if (pooled_ && st) cudaFreeAsync(q, st);
+        else cudaFree(q);
+    }
+    if (st) cudaStreamSynchronize(st);
+    DeviceRes *r = device_res(dev);
+    if (h_pin && !(r && give_pinned_slot(*r, h_pin))) cudaFreeHost(h_pin);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -115,15 +200,14 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         if (err.load() != ACO_OK) return err.load();
     }
     // ---- device
-    int dc = 0;
-    if (cudaGetDeviceCount(&dc) != cudaSuccess || dc <= p.device || p.device < 0) return ACO_ERR_NO_DEVICE;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, p.device) != cudaSuccess || prop.major < 10) return ACO_ERR_NO_DEVICE;
-    sm_count = prop.multiProcessorCount;
+    DeviceRes *res = device_res(p.device);
+    if (!res || res->rc != ACO_OK) return ACO_ERR_NO_DEVICE;
+    sm_count = res->sm;
     int rc = set_device();
     if (rc != ACO_OK) return rc;
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    CK(cudaMallocHost(&h_pin, 64));
+    h_pin = take_pinned_slot(*res);
+    if (!h_pin) CK(cudaMallocHost(&h_pin, 64));
 
     // ---- arena layout
     size_t off = 0;
@@ -179,7 +263,12 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     const size_t o_items = take((size_t)total_ants * sizeof(int2));
 
     void *arena = nullptr;
-    if (cudaMalloc(&arena, off) != cudaSuccess) return ACO_ERR_NOMEM;
+    if (res->pool && cudaMallocFromPoolAsync(&arena, off, res->pool, st) == cudaSuccess) {
+        pooled_ = true;
+    } else {
+        cudaGetLastError(); // clear a failed pool allocation before trying the plain one
+        if (cudaMalloc(&arena, off) != cudaSuccess) return ACO_ERR_NOMEM;
+    }
     allocs_.push_back(arena);
     arena_ = arena;
     CK(cudaMemsetAsync(arena, 0, off, st));

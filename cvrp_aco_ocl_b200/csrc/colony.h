@@ -15,6 +15,11 @@
 
 namespace aco {
 
+// The last CUDA error a library call turned into ACO_ERR_CUDA on this thread
+// (aco_last_cuda_error reports it).
+void note_cuda_error(cudaError_t e);
+cudaError_t last_cuda_error();
+
 struct InstanceSpec { // the fields of aco_instance
     int n;
     const float *x, *y;
@@ -92,6 +97,7 @@ private:
     int run_rows_one(int b, int mode);
     std::vector<void *> allocs_;
     void *arena_ = nullptr;
+    bool pooled_ = false; // arena from the device's memory pool (freed stream-ordered)
     unsigned long long *t0_d_ = nullptr;
     int2 *items_d_ = nullptr;
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;

@@ -201,15 +201,18 @@ void compute_distances(int n, const float *x, const float *y, int dist_type, flo
 // the left end, Lomuto partition with strict <, recursion on [left, last] and
 // [last+1, right]); an explicit stack keeps deep recursion off the C stack.
 // ---------------------------------------------------------------------------
+// Only positions below `keep` are needed: a range that starts at or beyond it
+// is never sorted, which leaves positions [0, keep) exactly as the full sort
+// would (the recursion only permutes elements inside disjoint ranges).
 namespace {
-void quicksort_pairs(float *v, int *idx, int left, int right, std::vector<std::pair<int, int>> &stack)
+void quicksort_pairs(float *v, int *idx, int left, int right, int keep, std::vector<std::pair<int, int>> &stack)
 {
     stack.clear();
     stack.emplace_back(left, right);
     while (!stack.empty()) {
         auto [l, r] = stack.back();
         stack.pop_back();
-        if (l >= r) continue;
+        if (l >= r || l >= keep) continue;
         int m = (l + r) / 2;
         std::swap(v[l], v[m]);
         std::swap(idx[l], idx[m]);
@@ -246,7 +249,7 @@ int compute_nn_lists(int n, const float *dist, int nn_ls, int nn_ants, std::vect
         }
         v[node] = INFINITY;
         v[0] = INFINITY;
-        quicksort_pairs(v.data(), idx.data(), 0, n - 1, stack);
+        quicksort_pairs(v.data(), idx.data(), 0, n - 1, depth, stack);
         for (int i = 0; i < depth; i++) nn[(size_t)node * depth + i] = idx[i];
     }
     return depth;

@@ -43,7 +43,10 @@ namespace {
 #define CK(x)                                                                                                  \
     do {                                                                                                       \
         cudaError_t e_ = (x);                                                                                  \
-        if (e_ != cudaSuccess) return ACO_ERR_CUDA;                                                            \
+        if (e_ != cudaSuccess) {                                                                               \
+            aco::note_cuda_error(e_);                                                                          \
+            return ACO_ERR_CUDA;                                                                               \
+        }                                                                                                      \
     } while (0)
 
 // Parameter checks shared by aco_create and aco_batch_create.
@@ -254,6 +257,12 @@ int aco_make_seeds(int seed_time, int *rnd_seed, int n_ants, int nloc, int *seed
     if (!rnd_seed || !seeds || n_ants <= 0 || nloc <= 0) return ACO_ERR_INVALID;
     make_seeds(seed_time, rnd_seed, n_ants, nloc, seeds);
     return ACO_OK;
+}
+
+const char *aco_last_cuda_error(void)
+{
+    const cudaError_t e = last_cuda_error();
+    return e == cudaSuccess ? "no error" : cudaGetErrorString(e);
 }
 
 const char *aco_strerror(int code)

@@ -171,6 +171,9 @@ int aco_set_state(aco_solver *s, const float *tau, const float *total_info, cons
 /* sticky device status of the last launches (ACO_OK or an ACO_ERR_* code). */
 int aco_status(aco_solver *s);
 const char *aco_strerror(int code);
+/* CUDA's description of the last CUDA error that a call on this thread turned
+ * into ACO_ERR_CUDA (diagnostics; no reference counterpart). */
+const char *aco_last_cuda_error(void);
 
 /* ---- timing and interop --------------------------------------------------- */
 /* the solver's CUDA stream (a cudaStream_t), for event timing by the caller. */
