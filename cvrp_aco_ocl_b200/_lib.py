@@ -36,7 +36,7 @@ EXPORTED = [
     "aco_batch_get_solutions", "aco_batch_get_pheromone", "aco_batch_time_phases", "aco_batch_get_stream",
     "aco_batch_destroy", "aco_autotune", "aco_batch_autotune", "aco_mpnn_param_count", "aco_mpnn_workspace_bytes",
     "aco_mpnn_forward", "aco_mpnn_grad", "aco_mpnn_adam", "aco_mpnn_status", "aco_set_prior", "aco_batch_set_prior",
-    "aco_last_cuda_error",
+    "aco_last_cuda_error", "aco_compute_distances_device", "aco_compute_nn_lists_device",
 ]
 
 
@@ -62,7 +62,7 @@ class AcoParams(ctypes.Structure):
         ("max_iteration", ctypes.c_int), ("max_runtime", ctypes.c_float), ("ls_pass_limit", ctypes.c_int),
         ("record_cap", ctypes.c_int), ("device", ctypes.c_int), ("use_graph", ctypes.c_int),
         ("ants_per_block", ctypes.c_int), ("warps_per_ant", ctypes.c_int), ("ls_warps", ctypes.c_int),
-        ("stage_matrix", ctypes.c_int),
+        ("stage_matrix", ctypes.c_int), ("host_prep", ctypes.c_int),
     ]
 
 
@@ -144,6 +144,8 @@ def lib() -> ctypes.CDLL:
         L.aco_batch_set_prior.argtypes = [vp, ip, vp, ip]
         L.aco_last_cuda_error.argtypes = []
         L.aco_last_cuda_error.restype = ctypes.c_char_p
+        L.aco_compute_distances_device.argtypes = [ip, vp, vp, ip, vp, ip, vp]
+        L.aco_compute_nn_lists_device.argtypes = [ip, vp, ip, ip, ip, vp, ctypes.POINTER(ip), vp]
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
         _lib = L
     return _lib

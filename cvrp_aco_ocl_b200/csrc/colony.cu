@@ -64,16 +64,31 @@ int prep_instance(const InstanceSpec &sp, const aco_params &p, InstHost &ih)
     ih.capacity = sp.capacity;
     ih.max_dist = sp.max_dist;
     ih.serv_time = sp.serv_time;
-    ih.dist.resize((size_t)n * n);
-    if (sp.dist) std::memcpy(ih.dist.data(), sp.dist, sizeof(float) * (size_t)n * n);
-    else compute_distances(n, sp.x, sp.y, sp.dist_type, ih.dist.data());
     ih.demand.assign(sp.demand, sp.demand + n);
+    ih.device_prep = !sp.dist && !p.host_prep && device_dist_supported(sp.dist_type) && nn_rows_per_cta(n) >= 1;
+    ih.x = sp.x;
+    ih.y = sp.y;
+    ih.dist_type = sp.dist_type;
+    if (!ih.device_prep) {
+        ih.dist.resize((size_t)n * n);
+        if (sp.dist) std::memcpy(ih.dist.data(), sp.dist, sizeof(float) * (size_t)n * n);
+        else compute_distances(n, sp.x, sp.y, sp.dist_type, ih.dist.data());
+    }
     for (int i = 1; i < n; i++) { // a customer nobody can serve makes construct loop forever (kernel.cl:438,461)
         if (ih.demand[i] > ih.capacity) return ACO_ERR_INFEASIBLE;
-        const float reach = (0.0f + (ih.dist[i] + ih.serv_time)) + ih.dist[(size_t)i * n];
+        if (std::isinf(ih.max_dist) && ih.max_dist > 0) continue;
+        const float d0i = ih.device_prep ? point_distance(sp.x, sp.y, sp.dist_type, 0, i) : ih.dist[i];
+        const float di0 = ih.device_prep ? point_distance(sp.x, sp.y, sp.dist_type, i, 0) : ih.dist[(size_t)i * n];
+        const float reach = (0.0f + (d0i + ih.serv_time)) + di0;
         if (!(reach <= ih.max_dist)) return ACO_ERR_INFEASIBLE;
     }
-    ih.depth = compute_nn_lists(n, ih.dist.data(), ih.nn_ls, ih.K, ih.nn);
+    if (ih.device_prep) {
+        int depth = std::max(ih.nn_ls, ih.K);
+        if (depth >= n) depth = n - 1;
+        ih.depth = std::max(depth, 0);
+    } else {
+        ih.depth = compute_nn_lists(n, ih.dist.data(), ih.nn_ls, ih.K, ih.nn);
+    }
     return ACO_OK;
 }
 
@@ -218,7 +233,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     };
     struct Offs {
         size_t dist, heur, tau, total, chc, dem, key, jump, adv, cand32, nn16, nnls, seeds, sol, lens, elites, succ,
-            dep, dtau, rec, nbsf, iter;
+            dep, dtau, rec, nbsf, iter, xy, nnfull;
     };
     std::vector<Offs> offs(count);
     for (int b = 0; b < count; b++) {
@@ -244,6 +259,8 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         o.rec = take((size_t)p.record_cap * sizeof(aco_record));
         o.nbsf = take(4);
         o.iter = take(4);
+        o.xy = ih.device_prep ? take((size_t)2 * ih.n4 * 4) : 0;
+        o.nnfull = ih.device_prep ? take((size_t)ih.n * std::max(1, ih.depth) * 4) : 0;
     }
     const size_t o_status = take(4), o_t0 = take(8), o_queue = take(4);
     total_ants = 0;
@@ -287,6 +304,10 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         ih.succ_d = (int *)(base + o.succ); ih.dep_d = (uint32_t *)(base + o.dep);
         ih.dtau_d = (float *)(base + o.dtau); ih.rec_d = (aco_record *)(base + o.rec);
         ih.nbsf_d = (int *)(base + o.nbsf); ih.iter_d = (int *)(base + o.iter);
+        if (ih.device_prep) {
+            ih.xy_d = (float *)(base + o.xy);
+            ih.nnfull_d = (int *)(base + o.nnfull);
+        }
     }
     status_d = (int *)(base + o_status);
     t0_d_ = (unsigned long long *)(base + o_t0);
@@ -403,11 +424,23 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     for (int b = 0; b < count; b++) {
         InstHost &ih = inst[b];
         const int n = ih.n;
-        ok = ok && cudaMemcpy2DAsync(ih.dist_d, (size_t)ih.ld * 4, ih.dist.data(), (size_t)n * 4, (size_t)n * 4, n,
-                                     cudaMemcpyHostToDevice, st) == cudaSuccess;
         std::vector<int> dem4(ih.n4, 0);
         std::copy(ih.demand.begin(), ih.demand.end(), dem4.begin());
         up(ih.dem_d, dem4.data(), dem4.size() * 4);
+        if (ih.device_prep) { // distances, lists and tables on the device (prep.cu)
+            up(ih.xy_d, ih.x, (size_t)n * 4);
+            up(ih.xy_d + ih.n4, ih.y, (size_t)n * 4);
+            ok = ok && launch_dist(n, ih.xy_d, ih.xy_d + ih.n4, ih.dist_type, ih.dist_d, ih.ld, sm_count, st) ==
+                           cudaSuccess;
+            if (ih.depth > 0) {
+                ok = ok && launch_nn(n, ih.dist_d, ih.ld, ih.depth, ih.nnfull_d, status_d, st) == cudaSuccess;
+                ok = ok && launch_tables(n, ih.nnfull_d, ih.depth, ih.K, ih.Kp, ih.nn_ls, ih.dem_d, ih.nn16_d,
+                                         ih.cand32_d, ih.nnls_d, sm_count, st) == cudaSuccess;
+            }
+        } else {
+            ok = ok && cudaMemcpy2DAsync(ih.dist_d, (size_t)ih.ld * 4, ih.dist.data(), (size_t)n * 4, (size_t)n * 4,
+                                         n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+        }
         if (!throughput) {
             const std::vector<int> prio = tournament_priority(n);
             std::vector<uint32_t> key(ih.n4, 0);
@@ -421,7 +454,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
             up(ih.jump_d, jump.data(), jump.size() * 4);
             up(ih.adv_d, adv.data(), adv.size() * 4);
         }
-        if (ih.K > 0) {
+        if (ih.K > 0 && !ih.device_prep) {
             std::vector<uint16_t> nn16((size_t)n * ih.Kp, 0);
             std::vector<uint32_t> cand32((size_t)n * ih.Kp, 0); // padding entries: node 0 (always visited)
             for (int i = 0; i < n; i++)
@@ -433,10 +466,12 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
             up(ih.nn16_d, nn16.data(), nn16.size() * 2);
             up(ih.cand32_d, cand32.data(), cand32.size() * 4);
         }
-        std::vector<int> nnls((size_t)n * std::max(1, ih.nn_ls), 0);
-        for (int i = 0; i < n; i++)
-            for (int j = 0; j < ih.nn_ls; j++) nnls[(size_t)i * ih.nn_ls + j] = ih.nn[(size_t)i * ih.depth + j];
-        up(ih.nnls_d, nnls.data(), nnls.size() * 4);
+        if (!ih.device_prep) {
+            std::vector<int> nnls((size_t)n * std::max(1, ih.nn_ls), 0);
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < ih.nn_ls; j++) nnls[(size_t)i * ih.nn_ls + j] = ih.nn[(size_t)i * ih.depth + j];
+            up(ih.nnls_d, nnls.data(), nnls.size() * 4);
+        }
         std::vector<int> seeds((size_t)ih.A * ih.nloc);
         int rs = p.rnd_seed + b; // instance b of a batch: rnd_seed + b
         make_seeds(p.seed_time, &rs, ih.A, ih.nloc, seeds.data());
@@ -480,10 +515,12 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     rc = run_rows(ROW_HEUR, 0.f);
     if (rc != ACO_OK) return rc;
     CK(cudaStreamSynchronize(st));
-    for (InstHost &ih : inst) { // the host copies of the lists are no longer needed
+    for (InstHost &ih : inst) { // the host copies are no longer needed
         std::vector<int>().swap(ih.nn);
+        std::vector<float>().swap(ih.dist);
+        ih.x = ih.y = nullptr;
     }
-    return ACO_OK;
+    return sync_status();
 }
 
 int Colony::run_rows(int mode, float trail)

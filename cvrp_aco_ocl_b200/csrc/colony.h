@@ -35,6 +35,9 @@ struct InstHost {
     int capacity = 0;
     float max_dist = 0, serv_time = 0;
     bool smat = false, packed = false, gtab = false;
+    bool device_prep = false;              // distances and lists computed on the device
+    const float *x = nullptr, *y = nullptr; // caller's coordinates (valid during create)
+    int dist_type = 0;
     std::vector<float> dist; // n*n
     std::vector<int> demand;
     std::vector<int> nn;     // n x depth
@@ -45,6 +48,8 @@ struct InstHost {
     int *succ_d = nullptr, *nbsf_d = nullptr, *iter_d = nullptr;
     uint32_t *key_d = nullptr, *jump_d = nullptr, *adv_d = nullptr, *cand32_d = nullptr, *dep_d = nullptr;
     uint16_t *nn16_d = nullptr;
+    float *xy_d = nullptr; // device preprocessing: coordinates, then full lists (n x depth)
+    int *nnfull_d = nullptr;
     float *lens_d = nullptr, *dtau_d = nullptr;
     aco_record *rec_d = nullptr;
 };

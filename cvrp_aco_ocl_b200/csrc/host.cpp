@@ -180,6 +180,16 @@ int d_att(const float *x, const float *y, int i, int j)
 }
 } // namespace
 
+float point_distance(const float *x, const float *y, int dist_type, int i, int j)
+{
+    switch (dist_type) {
+    case ACO_DIST_CEIL_2D: return (float)d_ceil(x, y, i, j);
+    case ACO_DIST_GEO: return (float)d_geo(x, y, i, j);
+    case ACO_DIST_ATT: return (float)d_att(x, y, i, j);
+    default: return d_euc(x, y, i, j);
+    }
+}
+
 void compute_distances(int n, const float *x, const float *y, int dist_type, float *dist)
 {
     for (int i = 0; i < n; i++) {

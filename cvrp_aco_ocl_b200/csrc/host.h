@@ -29,6 +29,8 @@ int read_vrplib(const char *path, VrpFile &out, std::string &err);
 
 // compute_distances (vrpHelper.cpp:160-184).
 void compute_distances(int n, const float *x, const float *y, int dist_type, float *dist);
+// One entry of that matrix.
+float point_distance(const float *x, const float *y, int dist_type, int i, int j);
 
 // compute_nn_lists (vrpHelper.cpp:188-236); returns the depth actually used.
 int compute_nn_lists(int n, const float *dist, int nn_ls, int nn_ants, std::vector<int> &nn);

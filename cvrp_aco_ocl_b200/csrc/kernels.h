@@ -131,4 +131,13 @@ size_t construct_nn_smem(int n, int K, int Kp, int ants_per_cta, bool stage_tota
                          bool global_table = false);
 size_t local_search_smem(int n, int warps);
 
+// Device preprocessing (prep.cu).
+bool device_dist_supported(int dist_type);
+size_t nn_rows_per_cta(int n);
+cudaError_t launch_dist(int n, const float *x, const float *y, int dist_type, float *dist, int ld, int sm_count,
+                        cudaStream_t st);
+cudaError_t launch_nn(int n, const float *dist, int ld, int depth, int *nn, int *status, cudaStream_t st);
+cudaError_t launch_tables(int n, const int *nn, int depth, int K, int Kp, int nn_ls, const int *demand, uint16_t *nn16,
+                          uint32_t *cand32, int *nnls, int sm_count, cudaStream_t st);
+
 } // namespace aco

@@ -1,0 +1,194 @@
+// prep.cu -- instance preprocessing on the device: the distance matrix
+// (compute_distances, vrpHelper.cpp:160-184, with the per-type formulas of
+// vrpHelper.cpp:35-158) and the nearest-neighbour lists (compute_nn_lists,
+// vrpHelper.cpp:188-236, sorted by utilities.cpp:246-266), bit-identical to
+// the host versions in host.cpp.
+//
+// Distances: EUC_2D, CEIL_2D and ATT use only correctly rounded operations
+// (fp32 products and sums, fp32 or fp64 square root and division), so the
+// device reproduces the host bits.  GEO goes through cos/acos, whose last bits
+// differ between math libraries; it stays on the host.
+//
+// Lists: one thread per row runs the reference's quicksort (middle pivot
+// swapped to the left end, Lomuto partition with strict <, both halves
+// recursed) on its row in shared memory.  Only positions below the list depth
+// are needed, so ranges starting at or beyond it are skipped; the ranges are
+// disjoint, so the order they are processed in does not matter and the
+// smaller one goes first (explicit stack of at most log2(n) + 1 entries).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "../../include/cvrp_aco.h"
+#include "kernels.h"
+
+namespace aco {
+namespace {
+
+__device__ __forceinline__ float dist_of(const float *x, const float *y, int type, int i, int j)
+{
+    const float dx = __fsub_rn(x[i], x[j]), dy = __fsub_rn(y[i], y[j]);
+    const float s = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+    if (type == ACO_DIST_CEIL_2D) return (float)(int)ceilf(__fsqrt_rn(s));
+    if (type == ACO_DIST_ATT) {
+        const float r = (float)__dsqrt_rn(__ddiv_rn((double)s, 10.0));
+        const float t = (float)(int)r;
+        return (float)(t < r ? (int)t + 1 : (int)t);
+    }
+    return __fsqrt_rn(s);
+}
+
+__global__ void dist_kernel(int n, const float *x, const float *y, int type, float *dist, int ld)
+{
+    const size_t total = (size_t)n * n;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / n), j = (int)(e - (size_t)i * n);
+        dist[(size_t)i * ld + j] = dist_of(x, y, type, i, j);
+    }
+}
+
+constexpr int kStack = 40;
+
+__global__ void nn_kernel(int n, const float *dist, int ld, int depth, int rows_per_cta, int *nn, int *status)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int row = blockIdx.x * rows_per_cta + threadIdx.x;
+    if (threadIdx.x >= rows_per_cta || row >= n) return;
+    float *v = reinterpret_cast<float *>(sm) + (size_t)threadIdx.x * 2 * n;
+    int *idx = reinterpret_cast<int *>(v + n);
+    for (int i = 0; i < n; i++) {
+        v[i] = dist[(size_t)row * ld + i];
+        idx[i] = i;
+    }
+    v[row] = __int_as_float(0x7f800000); // the node itself and the depot never make the list
+    v[0] = __int_as_float(0x7f800000);
+    int sl[kStack], sr[kStack], top = 0;
+    sl[0] = 0;
+    sr[0] = n - 1;
+    top = 1;
+    while (top > 0) {
+        top--;
+        const int l = sl[top], r = sr[top];
+        if (l >= r || l >= depth) continue;
+        const int m = (l + r) / 2;
+        float tv = v[l]; v[l] = v[m]; v[m] = tv;
+        int ti = idx[l]; idx[l] = idx[m]; idx[m] = ti;
+        int last = l;
+        const float pv = v[l];
+        for (int k = l + 1; k <= r; k++)
+            if (v[k] < pv) {
+                ++last;
+                tv = v[last]; v[last] = v[k]; v[k] = tv;
+                ti = idx[last]; idx[last] = idx[k]; idx[k] = ti;
+            }
+        tv = v[l]; v[l] = v[last]; v[last] = tv;
+        ti = idx[l]; idx[l] = idx[last]; idx[last] = ti;
+        // ranges [l, last] and [last+1, r]: push the larger first
+        const bool left_small = (last - l) <= (r - last - 1);
+        if (top + 2 > kStack) { // cannot happen (depth <= log2(n) + 1); report rather than overflow
+            if (status) atomicCAS(status, 0, ACO_ERR_CAPACITY);
+            return;
+        }
+        if (left_small) {
+            sl[top] = last + 1; sr[top] = r; top++;
+            sl[top] = l; sr[top] = last; top++;
+        } else {
+            sl[top] = l; sr[top] = last; top++;
+            sl[top] = last + 1; sr[top] = r; top++;
+        }
+    }
+    for (int i = 0; i < depth; i++) nn[(size_t)row * depth + i] = idx[i];
+}
+
+// Candidate and 2-opt tables from the lists: nn16 / cand32 (first K, padded
+// with node 0 to Kp) and the 2-opt list (first nn_ls).
+__global__ void tables_kernel(int n, const int *nn, int depth, int K, int Kp, int nn_ls, const int *demand,
+                              uint16_t *nn16, uint32_t *cand32, int *nnls)
+{
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * Kp + n * nn_ls; e += gridDim.x * blockDim.x) {
+        if (e < n * Kp) {
+            const int i = e / Kp, j = e - i * Kp;
+            const int c = j < K ? nn[(size_t)i * depth + j] : 0;
+            nn16[e] = (uint16_t)c;
+            cand32[e] = (uint32_t)c | ((uint32_t)(demand[c] & 0xFFFF) << 16);
+        } else {
+            const int f = e - n * Kp, i = f / nn_ls, j = f - i * nn_ls;
+            nnls[f] = nn[(size_t)i * depth + j];
+        }
+    }
+}
+
+} // namespace
+
+bool device_dist_supported(int dist_type) { return dist_type != ACO_DIST_GEO; }
+
+size_t nn_rows_per_cta(int n)
+{
+    const size_t per_row = (size_t)8 * n;
+    size_t rows = (size_t)(200 * 1024) / per_row;
+    return std::min<size_t>(rows, 32);
+}
+
+cudaError_t launch_dist(int n, const float *x, const float *y, int dist_type, float *dist, int ld, int sm_count,
+                        cudaStream_t st)
+{
+    const size_t total = (size_t)n * n;
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)sm_count * 16);
+    dist_kernel<<<std::max(blocks, 1), 256, 0, st>>>(n, x, y, dist_type, dist, ld);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nn(int n, const float *dist, int ld, int depth, int *nn, int *status, cudaStream_t st)
+{
+    const int rows = (int)nn_rows_per_cta(n);
+    if (rows < 1) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)rows * 8 * n;
+    cudaError_t e = cudaFuncSetAttribute(nn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    nn_kernel<<<(n + rows - 1) / rows, 32, smem, st>>>(n, dist, ld, depth, rows, nn, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tables(int n, const int *nn, int depth, int K, int Kp, int nn_ls, const int *demand, uint16_t *nn16,
+                          uint32_t *cand32, int *nnls, int sm_count, cudaStream_t st)
+{
+    const int total = n * Kp + n * nn_ls;
+    const int blocks = std::max(1, std::min((total + 255) / 256, sm_count * 8));
+    tables_kernel<<<blocks, 256, 0, st>>>(n, nn, depth, K, Kp, nn_ls, demand, nn16, cand32, nnls);
+    return cudaGetLastError();
+}
+
+} // namespace aco
+
+using namespace aco;
+
+extern "C" {
+
+int aco_compute_distances_device(int n, const float *x, const float *y, int dist_type, float *dist, int ld,
+                                 void *stream)
+{
+    if (n < 1 || !x || !y || !dist || ld < n || !device_dist_supported(dist_type)) return ACO_ERR_INVALID;
+    int dev = 0, sm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+    return launch_dist(n, x, y, dist_type, dist, ld, sm, static_cast<cudaStream_t>(stream)) == cudaSuccess
+               ? ACO_OK
+               : ACO_ERR_CUDA;
+}
+
+int aco_compute_nn_lists_device(int n, const float *dist, int ld, int nn_ls, int nn_ants, int *nn, int *depth,
+                                void *stream)
+{
+    if (n < 2 || !dist || !depth || ld < n || nn_rows_per_cta(n) < 1) return ACO_ERR_INVALID;
+    int d = nn_ls >= nn_ants ? nn_ls : nn_ants;
+    if (d >= n) d = n - 1;
+    if (d < 0) d = 0;
+    *depth = d;
+    if (d == 0) return ACO_OK;
+    if (!nn) return ACO_ERR_INVALID;
+    return launch_nn(n, dist, ld, d, nn, nullptr, static_cast<cudaStream_t>(stream)) == cudaSuccess ? ACO_OK
+                                                                                                     : ACO_ERR_CUDA;
+}
+
+} // extern "C"

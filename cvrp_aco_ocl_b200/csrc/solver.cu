@@ -64,6 +64,7 @@ int check_params(const aco_params &p, int n)
     if (p.ants_per_block < 0 || p.ants_per_block > 16) return ACO_ERR_INVALID;
     if (p.ls_warps < 0 || p.ls_warps > 32) return ACO_ERR_INVALID;
     if (p.stage_matrix < -1 || p.stage_matrix > 0) return ACO_ERR_INVALID;
+    if (p.host_prep < 0 || p.host_prep > 1) return ACO_ERR_INVALID;
     if (!(p.rho > 0.0f && p.rho <= 1.0f)) return ACO_ERR_INVALID;
     if (p.n_ants > 56 * 1024) return ACO_ERR_INVALID; // the statistics kernel holds n_ants lengths in shared memory
     return ACO_OK;

@@ -90,6 +90,8 @@ typedef struct aco_params {
     int ls_warps;         /* 0 = autotuned; else warps per 2-opt CTA (1..32, one route per warp at a time) */
     int stage_matrix;     /* throughput construct: 0 = stage the whole total_info matrix in shared memory when
                              it fits (used by the no-candidate fallback); -1 = never, rows are read through L2 */
+    int host_prep;        /* 0 = distances and neighbour lists computed on the device when the distance type
+                             allows (all but GEO; bit-identical to the host); 1 = on the host */
 } aco_params;
 
 /* One best-so-far record {iteration, length, seconds since init} (problem.h:62-66). */
@@ -117,6 +119,15 @@ int aco_compute_distances(int n, const float *x, const float *y, int dist_type, 
 /* compute_nn_lists (vrpHelper.cpp:188-236, sort2 tie order utilities.cpp:246-266):
  * depth = min(max(nn_ls, nn_ants), n-1) entries per node, written to nn (n*depth). */
 int aco_compute_nn_lists(int n, const float *dist, int nn_ls, int nn_ants, int *nn, int *depth);
+/* The same two steps on the device (device pointers; no reference counterpart as an
+ * entry point): distances into an n x ld matrix (EUC_2D, CEIL_2D, ATT; GEO is
+ * ACO_ERR_INVALID because its cos/acos bits depend on the math library), and
+ * the lists (n x depth, depth = min(max(nn_ls, nn_ants), n-1)) from an n x ld
+ * matrix, in the reference's quicksort tie order.  Both only enqueue work. */
+int aco_compute_distances_device(int n, const float *x, const float *y, int dist_type, float *dist, int ld,
+                                 void *stream);
+int aco_compute_nn_lists_device(int n, const float *dist, int ld, int nn_ls, int nn_ants, int *nn, int *depth,
+                                void *stream);
 
 /* check_solution (problem.cpp:226-319): 1 valid, 0 invalid, <0 error. */
 int aco_check_solution(const aco_instance *inst, const int *tour, int tour_size);
