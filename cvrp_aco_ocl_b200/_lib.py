@@ -36,7 +36,8 @@ EXPORTED = [
     "aco_batch_get_solutions", "aco_batch_get_pheromone", "aco_batch_time_phases", "aco_batch_get_stream",
     "aco_batch_destroy", "aco_autotune", "aco_batch_autotune", "aco_mpnn_param_count", "aco_mpnn_workspace_bytes",
     "aco_mpnn_forward", "aco_mpnn_grad", "aco_mpnn_adam", "aco_mpnn_status", "aco_set_prior", "aco_batch_set_prior",
-    "aco_last_cuda_error", "aco_compute_distances_device", "aco_compute_nn_lists_device",
+    "aco_last_cuda_error", "aco_compute_distances_device", "aco_compute_nn_lists_device", "aco_validate",
+    "aco_write_solution", "aco_batch_validate", "aco_batch_write_solutions", "aco_batch_get_bsf_records",
 ]
 
 
@@ -146,6 +147,11 @@ def lib() -> ctypes.CDLL:
         L.aco_last_cuda_error.restype = ctypes.c_char_p
         L.aco_compute_distances_device.argtypes = [ip, vp, vp, ip, vp, ip, vp]
         L.aco_compute_nn_lists_device.argtypes = [ip, vp, ip, ip, ip, vp, ctypes.POINTER(ip), vp]
+        L.aco_validate.argtypes = [vp, vp, ctypes.POINTER(ip)]
+        L.aco_write_solution.argtypes = [vp, ctypes.c_char_p]
+        L.aco_batch_validate.argtypes = [vp, vp, ctypes.POINTER(ip)]
+        L.aco_batch_write_solutions.argtypes = [vp, ctypes.c_char_p]
+        L.aco_batch_get_bsf_records.argtypes = [vp, ip, vp, ip, ctypes.POINTER(ip)]
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
         _lib = L
     return _lib

@@ -288,6 +288,18 @@ class Solver:
                   "aco_get_bsf_records")
         return [(arr[i].iter, arr[i].length, arr[i].time) for i in range(k)]
 
+    def validate(self) -> Tuple[np.ndarray, int]:
+        """Device check of every tour slot (ants, then best-so-far): flags (1 =
+        valid) and the number of invalid slots."""
+        flags = np.zeros(self.A + 1, np.int32)
+        bad = ctypes.c_int()
+        check(lib().aco_validate(self.h, ptr(flags), ctypes.byref(bad)), "aco_validate")
+        return flags, bad.value
+
+    def write_solution(self, path: str) -> None:
+        """The best-so-far tour in print_solution_to_file's block format."""
+        check(lib().aco_write_solution(self.h, path.encode()), "aco_write_solution")
+
     def set_prior(self, prior=None):
         """heur = eta^beta * prior (n x n, finite, >= 0); None restores eta^beta."""
         if prior is None:
@@ -412,6 +424,27 @@ class Batch:
         ms = np.zeros(4, np.float32)
         check(lib().aco_batch_time_phases(self.h, n_iter, ptr(ms)), "aco_batch_time_phases")
         return ms
+
+    def validate(self) -> Tuple[np.ndarray, int]:
+        """Device check of every tour of every instance: invalid slots per
+        instance and in total."""
+        inv = np.zeros(len(self.problems), np.int32)
+        bad = ctypes.c_int()
+        check(lib().aco_batch_validate(self.h, ptr(inv), ctypes.byref(bad)), "aco_batch_validate")
+        return inv, bad.value
+
+    def write_solutions(self, path: str) -> None:
+        check(lib().aco_batch_write_solutions(self.h, path.encode()), "aco_batch_write_solutions")
+
+    def records(self, b: int) -> List[Tuple[int, float, float]]:
+        cnt = ctypes.c_int()
+        check(lib().aco_batch_get_bsf_records(self.h, b, None, 0, ctypes.byref(cnt)), "aco_batch_get_bsf_records")
+        k = cnt.value
+        arr = (AcoRecord * max(k, 1))()
+        if k:
+            check(lib().aco_batch_get_bsf_records(self.h, b, ctypes.cast(arr, ctypes.c_void_p), k, ctypes.byref(cnt)),
+                  "aco_batch_get_bsf_records")
+        return [(arr[i].iter, arr[i].length, arr[i].time) for i in range(k)]
 
     def set_prior(self, b: int, prior=None):
         """Prior of instance b (see Solver.set_prior)."""

@@ -273,6 +273,8 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     }
     const size_t o_ant_inst = take((size_t)total_ants * 4), o_ant_base = take((size_t)(count + 1) * 4);
     const size_t o_row_base = take((size_t)(count + 1) * 4), o_zero_base = take(16);
+    const size_t o_slot_base = take((size_t)(count + 1) * 4), o_valid = take((size_t)(total_ants + count) * 4);
+    const size_t o_invalid = take((size_t)count * 4);
     const size_t o_cargs = take(sizeof(ConstructArgs) * count), o_largs = take(sizeof(LocalSearchArgs) * count);
     const size_t o_sargs = take(sizeof(StatsArgs) * count), o_uargs = take(sizeof(UpdateArgs) * count);
     // construct work items {instance, first ant}, larger instances first
@@ -316,6 +318,9 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     ant_base_d_ = (int *)(base + o_ant_base);
     row_base_d_ = (int *)(base + o_row_base);
     zero_base_d_ = (int *)(base + o_zero_base); // {0}: row base of a one-instance launch
+    slot_base_d_ = (int *)(base + o_slot_base);
+    valid_d_ = (int *)(base + o_valid);
+    invalid_d_ = (int *)(base + o_invalid);
     cargs_d_ = (ConstructArgs *)(base + o_cargs);
     largs_d_ = (LocalSearchArgs *)(base + o_largs);
     sargs_d_ = (StatsArgs *)(base + o_sargs);
@@ -510,6 +515,9 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     up(ant_inst_d_, ant_inst.data(), ant_inst.size() * 4);
     up(ant_base_d_, ant_base.data(), ant_base.size() * 4);
     up(row_base_d_, row_base.data(), row_base.size() * 4);
+    slot_base_h_.assign(count + 1, 0);
+    for (int b = 0; b < count; b++) slot_base_h_[b + 1] = slot_base_h_[b] + inst[b].A + 1;
+    up(slot_base_d_, slot_base_h_.data(), slot_base_h_.size() * 4);
     up(items_d_, items.data(), items.size() * sizeof(int2));
     if (!ok) return ACO_ERR_CUDA;
     rc = run_rows(ROW_HEUR, 0.f);
@@ -559,6 +567,32 @@ int Colony::set_prior(int b, const float *prior, int ld)
     }
     if (rc == ACO_OK && initialized) rc = run_rows_one(b, ROW_TOTAL);
     if (rc != ACO_OK) return rc;
+    return sync_status();
+}
+
+int Colony::validate(int *flags, int *invalid_per_inst, int *n_invalid)
+{
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    const int count = (int)inst.size();
+    int a_max = 0, n_max = 0;
+    for (const InstHost &ih : inst) {
+        a_max = std::max(a_max, ih.A);
+        n_max = std::max(n_max, ih.n);
+    }
+    CK(cudaMemsetAsync(invalid_d_, 0, sizeof(int) * count, st));
+    CK(launch_validate(cargs_d_, count, a_max + 1, n_max, valid_d_, slot_base_d_, invalid_d_, st));
+    std::vector<int> inv(count);
+    CK(cudaMemcpyAsync(inv.data(), invalid_d_, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+    if (flags)
+        CK(cudaMemcpyAsync(flags, valid_d_, sizeof(int) * slot_base_h_[count], cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    long long total = 0;
+    for (int b = 0; b < count; b++) {
+        total += inv[b];
+        if (invalid_per_inst) invalid_per_inst[b] = inv[b];
+    }
+    if (n_invalid) *n_invalid = (int)total;
     return sync_status();
 }
 

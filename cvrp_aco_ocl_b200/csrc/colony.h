@@ -73,6 +73,9 @@ public:
     // heur = eta^beta * prior for instance b (prior: n x n host array, row stride ld;
     // null restores eta^beta); total_info follows when the colony is initialised
     int set_prior(int b, const float *prior, int ld);
+    // Check every tour slot on the device; flags (total slots, or null) and
+    // per-instance invalid counts (or null) are copied back.
+    int validate(int *flags, int *invalid_per_inst, int *n_invalid);
     int time_phases(int n_iter, float *ms4);
     int set_device() const;
 
@@ -107,6 +110,8 @@ private:
     int2 *items_d_ = nullptr;
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
     int *row_base_d_ = nullptr, *zero_base_d_ = nullptr;
+    int *slot_base_d_ = nullptr, *valid_d_ = nullptr, *invalid_d_ = nullptr;
+    std::vector<int> slot_base_h_;
     ConstructArgs *cargs_d_ = nullptr;
     LocalSearchArgs *largs_d_ = nullptr;
     StatsArgs *sargs_d_ = nullptr;

@@ -131,6 +131,12 @@ size_t construct_nn_smem(int n, int K, int Kp, int ants_per_cta, bool stage_tota
                          bool global_table = false);
 size_t local_search_smem(int n, int warps);
 
+// Tour validation (validate.cu): flags[slot_base[b] + s] = 1 if slot s of
+// instance b (ants, then best-so-far) is a valid tour whose stored length is
+// exact; invalid[b] counts the others (zeroed by the caller).
+cudaError_t launch_validate(const ConstructArgs *d_args, int n_inst, int max_slots, int max_n, int *flags,
+                            const int *slot_base, int *invalid, cudaStream_t st);
+
 // Device preprocessing (prep.cu).
 bool device_dist_supported(int dist_type);
 size_t nn_rows_per_cta(int n);

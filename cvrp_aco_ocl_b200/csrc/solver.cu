@@ -17,6 +17,7 @@
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -528,6 +529,48 @@ int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *
     return ACO_OK;
 }
 
+int aco_validate(aco_solver *s, int *flags, int *n_invalid)
+{
+    if (!s) return ACO_ERR_INVALID;
+    return s->c.validate(flags, nullptr, n_invalid);
+}
+
+namespace {
+// The reference's solution block (io.cpp:270-281) for one tour.
+void write_block(FILE *f, const int *tour, int size, float length)
+{
+    std::fprintf(f, "Begin Solution\n");
+    for (int i = 0; i < size; i++) std::fprintf(f, "%d ", tour[i]);
+    std::fprintf(f, "\nSolution Length %f\nEnd Solution\n", length);
+}
+
+int write_best(Colony &c, const char *path, bool batch)
+{
+    if (!path) return ACO_ERR_INVALID;
+    FILE *f = std::fopen(path, "w");
+    if (!f) return ACO_ERR_IO;
+    int rc = ACO_OK;
+    for (int b = 0; b < (int)c.inst.size() && rc == ACO_OK; b++) {
+        std::vector<int> tour(c.inst[b].T);
+        int size = 0;
+        float len = 0.f;
+        rc = copy_best(c, b, tour.data(), (int)tour.size(), &size, &len);
+        if (rc != ACO_OK) break;
+        if (batch) std::fprintf(f, "Instance %d\n", b);
+        write_block(f, tour.data(), size, len);
+    }
+    if (std::fclose(f) != 0 && rc == ACO_OK) rc = ACO_ERR_IO;
+    return rc;
+}
+} // namespace
+
+int aco_write_solution(aco_solver *s, const char *path)
+{
+    if (!s) return ACO_ERR_INVALID;
+    if (s->c.set_device() != ACO_OK) return ACO_ERR_CUDA;
+    return write_best(s->c, path, false);
+}
+
 int aco_set_prior(aco_solver *s, const float *prior, int ld)
 {
     if (!s) return ACO_ERR_INVALID;
@@ -624,6 +667,26 @@ int aco_batch_time_phases(aco_batch *b, int n_iter, float *ms4)
 {
     if (!b || !ms4 || n_iter <= 0) return ACO_ERR_INVALID;
     return b->c.time_phases(n_iter, ms4);
+}
+
+int aco_batch_validate(aco_batch *b, int *invalid_per_instance, int *n_invalid)
+{
+    if (!b) return ACO_ERR_INVALID;
+    return b->c.validate(nullptr, invalid_per_instance, n_invalid);
+}
+
+int aco_batch_write_solutions(aco_batch *b, const char *path)
+{
+    if (!b) return ACO_ERR_INVALID;
+    if (b->c.set_device() != ACO_OK) return ACO_ERR_CUDA;
+    return write_best(b->c, path, true);
+}
+
+int aco_batch_get_bsf_records(aco_batch *b, int idx, aco_record *out, int cap, int *count)
+{
+    if (!b || idx < 0 || idx >= (int)b->c.inst.size()) return ACO_ERR_INVALID;
+    if (b->c.set_device() != ACO_OK) return ACO_ERR_CUDA;
+    return copy_records(b->c, idx, out, cap, count);
 }
 
 int aco_batch_set_prior(aco_batch *b, int idx, const float *prior, int ld)

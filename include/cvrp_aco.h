@@ -205,6 +205,21 @@ int aco_time_phases(aco_solver *s, int n_iter, float *ms4);
  * in construct, bit 1: NN lists in 2-opt). */
 int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *staging_flags);
 
+/* ---- validation and output -------------------------------------------------
+ * aco_validate checks every tour slot (ants and best-so-far) on the device with
+ * check_solution's rules (problem.cpp:226-319: starts at the depot, every
+ * customer exactly once, every route non-empty, within capacity and
+ * max_distance) plus node-id range checks and an exact check of the stored
+ * length against the fp32 sum of the tour's edges (compute_tour_length,
+ * vrpHelper.cpp:244-253).  flags (A+1 ints, or NULL): 1 = valid.  The batch
+ * form counts invalid slots per instance (count ints, or NULL).
+ * aco_write_solution writes the best-so-far tour as print_solution_to_file
+ * does (io.cpp:270-281: "Begin Solution", the tour, "Solution Length %f",
+ * "End Solution"); the batch form writes one such block per instance, each
+ * after a line "Instance <index>". */
+int aco_validate(aco_solver *s, int *flags, int *n_invalid);
+int aco_write_solution(aco_solver *s, const char *path);
+
 /* ---- autotuner (no reference counterpart) -----------------------------------
  * Times launch configurations on the instance(s) and returns the fastest in
  * *out (a copy of *p with ants_per_block, ls_warps, stage_matrix -- and
@@ -282,6 +297,9 @@ int aco_mpnn_status(void *workspace, void *stream);
  * choice rule: use it with ACO_MODE_THROUGHPUT. */
 int aco_set_prior(aco_solver *s, const float *prior, int ld);
 int aco_batch_set_prior(aco_batch *b, int idx, const float *prior, int ld);
+int aco_batch_validate(aco_batch *b, int *invalid_per_instance, int *n_invalid);
+int aco_batch_write_solutions(aco_batch *b, const char *path);
+int aco_batch_get_bsf_records(aco_batch *b, int idx, aco_record *out, int cap, int *count);
 
 /* ---- pheromone update without allocation ---------------------------------
  * No counterpart in the reference.  For callers that cannot let this library
