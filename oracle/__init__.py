@@ -77,6 +77,9 @@ def lib():
         L.orc_compute_distances.argtypes = [ctypes.c_int, _f32p, _f32p, ctypes.c_int, _f32p]
         L.orc_compute_nn_lists.argtypes = [ctypes.c_int, _f32p, ctypes.c_int, ctypes.c_int, _i32p]
         L.orc_compute_nn_lists.restype = ctypes.c_int
+        L.orc_swap.argtypes = [ctypes.c_int, _f32p, _i32p, ctypes.c_int, ctypes.c_float, ctypes.c_float, _i32p,
+                               ctypes.c_int, ctypes.c_int]
+        L.orc_swap.restype = ctypes.c_int
         L.orc_tour_length.argtypes = [ctypes.c_int, _f32p, _i32p, ctypes.c_int]
         L.orc_tour_length.restype = ctypes.c_float
         L.orc_tour_length_f64.argtypes = [ctypes.c_int, _f32p, _i32p, ctypes.c_int]
@@ -283,6 +286,7 @@ def ref_lib():
         L.ref_read.restype = ctypes.c_long
         L.ref_problem_info.argtypes = [_i32p]
         L.ref_host_check_solution.argtypes = [_i32p, ctypes.c_int]
+        L.ref_swap.argtypes = [ctypes.c_char_p, _i32p, ctypes.c_int]
         L.ref_read_instance.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                         _f32p, _f32p, _i32p, _f32p, _i32p, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
@@ -355,3 +359,21 @@ def ref_read_instance(vrp_path: str, cap_nodes: int = 2048):
     return dict(n=N, capacity=cap.value, x=x[:N].copy(), y=y[:N].copy(), demand=dem[:N].copy(),
                 dist=dist[: N * N].reshape(N, N).copy(), nn=nn[: N * D].reshape(N, D).copy(),
                 optimum=opt.value, max_distance=md.value, service_time=st.value)
+
+
+def swap(dist, demand, capacity: int, tour, max_dist: float = math.inf, serv_time: float = 0.0,
+         max_swaps: int = 0):
+    """LocalSearch::swap restated (orc_swap) on a copy of `tour`: (tour, swaps)."""
+    d = np.ascontiguousarray(dist, np.float32)
+    t = np.ascontiguousarray(tour, np.int32).copy()
+    k = lib().orc_swap(d.shape[0], d.ravel(), np.ascontiguousarray(demand, np.int32), int(capacity), float(max_dist),
+                       float(serv_time), t, len(t), int(max_swaps))
+    return t, k
+
+
+def ref_swap(vrp_path: str, tour) -> np.ndarray:
+    """The reference's own LocalSearch::swap on a copy of `tour` (instance read from vrp_path)."""
+    t = np.ascontiguousarray(tour, np.int32).copy()
+    if ref_lib().ref_swap(vrp_path.encode(), t, len(t)) != 0:
+        raise RuntimeError("ref_swap failed")
+    return t

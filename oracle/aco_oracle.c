@@ -550,6 +550,89 @@ static int two_opt_single_route(const orc_state *s, int *tour, int rbeg, int ren
     return ORC_OK;
 }
 
+/* LocalSearch::swap (localSearch.cpp:301-410): first-improvement exchange of
+ * two customers, scanned i < j over tour positions; after an accepted swap the
+ * scan resumes at the same i (the reference's `i--`).  Float expressions keep
+ * the reference's evaluation order.  Returns the number of swaps applied, or
+ * -1 once more than max_swaps (> 0) were applied. */
+int orc_swap(int n, const float *dist, const int *demand, int capacity, float max_dist, float serv_time,
+             int *tour, int tour_size, int max_swaps)
+{
+    int *route_load = (int *)malloc(sizeof(int) * (size_t)(n > 1 ? n - 1 : 1));
+    float *route_dist = (float *)malloc(sizeof(float) * (size_t)(n > 1 ? n - 1 : 1));
+#define D(a, b) dist[(size_t)(a) * n + (b)]
+    int load = 0, k = 0, beg = 0, swaps = 0;
+    float dd = 0;
+    for (int i = 1; i < tour_size; i++) { /* step 1: route loads and lengths */
+        load += demand[tour[i]];
+        dd += D(tour[i - 1], tour[i]);
+        if (tour[i] == 0) {
+            route_load[k] = load;
+            route_dist[k] = dd + serv_time * (float)(i - beg - 1);
+            k++;
+            load = 0;
+            dd = 0;
+            beg = i;
+        }
+    }
+    int p1 = 0;
+    for (int i = 1; i < tour_size; i++) { /* step 2 */
+        const int n1 = tour[i];
+        if (n1 == 0) {
+            p1++;
+            continue;
+        }
+        const int p_n1 = tour[i - 1], s_n1 = tour[i + 1];
+        int p2 = p1;
+        for (int j = i + 1; j < tour_size; j++) {
+            const int n2 = tour[j];
+            if (n2 == 0) {
+                p2++;
+                continue;
+            }
+            const int p_n2 = tour[j - 1], s_n2 = tour[j + 1];
+            float gain;
+            if (j == i + 1)
+                gain = -(D(p_n1, n1) + D(n2, s_n2)) + (D(p_n1, n2) + D(n1, s_n2));
+            else
+                gain = -(D(p_n1, n1) + D(n1, s_n1) + D(p_n2, n2) + D(n2, s_n2)) +
+                       (D(p_n1, n2) + D(n2, s_n1) + D(p_n2, n1) + D(n1, s_n2));
+            if (!(gain < -EPSILON)) continue;
+            int load1, load2;
+            float dist1, dist2;
+            if (p1 != p2) {
+                load1 = route_load[p1] - demand[n1] + demand[n2];
+                load2 = route_load[p2] - demand[n2] + demand[n1];
+                dist1 = route_dist[p1] - (D(p_n1, n1) + D(n1, s_n1)) + (D(p_n1, n2) + D(n2, s_n1));
+                dist2 = route_dist[p2] - (D(p_n2, n2) + D(n2, s_n2)) + (D(p_n2, n1) + D(n1, s_n2));
+                if ((load1 > capacity || load2 > capacity) || (dist1 > max_dist || dist2 > max_dist)) continue;
+            } else {
+                load1 = route_load[p1];
+                load2 = load1;
+                dist1 = route_dist[p1] + gain;
+                dist2 = dist1;
+            }
+            tour[i] = n2;
+            tour[j] = n1;
+            route_load[p1] = load1;
+            route_load[p2] = load2;
+            route_dist[p1] = dist1;
+            route_dist[p2] = dist2;
+            if (++swaps > max_swaps && max_swaps > 0) {
+                free(route_load);
+                free(route_dist);
+                return -1;
+            }
+            i--;
+            break;
+        }
+    }
+#undef D
+    free(route_load);
+    free(route_dist);
+    return swaps;
+}
+
 static int local_search_one(const orc_state *s, int ant, ls_ws *w)
 {
     const int n = s->n, T = 2 * n;
@@ -578,7 +661,14 @@ static int local_search_one(const orc_state *s, int ant, ls_ws *w)
     }
     for (int i = 0; i < tour_size; i++) tour[i] = w->tour_wrk[i]; /* kernel.cl:530-538 */
     float len = 0;
-    for (int i = 0; i < tour_size - 1; i++) len += w->dist_tour_wrk[i];
+    if (s->ls_flag & 2) { /* second stage: swap, then compute_tour_length (localSearch.cpp:63-70) */
+        const int sw = orc_swap(n, s->dist, s->demand, s->capacity, s->max_dist, s->serv_time, tour, tour_size,
+                                ORC_SWAP_LIMIT_PER_NODE * n);
+        if (sw < 0 && ORC_ERR_LS_LIMIT < status) status = ORC_ERR_LS_LIMIT;
+        for (int i = 0; i < tour_size - 1; i++) len += s->dist[(size_t)tour[i] * n + tour[i + 1]];
+    } else {
+        for (int i = 0; i < tour_size - 1; i++) len += w->dist_tour_wrk[i];
+    }
     s->lens[ant] = len;
     return status;
 }

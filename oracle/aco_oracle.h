@@ -32,7 +32,8 @@ typedef struct orc_state {
     int capacity;
     float max_dist, serv_time;
     float alpha, beta, rho;
-    int ls_flag;          /* run 2-opt after every construct (and in the bootstrap) */
+    int ls_flag;          /* bit 0: 2-opt after every construct (and in the bootstrap);
+                             bit 1: then the inter-route swap stage (orc_swap) */
     int step_limit_passes;/* max 2-opt improvement passes per route (0 = unbounded) */
     const float *dist;    /* n*n */
     const int *demand;    /* n */
@@ -65,6 +66,11 @@ float orc_pow_rule(float x, float e);
 /* ---- hot path phases --------------------------------------------------- */
 int orc_construct(orc_state *s, int n_threads);
 int orc_local_search(orc_state *s, int n_threads);
+/* LocalSearch::swap (localSearch.cpp:301-410) on one tour; returns the number
+ * of swaps, or -1 once more than max_swaps (> 0) were applied. */
+#define ORC_SWAP_LIMIT_PER_NODE 64
+int orc_swap(int n, const float *dist, const int *demand, int capacity, float max_dist, float serv_time,
+             int *tour, int tour_size, int max_swaps);
 void orc_find_best(orc_state *s);
 void orc_update_best_so_far(orc_state *s, float time);
 void orc_get_elites(orc_state *s);

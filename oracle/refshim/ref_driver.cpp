@@ -23,6 +23,7 @@
 #define private public
 #include "gpu/g_aco.h"
 #include "gpu/g_type.h"
+#include "localSearch.h"
 #undef private
 
 extern "C" {
@@ -198,6 +199,19 @@ int ref_read_instance(const char *vrp_path, int *n_out, int *capacity_out, float
         }
     }
     return 0;
+}
+
+/* The reference's CPU inter-route swap (LocalSearch::swap, localSearch.cpp:301-410)
+ * applied in place to one tour of the instance in vrp_path (read_instance_file +
+ * init_problem; no OpenCL state involved). */
+int ref_swap(const char *vrp_path, int *tour, int tour_size)
+{
+    Problem *inst = new Problem(0);
+    read_instance_file(inst, vrp_path);
+    init_problem(inst);
+    LocalSearch ls(inst);
+    ls.swap(tour, tour_size);
+    return 0; /* inst leaked on purpose, as in ref_read_instance */
 }
 
 } /* extern "C" */

@@ -154,3 +154,58 @@ def test_check_solution_and_lengths():
         assert abs(oracle.tour_length_f64(g["dist"], tour) - g["it3_lens"][a]) < 1e-3
     bad = np.array([0, 1, 1, 0], np.int32)
     assert not oracle.check_solution(g["dist"], g["demand"], int(g["capacity"]), bad)
+
+
+def random_tours(inst, count, seed, dist=None):
+    """Valid tours: customers in random order, cut into routes greedily by
+    capacity and (given the distances) by the route-length limit."""
+    import math
+    rng = np.random.default_rng(seed)
+    md = inst.max_distance if math.isfinite(inst.max_distance) else math.inf
+    out = []
+    for _ in range(count):
+        order = rng.permutation(np.arange(1, inst.n))
+        tour, load, rlen = [0], 0, 0.0
+        for c in order:
+            d = int(inst.demand[c])
+            if dist is not None:
+                prev = tour[-1]
+                longer = rlen + dist[prev, c] + inst.service_time + dist[c, 0]
+            else:
+                longer = 0.0
+            if load + d > inst.capacity or (tour[-1] != 0 and longer > md * 0.999):
+                tour.append(0)
+                load, rlen = 0, 0.0
+            rlen += (dist[tour[-1], c] + inst.service_time) if dist is not None else 0.0
+            tour.append(int(c))
+            load += d
+        tour.append(0)
+        out.append(np.array(tour, np.int32))
+    return out
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference sources not built here")
+@pytest.mark.parametrize("seed,nc,max_distance,service", [(31, 40, None, 0.0), (32, 120, None, 0.0),
+                                                          (33, 50, 400.0, 2.0)])
+def test_swap_matches_reference_swap(tmp_path, seed, nc, max_distance, service):
+    """The oracle's swap stage against the reference's own LocalSearch::swap."""
+    import dataclasses
+    import math
+    inst = I.gen_uniform_small(seed, nc) if nc < 60 else I.gen_mixed(seed, nc)
+    if max_distance is not None:
+        inst = dataclasses.replace(inst, max_distance=max_distance, service_time=service)
+    p = str(tmp_path / "x.vrp")
+    I.write_vrplib(inst, p)
+    info = oracle.ref_read_instance(p)
+    md = inst.max_distance if math.isfinite(inst.max_distance) else math.inf
+    changed = checked = 0
+    for t in random_tours(inst, 16, seed, info["dist"]):
+        if not oracle.check_solution(info["dist"], inst.demand, inst.capacity, t, md, inst.service_time):
+            continue
+        want = oracle.ref_swap(p, t)
+        got, k = oracle.swap(info["dist"], inst.demand, inst.capacity, t, md, inst.service_time)
+        assert np.array_equal(got, want)
+        assert oracle.check_solution(info["dist"], inst.demand, inst.capacity, got, md, inst.service_time)
+        checked += 1
+        changed += int(k > 0)
+    assert checked >= 4 and changed > 0
