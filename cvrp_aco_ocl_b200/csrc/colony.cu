@@ -28,6 +28,7 @@ namespace {
 
 // 227 KB per CTA minus room for the kernels' static shared memory
 constexpr size_t kSmemBudget = 226 * 1024;
+constexpr int kSwapLimitPerNode = 64; // accepted swaps per node and tour before ACO_ERR_LS_LIMIT
 
 int exp_as_int(float e)
 {
@@ -280,6 +281,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     // construct work items {instance, first ant}, larger instances first
     // (set after cn_apc is known; sized for apc = 1)
     const size_t o_items = take((size_t)total_ants * sizeof(int2));
+    const size_t o_sw_items = take((size_t)total_ants * sizeof(int2));
 
     void *arena = nullptr;
     if (res->pool && cudaMallocFromPoolAsync(&arena, off, res->pool, st) == cudaSuccess) {
@@ -326,6 +328,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     sargs_d_ = (StatsArgs *)(base + o_sargs);
     uargs_d_ = (UpdateArgs *)(base + o_uargs);
     items_d_ = (int2 *)(base + o_items);
+    sw_items_d_ = (int2 *)(base + o_sw_items);
 
     // ---- configuration (shared-memory budgets over the largest instance)
     const bool throughput = p.mode == ACO_MODE_THROUGHPUT;
@@ -393,12 +396,22 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         ls_smem = 0;
         for (const InstHost &ih : inst) ls_smem = std::max(ls_smem, local_search_smem(ih.n, ls_warps));
     }
+    if (p.ls_flag & 2) { // swap stage: as many ants per CTA as their shared arrays allow, up to 8
+        int n_max = 0, ld_of_max = 32;
+        for (const InstHost &ih : inst)
+            if (ih.n > n_max) { n_max = ih.n; ld_of_max = ih.ld; }
+        sw_apc = 8;
+        while (sw_apc > 1 && swap_smem(n_max, ld_of_max, sw_apc) > kSmemBudget) sw_apc--;
+        sw_smem = 0;
+        for (const InstHost &ih : inst) sw_smem = std::max(sw_smem, swap_smem(ih.n, ih.ld, sw_apc));
+        if (sw_smem > kSmemBudget) return ACO_ERR_INVALID; // the tour arrays of one ant do not fit
+    }
     stats_smem = (size_t)A_max * sizeof(float);
     if (stats_smem > kSmemBudget) return ACO_ERR_INVALID; // n_ants lengths must fit in shared memory
 
     // ---- host tables and uploads
     std::vector<int> ant_inst(total_ants), ant_base(count + 1), row_base(count + 1);
-    std::vector<int2> items;
+    std::vector<int2> items, swi;
     {
         int a0 = 0, r0 = 0;
         for (int b = 0; b < count; b++) {
@@ -416,6 +429,9 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         for (int b : order)
             for (int a0 = 0; a0 < inst[b].A; a0 += cn_apc) items.push_back(make_int2(b, a0));
         n_items = (int)items.size();
+        for (int b = 0; b < count; b++)
+            for (int a0 = 0; a0 < inst[b].A; a0 += sw_apc) swi.push_back(make_int2(b, a0));
+        sw_items = (int)swi.size();
     }
     cargs_h_.resize(count);
     std::vector<LocalSearchArgs> largs(count);
@@ -519,6 +535,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     for (int b = 0; b < count; b++) slot_base_h_[b + 1] = slot_base_h_[b] + inst[b].A + 1;
     up(slot_base_d_, slot_base_h_.data(), slot_base_h_.size() * 4);
     up(items_d_, items.data(), items.size() * sizeof(int2));
+    up(sw_items_d_, swi.data(), swi.size() * sizeof(int2));
     if (!ok) return ACO_ERR_CUDA;
     rc = run_rows(ROW_HEUR, 0.f);
     if (rc != ACO_OK) return rc;
@@ -610,6 +627,7 @@ int Colony::construct()
 int Colony::local_search()
 {
     CK(launch_local_search(largs_d_, ant_inst_d_, ant_base_d_, total_ants, ls_warps, ls_smem, st));
+    if (p.ls_flag & 2) CK(launch_swap(cargs_d_, sw_items_d_, sw_items, sw_apc, sw_smem, kSwapLimitPerNode, st));
     return ACO_OK;
 }
 

@@ -94,6 +94,8 @@ public:
     int cn_apc = 1;
     size_t cn_smem = 0;
     int ls_warps = 1;
+    int sw_apc = 1, sw_items = 0; // swap stage: ants per CTA, work items
+    size_t sw_smem = 0;
     size_t ls_smem = 0, stats_smem = 0;
     int ld_max = 32, total_ants = 0, total_rows = 0, n_items = 0;
     bool fin_any = false;
@@ -107,7 +109,7 @@ private:
     void *arena_ = nullptr;
     bool pooled_ = false; // arena from the device's memory pool (freed stream-ordered)
     unsigned long long *t0_d_ = nullptr;
-    int2 *items_d_ = nullptr;
+    int2 *items_d_ = nullptr, *sw_items_d_ = nullptr;
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
     int *row_base_d_ = nullptr, *zero_base_d_ = nullptr;
     int *slot_base_d_ = nullptr, *valid_d_ = nullptr, *invalid_d_ = nullptr;

@@ -137,6 +137,12 @@ size_t local_search_smem(int n, int warps);
 cudaError_t launch_validate(const ConstructArgs *d_args, int n_inst, int max_slots, int max_n, int *flags,
                             const int *slot_base, int *invalid, cudaStream_t st);
 
+// Inter-route swap stage (swap.cu): one CTA per item {instance, first ant}
+// with `apc` ants (one warp each).
+size_t swap_smem(int n, int ld, int apc);
+cudaError_t launch_swap(const ConstructArgs *d_args, const int2 *d_items, int n_items, int apc, size_t smem,
+                        int max_swaps_per_node, cudaStream_t st);
+
 // Device preprocessing (prep.cu).
 bool device_dist_supported(int dist_type);
 size_t nn_rows_per_cta(int n);

@@ -73,7 +73,8 @@ typedef struct aco_params {
     int ras_ranks;        /* 6 (kernel.cl:12): the best-so-far ant + ras_ranks-1 iteration elites */
     int nn_ants;          /* candidate-list length for ACO_MODE_THROUGHPUT (default min(25, n-2)) */
     int nn_ls;            /* 2-opt neighbour-list depth, <= n-2 (default n-2, problem.cpp:191-193) */
-    int ls_flag;          /* 1 = 2-opt after every construction (default 1, problem.cpp:203) */
+    int ls_flag;          /* 1 = 2-opt after every construction (default 1, problem.cpp:203); 3 = 2-opt then
+                             the inter-route swap of the CPU local search (localSearch.cpp:51-81,301-410) */
     int mode;             /* ACO_MODE_* (default PARITY) */
     int nloc;             /* work-items per ant of the reference's construct kernel: maxWorkGroupSize/4
                              (g_aco.cpp:41); sets the RNG lane layout; a power of two in [32, 1024], default 256 */

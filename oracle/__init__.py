@@ -190,7 +190,7 @@ class Oracle:
         st.capacity = int(capacity)
         st.max_dist, st.serv_time = float(max_dist), float(serv_time)
         st.alpha, st.beta, st.rho = alpha, beta, rho
-        st.ls_flag = int(bool(ls_flag))
+        st.ls_flag = int(ls_flag)  # 1: 2-opt; 3: 2-opt then the swap stage
         st.step_limit_passes = int(ls_pass_limit)
         for name in ("dist", "demand", "nn_list", "tau", "total", "seeds", "solutions", "lens", "elites"):
             setattr(st, name, getattr(self, name).ctypes.data)

@@ -291,3 +291,21 @@ def test_throughput_candidate_table_in_global_memory(gpu):
         compare_state(S, O)
         S.iterate(1); O.run_iteration(throughput=True)
         compare_state(S, O)
+
+
+@pytest.mark.parametrize("mode,n_cust,A", [(MODE_PARITY, 100, 48), (MODE_THROUGHPUT, 200, 64),
+                                           (MODE_THROUGHPUT, 600, 32)])
+def test_swap_stage_vs_oracle(gpu, mode, n_cust, A):
+    """ls_flag = 3: 2-opt then the inter-route swap of the CPU local search."""
+    inst = I.gen_mixed(400 + n_cust, n_cust) if n_cust < 500 else I.gen_large(400 + n_cust, n_cust)
+    S, O = build_pair(inst, A, 256, 1796300000, 55, 3, 25, mode=mode,
+                      nn_ants=25 if mode == MODE_THROUGHPUT else 0)
+    thr = mode == MODE_THROUGHPUT
+    with S:
+        S.init(); O.init_aco(throughput=thr)
+        compare_state(S, O)
+        for _ in range(2):
+            S.iterate(1); O.run_iteration(throughput=thr)
+            compare_state(S, O)
+        flags, bad = S.validate()
+        assert bad == 0
