@@ -38,6 +38,7 @@ EXPORTED = [
     "aco_mpnn_forward", "aco_mpnn_grad", "aco_mpnn_adam", "aco_mpnn_status", "aco_set_prior", "aco_batch_set_prior",
     "aco_last_cuda_error", "aco_compute_distances_device", "aco_compute_nn_lists_device", "aco_validate",
     "aco_write_solution", "aco_batch_validate", "aco_batch_write_solutions", "aco_batch_get_bsf_records",
+    "aco_save_checkpoint", "aco_load_checkpoint", "aco_batch_save_checkpoint", "aco_batch_load_checkpoint",
 ]
 
 
@@ -152,6 +153,9 @@ def lib() -> ctypes.CDLL:
         L.aco_batch_validate.argtypes = [vp, vp, ctypes.POINTER(ip)]
         L.aco_batch_write_solutions.argtypes = [vp, ctypes.c_char_p]
         L.aco_batch_get_bsf_records.argtypes = [vp, ip, vp, ip, ctypes.POINTER(ip)]
+        for name in ("aco_save_checkpoint", "aco_load_checkpoint", "aco_batch_save_checkpoint",
+                     "aco_batch_load_checkpoint"):
+            getattr(L, name).argtypes = [vp, ctypes.c_char_p]
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
         _lib = L
     return _lib

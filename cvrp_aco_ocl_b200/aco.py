@@ -300,6 +300,13 @@ class Solver:
         """The best-so-far tour in print_solution_to_file's block format."""
         check(lib().aco_write_solution(self.h, path.encode()), "aco_write_solution")
 
+    def save_checkpoint(self, path: str) -> None:
+        check(lib().aco_save_checkpoint(self.h, path.encode()), "aco_save_checkpoint")
+
+    def load_checkpoint(self, path: str) -> None:
+        """Resume from a checkpoint of a solver with the same instance and parameters."""
+        check(lib().aco_load_checkpoint(self.h, path.encode()), "aco_load_checkpoint")
+
     def set_prior(self, prior=None):
         """heur = eta^beta * prior (n x n, finite, >= 0); None restores eta^beta."""
         if prior is None:
@@ -435,6 +442,12 @@ class Batch:
 
     def write_solutions(self, path: str) -> None:
         check(lib().aco_batch_write_solutions(self.h, path.encode()), "aco_batch_write_solutions")
+
+    def save_checkpoint(self, path: str) -> None:
+        check(lib().aco_batch_save_checkpoint(self.h, path.encode()), "aco_batch_save_checkpoint")
+
+    def load_checkpoint(self, path: str) -> None:
+        check(lib().aco_batch_load_checkpoint(self.h, path.encode()), "aco_batch_load_checkpoint")
 
     def records(self, b: int) -> List[Tuple[int, float, float]]:
         cnt = ctypes.c_int()

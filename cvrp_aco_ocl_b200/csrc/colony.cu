@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <thread>
@@ -611,6 +612,128 @@ int Colony::validate(int *flags, int *invalid_per_inst, int *n_invalid)
     }
     if (n_invalid) *n_invalid = (int)total;
     return sync_status();
+}
+
+// ---- checkpoint ---------------------------------------------------------
+// File: the magic, a header describing the colony (count, then per instance
+// n, A, nloc, mode, K, nn_ls, ras_ranks, record_cap and the fp32 bits of
+// alpha, beta, rho), then per instance its iteration counter, number of
+// best-so-far records, tau (n x n), tours and lengths (the reference layout),
+// lane seeds and records.  Integers and floats are stored in host byte order.
+namespace {
+constexpr char kMagic[8] = {'A', 'C', 'O', 'C', 'K', 'P', 'T', '1'};
+
+struct FileCloser {
+    FILE *f;
+    ~FileCloser()
+    {
+        if (f) std::fclose(f);
+    }
+};
+} // namespace
+
+static std::vector<int> checkpoint_header(const Colony &c)
+{
+    std::vector<int> h;
+    h.push_back((int)c.inst.size());
+    for (const InstHost &ih : c.inst) {
+        int a, b, r;
+        std::memcpy(&a, &c.p.alpha, 4);
+        std::memcpy(&b, &c.p.beta, 4);
+        std::memcpy(&r, &c.p.rho, 4);
+        const int v[] = {ih.n, ih.A, ih.nloc, c.p.mode, ih.K, ih.nn_ls, ih.R, c.p.record_cap, a, b, r};
+        h.insert(h.end(), v, v + sizeof(v) / sizeof(v[0]));
+    }
+    return h;
+}
+
+int Colony::save_checkpoint(const char *path)
+{
+    if (!path) return ACO_ERR_INVALID;
+    if (!initialized) return ACO_ERR_STATE;
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    rc = sync_status();
+    if (rc != ACO_OK) return rc;
+    FileCloser fc{std::fopen(path, "wb")};
+    if (!fc.f) return ACO_ERR_IO;
+    const std::vector<int> h = checkpoint_header(*this);
+    const int hn = (int)h.size();
+    bool ok = std::fwrite(kMagic, 1, 8, fc.f) == 8 && std::fwrite(&hn, 4, 1, fc.f) == 1 &&
+              std::fwrite(h.data(), 4, h.size(), fc.f) == h.size();
+    for (const InstHost &ih : inst) {
+        if (!ok) break;
+        const size_t nn = (size_t)ih.n * ih.n, ns = (size_t)ih.T * (ih.A + 1) + 1, nseed = (size_t)ih.A * ih.nloc;
+        int it = 0, nb = 0;
+        std::vector<float> tau(nn), lens(ih.A + 1);
+        std::vector<int> sol(ns), seeds(nseed);
+        std::vector<aco_record> rec(p.record_cap);
+        CK(cudaMemcpyAsync(&it, ih.iter_d, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&nb, ih.nbsf_d, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpy2DAsync(tau.data(), (size_t)ih.n * 4, ih.tau_d, (size_t)ih.ld * 4, (size_t)ih.n * 4, ih.n,
+                             cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(sol.data(), ih.sol_d, ns * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(lens.data(), ih.lens_d, lens.size() * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(seeds.data(), ih.seeds_d, nseed * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(rec.data(), ih.rec_d, rec.size() * sizeof(aco_record), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        ok = std::fwrite(&it, 4, 1, fc.f) == 1 && std::fwrite(&nb, 4, 1, fc.f) == 1 &&
+             std::fwrite(tau.data(), 4, nn, fc.f) == nn && std::fwrite(sol.data(), 4, ns, fc.f) == ns &&
+             std::fwrite(lens.data(), 4, lens.size(), fc.f) == lens.size() &&
+             std::fwrite(seeds.data(), 4, nseed, fc.f) == nseed &&
+             std::fwrite(rec.data(), sizeof(aco_record), rec.size(), fc.f) == rec.size();
+    }
+    if (!ok) return ACO_ERR_IO;
+    const int cr = std::fclose(fc.f);
+    fc.f = nullptr;
+    return cr == 0 ? ACO_OK : ACO_ERR_IO;
+}
+
+int Colony::load_checkpoint(const char *path)
+{
+    if (!path) return ACO_ERR_INVALID;
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    FileCloser fc{std::fopen(path, "rb")};
+    if (!fc.f) return ACO_ERR_IO;
+    char magic[8];
+    int hn = 0;
+    if (std::fread(magic, 1, 8, fc.f) != 8 || std::memcmp(magic, kMagic, 8) != 0) return ACO_ERR_IO;
+    const std::vector<int> want = checkpoint_header(*this);
+    if (std::fread(&hn, 4, 1, fc.f) != 1 || hn != (int)want.size()) return ACO_ERR_INVALID;
+    std::vector<int> h(hn);
+    if (std::fread(h.data(), 4, h.size(), fc.f) != h.size()) return ACO_ERR_IO;
+    if (h != want) return ACO_ERR_INVALID; // another instance set or other parameters
+    for (InstHost &ih : inst) {
+        const size_t nn = (size_t)ih.n * ih.n, ns = (size_t)ih.T * (ih.A + 1) + 1, nseed = (size_t)ih.A * ih.nloc;
+        int it = 0, nb = 0;
+        std::vector<float> tau(nn), lens(ih.A + 1);
+        std::vector<int> sol(ns), seeds(nseed);
+        std::vector<aco_record> rec(p.record_cap);
+        const bool ok = std::fread(&it, 4, 1, fc.f) == 1 && std::fread(&nb, 4, 1, fc.f) == 1 &&
+                        std::fread(tau.data(), 4, nn, fc.f) == nn && std::fread(sol.data(), 4, ns, fc.f) == ns &&
+                        std::fread(lens.data(), 4, lens.size(), fc.f) == lens.size() &&
+                        std::fread(seeds.data(), 4, nseed, fc.f) == nseed &&
+                        std::fread(rec.data(), sizeof(aco_record), rec.size(), fc.f) == rec.size();
+        if (!ok) return ACO_ERR_IO;
+        CK(cudaMemcpyAsync(ih.iter_d, &it, 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ih.nbsf_d, &nb, 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpy2DAsync(ih.tau_d, (size_t)ih.ld * 4, tau.data(), (size_t)ih.n * 4, (size_t)ih.n * 4, ih.n,
+                             cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ih.sol_d, sol.data(), ns * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ih.lens_d, lens.data(), lens.size() * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ih.seeds_d, seeds.data(), nseed * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ih.rec_d, rec.data(), rec.size() * sizeof(aco_record), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st)); // the host vectors go out of scope
+    }
+    rc = run_rows(ROW_TOTAL, 0.f); // total_info and the candidate table from the restored tau
+    if (rc != ACO_OK) return rc;
+    CK(cudaMemsetAsync(status_d, 0, sizeof(int), st));
+    CK(launch_t0(t0_d_, st)); // record times restart from the resume
+    t_init = std::chrono::steady_clock::now();
+    rc = sync_status();
+    if (rc == ACO_OK) initialized = true;
+    return rc;
 }
 
 int Colony::construct()

@@ -76,6 +76,11 @@ public:
     // Check every tour slot on the device; flags (total slots, or null) and
     // per-instance invalid counts (or null) are copied back.
     int validate(int *flags, int *invalid_per_inst, int *n_invalid);
+    // Everything the next iteration reads, to a file / back from it (a colony
+    // created with the same instances and parameters; total_info and the
+    // candidate table are recomputed from tau).
+    int save_checkpoint(const char *path);
+    int load_checkpoint(const char *path);
     int time_phases(int n_iter, float *ms4);
     int set_device() const;
 

@@ -572,6 +572,10 @@ int aco_write_solution(aco_solver *s, const char *path)
     return write_best(s->c, path, false);
 }
 
+int aco_save_checkpoint(aco_solver *s, const char *path) { return s ? s->c.save_checkpoint(path) : ACO_ERR_INVALID; }
+
+int aco_load_checkpoint(aco_solver *s, const char *path) { return s ? s->c.load_checkpoint(path) : ACO_ERR_INVALID; }
+
 int aco_set_prior(aco_solver *s, const float *prior, int ld)
 {
     if (!s) return ACO_ERR_INVALID;
@@ -668,6 +672,16 @@ int aco_batch_time_phases(aco_batch *b, int n_iter, float *ms4)
 {
     if (!b || !ms4 || n_iter <= 0) return ACO_ERR_INVALID;
     return b->c.time_phases(n_iter, ms4);
+}
+
+int aco_batch_save_checkpoint(aco_batch *b, const char *path)
+{
+    return b ? b->c.save_checkpoint(path) : ACO_ERR_INVALID;
+}
+
+int aco_batch_load_checkpoint(aco_batch *b, const char *path)
+{
+    return b ? b->c.load_checkpoint(path) : ACO_ERR_INVALID;
 }
 
 int aco_batch_validate(aco_batch *b, int *invalid_per_instance, int *n_invalid)

@@ -221,6 +221,18 @@ int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *
 int aco_validate(aco_solver *s, int *flags, int *n_invalid);
 int aco_write_solution(aco_solver *s, const char *path);
 
+/* ---- checkpoint and resume (no reference counterpart) ------------------------
+ * aco_save_checkpoint writes everything the next iteration reads -- tau, the
+ * tours and lengths (best-so-far slot included), the lane seeds, the
+ * best-so-far records and the iteration counter -- after aco_init.
+ * aco_load_checkpoint restores it into a solver created with the same
+ * instance and parameters (ACO_ERR_INVALID otherwise; a prior must be set
+ * again before loading); total_info and the candidate table are recomputed
+ * from tau.  The iterations after a load are bit-identical to the ones the
+ * saving solver would have run.  Record times restart from the load. */
+int aco_save_checkpoint(aco_solver *s, const char *path);
+int aco_load_checkpoint(aco_solver *s, const char *path);
+
 /* ---- autotuner (no reference counterpart) -----------------------------------
  * Times launch configurations on the instance(s) and returns the fastest in
  * *out (a copy of *p with ants_per_block, ls_warps, stage_matrix -- and
@@ -299,6 +311,8 @@ int aco_mpnn_status(void *workspace, void *stream);
 int aco_set_prior(aco_solver *s, const float *prior, int ld);
 int aco_batch_set_prior(aco_batch *b, int idx, const float *prior, int ld);
 int aco_batch_validate(aco_batch *b, int *invalid_per_instance, int *n_invalid);
+int aco_batch_save_checkpoint(aco_batch *b, const char *path);
+int aco_batch_load_checkpoint(aco_batch *b, const char *path);
 int aco_batch_write_solutions(aco_batch *b, const char *path);
 int aco_batch_get_bsf_records(aco_batch *b, int idx, aco_record *out, int cap, int *count);
 
