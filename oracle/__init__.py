@@ -18,7 +18,7 @@ import math
 import os
 import subprocess
 import tempfile
-from typing import Optional
+from typing import List, Optional
 
 import numpy as np
 
@@ -80,6 +80,17 @@ def lib():
         L.orc_swap.argtypes = [ctypes.c_int, _f32p, _i32p, ctypes.c_int, ctypes.c_float, ctypes.c_float, _i32p,
                                ctypes.c_int, ctypes.c_int]
         L.orc_swap.restype = ctypes.c_int
+        L.orc_srandom.argtypes = [ctypes.c_void_p, ctypes.c_uint]
+        L.orc_random.argtypes = [ctypes.c_void_p]
+        L.orc_random.restype = ctypes.c_int32
+        L.orc_ns_propose.argtypes = [ctypes.c_int, _f32p, _i32p, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                     _i32p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_ns_apply.argtypes = [_i32p, ctypes.c_void_p]
+        L.orc_ns_seed.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.orc_ns_seed.restype = ctypes.c_uint
+        L.orc_ns_descent.argtypes = [ctypes.c_int, _f32p, _i32p, ctypes.c_int, ctypes.c_float, ctypes.c_float, _i32p,
+                                     ctypes.c_int, ctypes.c_uint, ctypes.c_int]
+        L.orc_ns_descent.restype = ctypes.c_int
         L.orc_tour_length.argtypes = [ctypes.c_int, _f32p, _i32p, ctypes.c_int]
         L.orc_tour_length.restype = ctypes.c_float
         L.orc_tour_length_f64.argtypes = [ctypes.c_int, _f32p, _i32p, ctypes.c_int]
@@ -287,6 +298,8 @@ def ref_lib():
         L.ref_problem_info.argtypes = [_i32p]
         L.ref_host_check_solution.argtypes = [_i32p, ctypes.c_int]
         L.ref_swap.argtypes = [ctypes.c_char_p, _i32p, ctypes.c_int]
+        L.ref_ns.argtypes = [ctypes.c_char_p, _i32p, ctypes.c_int, ctypes.c_uint, ctypes.c_int, ctypes.c_int,
+                             _i32p, _i32p, _f32p, _i32p, _i32p]
         L.ref_read_instance.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                         _f32p, _f32p, _i32p, _f32p, _i32p, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
@@ -377,3 +390,55 @@ def ref_swap(vrp_path: str, tour) -> np.ndarray:
     if ref_lib().ref_swap(vrp_path.encode(), t, len(t)) != 0:
         raise RuntimeError("ref_swap failed")
     return t
+
+
+class OrcRng(ctypes.Structure):
+    _fields_ = [("r", ctypes.c_uint32 * 31), ("f", ctypes.c_int), ("b", ctypes.c_int)]
+
+
+class OrcMove(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("valid", ctypes.c_int), ("gain", ctypes.c_float), ("pos1", ctypes.c_int),
+                ("pos2", ctypes.c_int)]
+
+
+def random_stream(seed: int, count: int) -> List[int]:
+    """glibc random() after srandom(seed), restated (orc_random)."""
+    g = OrcRng()
+    lib().orc_srandom(ctypes.byref(g), seed)
+    return [lib().orc_random(ctypes.byref(g)) for _ in range(count)]
+
+
+def ns_proposals(dist, demand, capacity, tour, seed: int, count: int, apply: bool, max_dist=math.inf, serv=0.0):
+    """The restated NeighbourSearch proposals (and applications) on a copy of
+    `tour`: list of (type, valid, gain, pos1, pos2) and the final tour."""
+    d = np.ascontiguousarray(dist, np.float32)
+    dem = np.ascontiguousarray(demand, np.int32)
+    t = np.ascontiguousarray(tour, np.int32).copy()
+    g = OrcRng()
+    lib().orc_srandom(ctypes.byref(g), seed)
+    out = []
+    for _ in range(count):
+        m = OrcMove()
+        lib().orc_ns_propose(d.shape[0], d.ravel(), dem, int(capacity), float(max_dist), float(serv), t, len(t),
+                             ctypes.byref(g), ctypes.byref(m))
+        out.append((m.type, m.valid, np.float32(m.gain), m.pos1, m.pos2))
+        if apply and m.type >= 0 and m.valid and np.float32(m.gain) < np.float32(-0.001):
+            lib().orc_ns_apply(t, ctypes.byref(m))
+    return out, t
+
+
+def ref_ns_proposals(vrp_path: str, tour, seed: int, count: int, apply: bool):
+    """The reference's own NeighbourSearch proposals on a copy of `tour`."""
+    t = np.ascontiguousarray(tour, np.int32).copy()
+    ty, va, p1, p2 = (np.zeros(count, np.int32) for _ in range(4))
+    ga = np.zeros(count, np.float32)
+    ref_lib().ref_ns(vrp_path.encode(), t, len(t), seed, count, int(apply), ty, va, ga, p1, p2)
+    return [(int(a), int(b), np.float32(c), int(d), int(e)) for a, b, c, d, e in zip(ty, va, ga, p1, p2)], t
+
+
+def ns_descent(dist, demand, capacity, tour, seed: int, rounds: int, max_dist=math.inf, serv=0.0):
+    d = np.ascontiguousarray(dist, np.float32)
+    t = np.ascontiguousarray(tour, np.int32).copy()
+    k = lib().orc_ns_descent(d.shape[0], d.ravel(), np.ascontiguousarray(demand, np.int32), int(capacity),
+                             float(max_dist), float(serv), t, len(t), seed, rounds)
+    return t, k

@@ -12,6 +12,8 @@
 #ifndef ACO_ORACLE_H
 #define ACO_ORACLE_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -91,4 +93,24 @@ int orc_init_aco_nn(orc_state *s, const int *nn_ants_list, int nn_ants, int n_th
 #ifdef __cplusplus
 }
 #endif
+
+/* ---- random neighbourhood moves (ns_oracle.c) ------------------------- */
+typedef struct orc_rng { uint32_t r[31]; int f, b; } orc_rng; /* glibc random(), TYPE_3 */
+void orc_srandom(orc_rng *g, unsigned seed);
+int32_t orc_random(orc_rng *g);
+typedef struct orc_move {
+    int type; /* 0 exchange, 1 insertion, 2 inversion, -1 none */
+    int valid;
+    float gain;
+    int pos1, pos2;
+} orc_move;
+void orc_ns_propose(int n, const float *dist, const int *demand, int cap, float max_dist, float serv,
+                    const int *tour, int size, orc_rng *g, orc_move *m);
+void orc_ns_apply(int *tour, const orc_move *m);
+/* seed of ant `ant`'s generator in iteration `iteration` */
+unsigned orc_ns_seed(int rnd_seed, int iteration, int ant);
+/* `rounds` proposals; the valid ones with gain < -EPSILON are applied */
+int orc_ns_descent(int n, const float *dist, const int *demand, int cap, float max_dist, float serv, int *tour,
+                   int size, unsigned seed, int rounds);
+
 #endif

@@ -1,6 +1,6 @@
 #!/usr/bin/env bash
 # Builds oracle/_ref/libcvrp_ref.so: the reference's own host code
-# (cvrp_ocl/{problem,io,vrpHelper,utilities,unix_timer,localSearch}.cpp, gpu/g_type.cpp,
+# (cvrp_ocl/{problem,io,vrpHelper,utilities,unix_timer,localSearch,neighbourSearch,move}.cpp, gpu/g_type.cpp,
 # gpu/g_aco.cpp) and its OpenCL kernels (gpu/kernel.cl, compiled as C++) linked
 # against the fake OpenCL runtime in oracle/refshim.  Test infrastructure only.
 #
@@ -35,7 +35,7 @@ INC=(-I"$HERE/refshim" -I"$SRC" -I"$SRC/gpu")
 } > "$TMP/kernel_cl.cpp"
 
 objs=()
-for f in problem io vrpHelper utilities unix_timer localSearch; do
+for f in problem io vrpHelper utilities unix_timer localSearch neighbourSearch move; do
   "$CXX" "${FLAGS[@]}" "${INC[@]}" -c "$SRC/$f.cpp" -o "$TMP/$f.o"
   objs+=("$TMP/$f.o")
 done

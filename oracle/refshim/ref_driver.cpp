@@ -24,6 +24,7 @@
 #include "gpu/g_aco.h"
 #include "gpu/g_type.h"
 #include "localSearch.h"
+#include "neighbourSearch.h"
 #undef private
 
 extern "C" {
@@ -212,6 +213,36 @@ int ref_swap(const char *vrp_path, int *tour, int tour_size)
     LocalSearch ls(inst);
     ls.swap(tour, tour_size);
     return 0; /* inst leaked on purpose, as in ref_read_instance */
+}
+
+/* `count` proposals of the reference's NeighbourSearch::search
+ * (neighbourSearch.cpp:72-95) on one tour of the instance in vrp_path, with
+ * libc's generator seeded by srandom(seed); with `apply`, the valid proposals
+ * whose gain is below -EPSILON are applied (Move::apply, move.cpp) before the
+ * next one.  type -1 marks a proposal the reference returns as NULL. */
+int ref_ns(const char *vrp_path, int *tour, int tour_size, unsigned seed, int count, int apply, int *type,
+           int *valid, float *gain, int *pos1, int *pos2)
+{
+    Problem *inst = new Problem(0);
+    read_instance_file(inst, vrp_path);
+    init_problem(inst);
+    NeighbourSearch ns(inst);
+    srandom(seed);
+    AntStruct ant;
+    ant.tour = tour;
+    ant.tour_size = tour_size;
+    ant.tour_length = 0;
+    for (int k = 0; k < count; k++) {
+        Move *m = ns.search(&ant);
+        if (!m) {
+            type[k] = -1; valid[k] = 0; gain[k] = 0; pos1[k] = pos2[k] = 0;
+            continue;
+        }
+        type[k] = (int)m->type; valid[k] = m->valid; gain[k] = m->gain; pos1[k] = m->pos_n1; pos2[k] = m->pos_n2;
+        if (apply && m->valid && m->gain < -EPSILON) m->apply();
+        delete m;
+    }
+    return 0;
 }
 
 } /* extern "C" */

@@ -209,3 +209,32 @@ def test_swap_matches_reference_swap(tmp_path, seed, nc, max_distance, service):
         checked += 1
         changed += int(k > 0)
     assert checked >= 4 and changed > 0
+
+
+def test_random_restatement_matches_libc():
+    """glibc random() (the generator NeighbourSearch draws from) restated."""
+    import ctypes
+    libc = ctypes.CDLL("libc.so.6")
+    libc.random.restype = ctypes.c_long
+    for seed in (1, 2, 12345, 2**31 - 1, 777777):
+        libc.srandom(ctypes.c_uint(seed))
+        want = [libc.random() for _ in range(500)]
+        assert oracle.random_stream(seed, 500) == want
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference sources not built here")
+@pytest.mark.parametrize("seed,nc,apply", [(41, 40, False), (42, 40, True), (43, 120, True)])
+def test_neighbourhood_moves_match_reference(tmp_path, seed, nc, apply):
+    """Proposals (type, validity, gain, positions) and applied moves of the
+    restated NeighbourSearch against the reference's own code."""
+    inst = I.gen_uniform_small(seed, nc) if nc < 60 else I.gen_mixed(seed, nc)
+    p = str(tmp_path / "x.vrp")
+    I.write_vrplib(inst, p)
+    info = oracle.ref_read_instance(p)
+    for k, t in enumerate(random_tours(inst, 3, seed, info["dist"])):
+        want, wt = oracle.ref_ns_proposals(p, t, 1000 + k, 300, apply)
+        got, gt = oracle.ns_proposals(info["dist"], inst.demand, inst.capacity, t, 1000 + k, 300, apply)
+        assert got == want
+        assert np.array_equal(gt, wt)
+        if apply:
+            assert oracle.check_solution(info["dist"], inst.demand, inst.capacity, gt)
