@@ -17,7 +17,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libcvrp_aco.so")
-SOURCES = ["host.cpp", "construct.cu", "local_search.cu", "pheromone.cu", "colony.cu", "solver.cu", "noalloc.cu", "mpnn.cu", "prep.cu", "validate.cu", "swap.cu"]
+SOURCES = ["host.cpp", "construct.cu", "local_search.cu", "pheromone.cu", "colony.cu", "solver.cu", "noalloc.cu", "mpnn.cu", "prep.cu", "validate.cu", "swap.cu", "ns.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
          "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-Xptxas", "-O3"]

@@ -283,6 +283,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     // (set after cn_apc is known; sized for apc = 1)
     const size_t o_items = take((size_t)total_ants * sizeof(int2));
     const size_t o_sw_items = take((size_t)total_ants * sizeof(int2));
+    const size_t o_ns_items = take((size_t)total_ants * sizeof(int2));
 
     void *arena = nullptr;
     if (res->pool && cudaMallocFromPoolAsync(&arena, off, res->pool, st) == cudaSuccess) {
@@ -330,6 +331,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     uargs_d_ = (UpdateArgs *)(base + o_uargs);
     items_d_ = (int2 *)(base + o_items);
     sw_items_d_ = (int2 *)(base + o_sw_items);
+    ns_items_d_ = (int2 *)(base + o_ns_items);
 
     // ---- configuration (shared-memory budgets over the largest instance)
     const bool throughput = p.mode == ACO_MODE_THROUGHPUT;
@@ -407,12 +409,20 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         for (const InstHost &ih : inst) sw_smem = std::max(sw_smem, swap_smem(ih.n, ih.ld, sw_apc));
         if (sw_smem > kSmemBudget) return ACO_ERR_INVALID; // the tour arrays of one ant do not fit
     }
+    if (p.ns_rounds > 0) { // random-descent stage: up to 8 ants per CTA
+        int n_max = 0;
+        for (const InstHost &ih : inst) n_max = std::max(n_max, ih.n);
+        ns_apc = 8;
+        while (ns_apc > 1 && ns_smem(n_max, ns_apc) > kSmemBudget) ns_apc--;
+        ns_smem_ = ns_smem(n_max, ns_apc);
+        if (ns_smem_ > kSmemBudget) return ACO_ERR_INVALID;
+    }
     stats_smem = (size_t)A_max * sizeof(float);
     if (stats_smem > kSmemBudget) return ACO_ERR_INVALID; // n_ants lengths must fit in shared memory
 
     // ---- host tables and uploads
     std::vector<int> ant_inst(total_ants), ant_base(count + 1), row_base(count + 1);
-    std::vector<int2> items, swi;
+    std::vector<int2> items, swi, nsi;
     {
         int a0 = 0, r0 = 0;
         for (int b = 0; b < count; b++) {
@@ -433,6 +443,9 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         for (int b = 0; b < count; b++)
             for (int a0 = 0; a0 < inst[b].A; a0 += sw_apc) swi.push_back(make_int2(b, a0));
         sw_items = (int)swi.size();
+        for (int b = 0; b < count; b++)
+            for (int a0 = 0; a0 < inst[b].A; a0 += ns_apc) nsi.push_back(make_int2(b, a0));
+        ns_items = (int)nsi.size();
     }
     cargs_h_.resize(count);
     std::vector<LocalSearchArgs> largs(count);
@@ -537,6 +550,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     up(slot_base_d_, slot_base_h_.data(), slot_base_h_.size() * 4);
     up(items_d_, items.data(), items.size() * sizeof(int2));
     up(sw_items_d_, swi.data(), swi.size() * sizeof(int2));
+    up(ns_items_d_, nsi.data(), nsi.size() * sizeof(int2));
     if (!ok) return ACO_ERR_CUDA;
     rc = run_rows(ROW_HEUR, 0.f);
     if (rc != ACO_OK) return rc;
@@ -754,6 +768,12 @@ int Colony::local_search()
     return ACO_OK;
 }
 
+int Colony::neighbourhood()
+{
+    CK(launch_ns(cargs_d_, sargs_d_, ns_items_d_, ns_items, ns_apc, ns_smem_, p.ns_rounds, p.rnd_seed, st));
+    return ACO_OK;
+}
+
 int Colony::stats(bool elites)
 {
     CK(launch_stats(sargs_d_, (int)inst.size(), elites ? 1 : 0, stats_smem, st));
@@ -773,6 +793,7 @@ int Colony::run_phases()
 {
     int rc = construct();
     if (rc == ACO_OK && p.ls_flag) rc = local_search();
+    if (rc == ACO_OK && p.ns_rounds > 0) rc = neighbourhood();
     if (rc == ACO_OK) rc = stats(true);
     if (rc == ACO_OK) rc = update();
     return rc;
@@ -854,6 +875,7 @@ int Colony::time_phases(int n_iter, float *ms4)
         rc = construct();
         CK(cudaEventRecord(ev[1], st));
         if (rc == ACO_OK && p.ls_flag) rc = local_search();
+        if (rc == ACO_OK && p.ns_rounds > 0) rc = neighbourhood();
         CK(cudaEventRecord(ev[2], st));
         if (rc == ACO_OK) rc = stats(true);
         CK(cudaEventRecord(ev[3], st));

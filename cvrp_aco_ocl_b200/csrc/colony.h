@@ -66,6 +66,7 @@ public:
     int sync_status();           // wait for the stream, read the sticky status
     int construct();
     int local_search();
+    int neighbourhood(); // the random-descent stage (ns_rounds > 0)
     int stats(bool elites);
     int update();
     int pheromone_init(float trail, bool from_bsf);
@@ -101,6 +102,8 @@ public:
     int ls_warps = 1;
     int sw_apc = 1, sw_items = 0; // swap stage: ants per CTA, work items
     size_t sw_smem = 0;
+    int ns_apc = 1, ns_items = 0; // random-descent stage
+    size_t ns_smem_ = 0;
     size_t ls_smem = 0, stats_smem = 0;
     int ld_max = 32, total_ants = 0, total_rows = 0, n_items = 0;
     bool fin_any = false;
@@ -114,7 +117,7 @@ private:
     void *arena_ = nullptr;
     bool pooled_ = false; // arena from the device's memory pool (freed stream-ordered)
     unsigned long long *t0_d_ = nullptr;
-    int2 *items_d_ = nullptr, *sw_items_d_ = nullptr;
+    int2 *items_d_ = nullptr, *sw_items_d_ = nullptr, *ns_items_d_ = nullptr;
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
     int *row_base_d_ = nullptr, *zero_base_d_ = nullptr;
     int *slot_base_d_ = nullptr, *valid_d_ = nullptr, *invalid_d_ = nullptr;

@@ -143,6 +143,12 @@ size_t swap_smem(int n, int ld, int apc);
 cudaError_t launch_swap(const ConstructArgs *d_args, const int2 *d_items, int n_items, int apc, size_t smem,
                         int max_swaps_per_node, cudaStream_t st);
 
+// Random-descent stage (ns.cu): one CTA per item {instance, first ant} with
+// `apc` ants, `rounds` neighbourhood-move proposals per ant.
+size_t ns_smem(int n, int apc);
+cudaError_t launch_ns(const ConstructArgs *d_args, const StatsArgs *d_sargs, const int2 *d_items, int n_items, int apc,
+                      size_t smem, int rounds, int rnd_seed, cudaStream_t st);
+
 // Device preprocessing (prep.cu).
 bool device_dist_supported(int dist_type);
 size_t nn_rows_per_cta(int n);

@@ -67,6 +67,7 @@ int check_params(const aco_params &p, int n)
     if (p.stage_matrix < -1 || p.stage_matrix > 0) return ACO_ERR_INVALID;
     if (p.host_prep < 0 || p.host_prep > 1) return ACO_ERR_INVALID;
     if (p.ls_flag != 0 && p.ls_flag != 1 && p.ls_flag != 3) return ACO_ERR_INVALID;
+    if (p.ns_rounds < 0 || p.ns_rounds > 1000000) return ACO_ERR_INVALID;
     if (!(p.rho > 0.0f && p.rho <= 1.0f)) return ACO_ERR_INVALID;
     if (p.n_ants > 56 * 1024) return ACO_ERR_INVALID; // the statistics kernel holds n_ants lengths in shared memory
     return ACO_OK;
@@ -489,7 +490,7 @@ void *aco_get_stream(aco_solver *s) { return s ? (void *)s->c.st : nullptr; }
 int aco_launches_per_iteration(aco_solver *s)
 {
     if (!s) return ACO_ERR_INVALID;
-    return 3 + (s->c.p.ls_flag ? 1 : 0) + ((s->c.p.ls_flag & 2) ? 1 : 0);
+    return 3 + (s->c.p.ls_flag ? 1 : 0) + ((s->c.p.ls_flag & 2) ? 1 : 0) + (s->c.p.ns_rounds > 0 ? 1 : 0);
 }
 
 int aco_time_iterations(aco_solver *s, int n_iter, float *ms)

@@ -48,6 +48,7 @@ class OrcState(ctypes.Structure):
         ("elites", ctypes.c_void_p), ("records", ctypes.c_void_p),
         ("record_cap", ctypes.c_int), ("num_bsf", ctypes.c_int),
         ("iteration", ctypes.c_int), ("update_flag", ctypes.c_int), ("status", ctypes.c_int),
+        ("ns_rounds", ctypes.c_int), ("ns_seed", ctypes.c_int),
     ]
 
 
@@ -179,7 +180,7 @@ class Oracle:
                  alpha: float = 1.0, beta: float = 2.0, rho: float = 0.1,
                  max_dist: float = math.inf, serv_time: float = 0.0, ls_flag: bool = False,
                  ls_pass_limit: int = 0, record_cap: int = 4096, nn_ants_list: Optional[np.ndarray] = None,
-                 n_threads: int = 1):
+                 n_threads: int = 1, ns_rounds: int = 0, ns_seed: int = 0):
         n = dist.shape[0]
         self.n, self.A, self.T = n, n_ants, 2 * n
         self.n_threads = n_threads
@@ -203,6 +204,7 @@ class Oracle:
         st.alpha, st.beta, st.rho = alpha, beta, rho
         st.ls_flag = int(ls_flag)  # 1: 2-opt; 3: 2-opt then the swap stage
         st.step_limit_passes = int(ls_pass_limit)
+        st.ns_rounds, st.ns_seed = int(ns_rounds), int(ns_seed)
         for name in ("dist", "demand", "nn_list", "tau", "total", "seeds", "solutions", "lens", "elites"):
             setattr(st, name, getattr(self, name).ctypes.data)
         st.records = ctypes.cast(self.records, ctypes.c_void_p)

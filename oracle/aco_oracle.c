@@ -811,10 +811,29 @@ int orc_init_aco(orc_state *s, int n_threads)
 
 /* g_ACO::run_aco_iteration + pheromone_update (g_aco.cpp:122-134, 233-243) and
  * the iteration++ of main.cpp:86. */
+/* The random-descent stage: every ant's tour takes ns_rounds NeighbourSearch
+ * proposals (ns_oracle.c), the valid improving ones applied, then its length is
+ * recomputed as compute_tour_length sums it (vrpHelper.cpp:244-253). */
+static void ns_stage(orc_state *s)
+{
+    const int n = s->n, T = 2 * n;
+    for (int a = 0; a < s->n_ants; a++) {
+        int *tour = s->solutions + (size_t)a * T;
+        const int size = tour[T - 1];
+        if (size < 2) continue;
+        orc_ns_descent(n, s->dist, s->demand, s->capacity, s->max_dist, s->serv_time, tour, size,
+                       orc_ns_seed(s->ns_seed, s->iteration, a), s->ns_rounds);
+        float len = 0;
+        for (int i = 0; i < size - 1; i++) len += s->dist[(size_t)tour[i] * n + tour[i + 1]];
+        s->lens[a] = len;
+    }
+}
+
 int orc_run_aco_iteration(orc_state *s, int n_threads)
 {
     int st = orc_construct(s, n_threads);
     if (st == ORC_OK && s->ls_flag) st = orc_local_search(s, n_threads);
+    if (st == ORC_OK && s->ns_rounds > 0) ns_stage(s);
     orc_find_best(s);
     orc_update_best_so_far(s, 0.0f);
     orc_pheromone_evaporation(s);
@@ -938,6 +957,7 @@ int orc_run_aco_iteration_nn(orc_state *s, const int *nn_ants_list, int nn_ants,
 {
     int st = orc_construct_nn(s, nn_ants_list, nn_ants, n_threads);
     if (st == ORC_OK && s->ls_flag) st = orc_local_search(s, n_threads);
+    if (st == ORC_OK && s->ns_rounds > 0) ns_stage(s);
     orc_find_best(s);
     orc_update_best_so_far(s, 0.0f);
     orc_pheromone_evaporation(s);

@@ -48,6 +48,8 @@ typedef struct orc_state {
     orc_record *records;  /* record_cap */
     int record_cap, num_bsf;
     int iteration, update_flag, status;
+    int ns_rounds;        /* random-move proposals per ant and iteration after the local search (0 = off) */
+    int ns_seed;          /* generator seeds: orc_ns_seed(ns_seed, iteration, ant) */
 } orc_state;
 
 /* ---- RNG, seeds -------------------------------------------------------- */

@@ -309,3 +309,29 @@ def test_swap_stage_vs_oracle(gpu, mode, n_cust, A):
             compare_state(S, O)
         flags, bad = S.validate()
         assert bad == 0
+
+
+@pytest.mark.parametrize("mode,n_cust,A,ls", [(MODE_PARITY, 80, 32, 1), (MODE_THROUGHPUT, 200, 64, 3),
+                                              (MODE_THROUGHPUT, 150, 48, 0)])
+def test_random_descent_stage_vs_oracle(gpu, mode, n_cust, A, ls):
+    """ns_rounds > 0: the reference's random neighbourhood moves after the local search."""
+    inst = I.gen_mixed(600 + n_cust, n_cust)
+    n, nloc, T0, rs0, rounds = inst.n, 256, 1796300000, 77, 40
+    prob = problem_of(inst.x, inst.y, inst.demand, inst.capacity)
+    p = params_for(n, A, nloc, T0, rs0, ls, 25, mode=mode, ns_rounds=rounds)
+    if mode == MODE_THROUGHPUT:
+        p.nn_ants = 25
+    dist = oracle.compute_distances(inst.x, inst.y)
+    nn = oracle.compute_nn_lists(dist, 25, 25)
+    seeds, _ = oracle.make_seeds(T0, rs0, A, nloc)
+    O = oracle.Oracle(dist, inst.demand, inst.capacity, A, nloc, nn, seeds, ls_flag=ls,
+                      nn_ants_list=nn if mode == MODE_THROUGHPUT else None, n_threads=8,
+                      ns_rounds=rounds, ns_seed=rs0)
+    thr = mode == MODE_THROUGHPUT
+    with Solver(prob, p) as S:
+        S.init(); O.init_aco(throughput=thr)
+        compare_state(S, O)
+        for _ in range(3):
+            S.iterate(1); O.run_iteration(throughput=thr)
+            compare_state(S, O)
+        assert S.validate()[1] == 0
