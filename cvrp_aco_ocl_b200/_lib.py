@@ -64,7 +64,8 @@ class AcoParams(ctypes.Structure):
         ("max_iteration", ctypes.c_int), ("max_runtime", ctypes.c_float), ("ls_pass_limit", ctypes.c_int),
         ("record_cap", ctypes.c_int), ("device", ctypes.c_int), ("use_graph", ctypes.c_int),
         ("ants_per_block", ctypes.c_int), ("warps_per_ant", ctypes.c_int), ("ls_warps", ctypes.c_int),
-        ("stage_matrix", ctypes.c_int), ("host_prep", ctypes.c_int), ("ns_rounds", ctypes.c_int),
+        ("stage_matrix", ctypes.c_int), ("host_prep", ctypes.c_int), ("fuse_ls", ctypes.c_int),
+        ("ns_rounds", ctypes.c_int),
     ]
 
 

@@ -284,6 +284,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     const size_t o_items = take((size_t)total_ants * sizeof(int2));
     const size_t o_sw_items = take((size_t)total_ants * sizeof(int2));
     const size_t o_ns_items = take((size_t)total_ants * sizeof(int2));
+    const size_t o_ls_needed = take((size_t)total_ants);
 
     void *arena = nullptr;
     if (res->pool && cudaMallocFromPoolAsync(&arena, off, res->pool, st) == cudaSuccess) {
@@ -332,6 +333,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     items_d_ = (int2 *)(base + o_items);
     sw_items_d_ = (int2 *)(base + o_sw_items);
     ns_items_d_ = (int2 *)(base + o_ns_items);
+    ls_needed_d_ = (uint8_t *)(base + o_ls_needed);
 
     // ---- configuration (shared-memory budgets over the largest instance)
     const bool throughput = p.mode == ACO_MODE_THROUGHPUT;
@@ -364,28 +366,47 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         if (p.ants_per_block > 0) cn_apc = std::min(16, p.ants_per_block);
         else if (count == 1) cn_apc = std::max(1, std::min(8, (inst[0].A + sm_count - 1) / sm_count));
         else cn_apc = std::max(1, std::min(16, total_ants / (sm_count * 2)));
-        bool fits = false;
-        while (!fits) {
-            cn_smem = 0;
-            fits = true;
+        // shared-memory plan of every instance for `apc` ants per CTA and `lsw`
+        // fused 2-opt warps (lsw > 0 needs the tables staged)
+        auto plan = [&](int apc, int lsw) {
+            size_t mx = 0;
             for (InstHost &ih : inst) {
                 bool packable = true;
                 for (int i = 0; i < ih.n; i++)
                     if (ih.demand[i] < 0 || ih.demand[i] > 0xFFFF) packable = false;
                 ih.smat = p.stage_matrix >= 0 && ih.n <= 1024 && packable &&
-                          construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, true, true) <= kSmemBudget;
-                ih.packed = packable && construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, ih.smat, true) <= kSmemBudget;
+                          construct_nn_smem(ih.n, ih.K, ih.Kp, apc, true, true, false, lsw) <= kSmemBudget;
+                ih.packed =
+                    packable && construct_nn_smem(ih.n, ih.K, ih.Kp, apc, ih.smat, true, false, lsw) <= kSmemBudget;
                 ih.gtab = false;
-                size_t need = construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, ih.smat, ih.packed);
-                if (need > kSmemBudget) { // the candidate table stays in global memory (read through L2)
-                    ih.gtab = true;
+                size_t need = construct_nn_smem(ih.n, ih.K, ih.Kp, apc, ih.smat, ih.packed, false, lsw);
+                if (need > kSmemBudget) {
+                    ih.gtab = true; // the candidate table stays in global memory (read through L2)
                     ih.packed = packable;
-                    need = construct_nn_smem(ih.n, ih.K, ih.Kp, cn_apc, false, ih.packed, true);
+                    need = construct_nn_smem(ih.n, ih.K, ih.Kp, apc, false, ih.packed, true, lsw);
                 }
-                if (need > kSmemBudget) fits = false;
-                cn_smem = std::max(cn_smem, need);
+                if (need > kSmemBudget) return false;
+                mx = std::max(mx, need);
             }
-            if (!fits) {
+            cn_smem = mx;
+            return true;
+        };
+        cn_lsw = 0;
+        int n_max = 0;
+        for (const InstHost &ih : inst) n_max = std::max(n_max, ih.n);
+        if ((p.ls_flag & 1) && p.fuse_ls == 1 && n_max <= 1024) { // 2-opt fused into the construct
+            // at most 4 constructing ants per CTA, the other warps (up to 16) improve
+            // routes, so completed routes do not queue
+            for (int apc = std::min(cn_apc, 4); apc >= 1 && cn_lsw == 0; apc--) {
+                const int lsw = 16 - apc;
+                if (plan(apc, lsw)) {
+                    cn_apc = apc;
+                    cn_lsw = lsw;
+                }
+            }
+        }
+        if (cn_lsw == 0) {
+            while (!plan(cn_apc, 0)) {
                 if (cn_apc > 1) cn_apc--;
                 else return ACO_ERR_INVALID; // candidate table of this size cannot be staged
             }
@@ -519,6 +540,8 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         c.total = ih.total_d; c.dist = ih.dist_d; c.demand = ih.dem_d; c.tiekey = ih.key_d; c.jump = ih.jump_d;
         c.adv = ih.adv_d; c.nn16 = ih.nn16_d; c.cand32 = ih.cand32_d; c.chc = ih.chc_d; c.K = ih.K; c.Kp = ih.Kp;
         c.smat = ih.smat ? 1 : 0; c.packed = ih.packed ? 1 : 0; c.gtab = ih.gtab ? 1 : 0;
+        c.nn_list = ih.nnls_d; c.nn_ls = ih.nn_ls; c.pass_limit = p.ls_pass_limit; c.ant_base = ant_base[b];
+        c.ls_needed = ls_needed_d_;
         c.seeds = ih.seeds_d; c.solutions = ih.sol_d; c.lens = ih.lens_d; c.status = status_d;
         LocalSearchArgs &l = largs[b];
         l = LocalSearchArgs{};
@@ -750,20 +773,25 @@ int Colony::load_checkpoint(const char *path)
     return rc;
 }
 
-int Colony::construct()
+int Colony::construct(bool fused)
 {
     if (p.mode != ACO_MODE_THROUGHPUT) {
         CK(launch_construct_parity(cargs_h_[0], cp_wpa, cp_apc, cp_stage, st));
         return ACO_OK;
     }
     CK(cudaMemsetAsync(queue_d_, 0, sizeof(int), st));
-    CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st));
+    const int lsw = fused && p.ls_flag ? cn_lsw : 0;
+    last_fused_ = lsw > 0;
+    CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st, lsw));
     return ACO_OK;
 }
 
 int Colony::local_search()
 {
-    CK(launch_local_search(largs_d_, ant_inst_d_, ant_base_d_, total_ants, ls_warps, ls_smem, st));
+    // after a fused construct only the ants it marked still need the 2-opt kernel
+    CK(launch_local_search(largs_d_, ant_inst_d_, ant_base_d_, total_ants, ls_warps, ls_smem, st,
+                           last_fused_ ? ls_needed_d_ : nullptr));
+    last_fused_ = false;
     if (p.ls_flag & 2) CK(launch_swap(cargs_d_, sw_items_d_, sw_items, sw_apc, sw_smem, kSwapLimitPerNode, st));
     return ACO_OK;
 }
@@ -791,7 +819,7 @@ int Colony::gather_candidates() { return p.mode == ACO_MODE_THROUGHPUT ? run_row
 
 int Colony::run_phases()
 {
-    int rc = construct();
+    int rc = construct(true);
     if (rc == ACO_OK && p.ls_flag) rc = local_search();
     if (rc == ACO_OK && p.ns_rounds > 0) rc = neighbourhood();
     if (rc == ACO_OK) rc = stats(true);
@@ -837,7 +865,7 @@ int Colony::init()
     t_init = std::chrono::steady_clock::now();
     // g_aco.cpp:79-92
     rc = pheromone_init(0.5f, false);
-    if (rc == ACO_OK) rc = construct();
+    if (rc == ACO_OK) rc = construct(true);
     if (rc == ACO_OK && p.ls_flag) rc = local_search();
     if (rc == ACO_OK) rc = stats(false);
     if (rc == ACO_OK) rc = pheromone_init(0.f, true);
@@ -872,7 +900,7 @@ int Colony::time_phases(int n_iter, float *ms4)
     for (int k = 0; k < 4; k++) ms4[k] = 0.f;
     for (int it = 0; it < n_iter && rc == ACO_OK; it++) {
         CK(cudaEventRecord(ev[0], st));
-        rc = construct();
+        rc = construct(true);
         CK(cudaEventRecord(ev[1], st));
         if (rc == ACO_OK && p.ls_flag) rc = local_search();
         if (rc == ACO_OK && p.ns_rounds > 0) rc = neighbourhood();

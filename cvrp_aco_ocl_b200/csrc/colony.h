@@ -64,7 +64,7 @@ public:
     int init();                  // g_ACO::init_aco for every instance
     int enqueue(int n_iter);     // n_iter iterations (graph replays), no sync
     int sync_status();           // wait for the stream, read the sticky status
-    int construct();
+    int construct(bool fused = false); // fused: with the 2-opt warps when configured
     int local_search();
     int neighbourhood(); // the random-descent stage (ns_rounds > 0)
     int stats(bool elites);
@@ -97,7 +97,7 @@ public:
     // launch configuration
     int cp_wpa = 1, cp_apc = 1;
     bool cp_stage = false;
-    int cn_apc = 1;
+    int cn_apc = 1, cn_lsw = 0; // throughput construct: ants per CTA, fused 2-opt warps (0 = separate kernel)
     size_t cn_smem = 0;
     int ls_warps = 1;
     int sw_apc = 1, sw_items = 0; // swap stage: ants per CTA, work items
@@ -118,6 +118,8 @@ private:
     bool pooled_ = false; // arena from the device's memory pool (freed stream-ordered)
     unsigned long long *t0_d_ = nullptr;
     int2 *items_d_ = nullptr, *sw_items_d_ = nullptr, *ns_items_d_ = nullptr;
+    uint8_t *ls_needed_d_ = nullptr;
+    bool last_fused_ = false;
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
     int *row_base_d_ = nullptr, *zero_base_d_ = nullptr;
     int *slot_base_d_ = nullptr, *valid_d_ = nullptr, *invalid_d_ = nullptr;

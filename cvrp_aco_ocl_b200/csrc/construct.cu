@@ -25,6 +25,7 @@
 
 #include "aco_device.cuh"
 #include "kernels.h"
+#include "two_opt.cuh"
 
 namespace aco {
 
@@ -233,12 +234,20 @@ __global__ void __launch_bounds__(512) construct_parity_kernel(ConstructArgs a)
 //     step, in step order.
 // ---------------------------------------------------------------------------
 struct NNLayout {
-    size_t bar, dem, d0, cand, chc, vis, tour, mat, bytes;
+    size_t bar, dem, d0, cand, chc, vis, tour, mat, rid, li, dt, pend, cnt, q, ready, ls, bytes;
+    int qcap;
 };
+
+// Shared memory of one 2-opt warp of the fused construct: distance tile,
+// in-route neighbour lists and counts, route node ids.
+constexpr size_t kLsWarpBytes = 32 * 32 * 4 + 32 * 32 + 32 + 64;
 
 // gtab: the candidate table is read from global memory (L2) instead of being
 // staged (instances whose table does not fit next to the per-ant buffers).
-__host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, bool smat, bool packed, bool gtab)
+// lsw > 0: the fused 2-opt (lsw improving warps): per ant the route id and
+// local index of every node and the edge lengths, the route queue.
+__host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, bool smat, bool packed, bool gtab,
+                                              int lsw = 0)
 {
     const size_t n4 = (size_t)((n + 3) & ~3);
     const size_t words = (size_t)((n + 31) / 32);
@@ -253,6 +262,18 @@ __host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, boo
     L.tour = o; o = al128(o + (size_t)apc * 2 * n * 2);
     L.mat = o;
     if (smat) o = al128(o + (size_t)n * n4 * 4);
+    L.qcap = apc * n + 64;
+    L.rid = L.li = L.dt = L.pend = L.cnt = L.q = L.ready = L.ls = o;
+    if (lsw > 0) {
+        L.rid = o; o = al128(o + (size_t)apc * n * 2);
+        L.li = o; o = al128(o + (size_t)apc * n);
+        L.dt = o; o = al128(o + (size_t)apc * 2 * n * 4);
+        L.pend = o; o = al128(o + (size_t)2 * apc * 4); // pending routes, deferred flag
+        L.cnt = o; o = al128(o + 4 * 4);                // slots allocated, tickets, construct warps done
+        L.q = o; o = al128(o + (size_t)L.qcap * 8);
+        L.ready = o; o = al128(o + (size_t)L.qcap * 4);
+        L.ls = o; o = al128(o + (size_t)lsw * kLsWarpBytes);
+    }
     L.bytes = o;
     (void)K;
     return L;
@@ -260,13 +281,104 @@ __host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, boo
 
 // One work item: ants [ant0, ant0 + apc) of instance a.  Returns false if the
 // staging copies did not arrive in time (uniform over the CTA).
-template <bool FIN, bool SMAT, bool PACKED, bool REGVIS, bool GTAB = false>
+__device__ __forceinline__ int ld_volatile(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
+
+constexpr uint32_t kSpinLimit = 1u << 26; // polls before a wait gives up (with 128 ns sleeps: seconds)
+
+// The 2-opt warps of the fused construct: take tickets in order, wait until
+// the route with that index is published (or every construct warp is done and
+// no route is left), improve it in registers (two_opt.cuh) and write it back
+// in place.  Routes of more than 32 nodes mark their ant for the 2-opt kernel.
+__device__ void fused_ls_warp(const ConstructArgs &a, unsigned char *smem, const NNLayout &L, int apc, int lsw_index,
+                              int ncw)
+{
+    const int lane = threadIdx.x & 31, n = a.n;
+    int *cnt = reinterpret_cast<int *>(smem + L.cnt);
+    int *pend = reinterpret_cast<int *>(smem + L.pend); // [0, apc) pending routes, [apc, 2 apc) deferred
+    const int2 *q = reinterpret_cast<const int2 *>(smem + L.q);
+    const int *ready = reinterpret_cast<const int *>(smem + L.ready);
+    unsigned char *w = smem + L.ls + (size_t)lsw_index * kLsWarpBytes;
+    float *tile = reinterpret_cast<float *>(w);
+    uint8_t *lnn = w + 32 * 32 * 4;
+    uint8_t *lcnt = lnn + 32 * 32;
+    uint16_t *rnode = reinterpret_cast<uint16_t *>(lcnt + 32);
+    int status = ACO_OK;
+    for (;;) {
+        int t = 0, state = 0; // state: 1 route ready, 2 nothing left, 3 timed out
+        if (lane == 0) {
+            t = atomicAdd(&cnt[1], 1);
+            for (uint32_t it = 0;; it++) {
+                if (t < L.qcap && ld_volatile(&ready[t])) { state = 1; break; }
+                if (ld_volatile(&cnt[2]) >= ncw && ld_volatile(&cnt[0]) <= t) { state = 2; break; }
+                if (it > kSpinLimit) { state = 3; break; }
+                if (it > 32) __nanosleep(128);
+            }
+        }
+        state = __shfl_sync(kFullMask, state, 0);
+        t = __shfl_sync(kFullMask, t, 0);
+        if (state == 3) {
+            status = ACO_ERR_TIMEOUT;
+            break;
+        }
+        if (state == 2) break;
+        __threadfence_block();
+        const volatile int *qe = reinterpret_cast<const volatile int *>(q + t);
+        const int2 e = make_int2(qe[0], qe[1]);
+        const int j = e.x & 0xff, r = e.x >> 8, rb = e.y & 0xffff, R = e.y >> 16;
+        uint16_t *tb = reinterpret_cast<uint16_t *>(smem + L.tour) + (size_t)j * 2 * n;
+        const uint16_t *rid = reinterpret_cast<const uint16_t *>(smem + L.rid) + (size_t)j * n;
+        const uint8_t *li = reinterpret_cast<const uint8_t *>(smem + L.li) + (size_t)j * n;
+        float *dt = reinterpret_cast<float *>(smem + L.dt) + (size_t)j * 2 * n;
+        if (R > kRL) { // longer routes: the whole ant goes to the 2-opt kernel
+            if (lane == 0) pend[apc + j] = 1;
+        } else {
+            // route-local state, as the 2-opt kernel builds it (local_search.cu)
+            const int v = lane < R ? (int)tb[rb + lane] : 0;
+            if (lane < R) rnode[lane] = (uint16_t)v;
+            __syncwarp();
+            for (int x = lane; x < R * kRL; x += 32) {
+                const int k1 = x >> 5, k2 = x & 31;
+                tile[x] = k2 < R ? __ldg(a.dist + (size_t)rnode[k1] * a.ld + rnode[k2]) : 0.f;
+            }
+            for (int k = 0; k < R; k++) {
+                const int node = rnode[k];
+                int c = 0;
+                for (int h0 = 0; h0 < a.nn_ls && c < R - 1; h0 += 32) {
+                    const int h = h0 + lane;
+                    const int n2 = h < a.nn_ls ? __ldg(a.nn_list + (size_t)node * a.nn_ls + h) : 0;
+                    const bool in = h < a.nn_ls && n2 != 0 && rid[n2] == r;
+                    const unsigned m = __ballot_sync(kFullMask, in);
+                    const int slot = c + __popc(m & ((1u << lane) - 1u));
+                    if (in && slot < kRL) lnn[k * kRL + slot] = li[n2];
+                    c += __popc(m);
+                }
+                if (lane == 0) lcnt[k] = (uint8_t)(c < R - 1 ? c : R - 1);
+            }
+            __syncwarp();
+            int tq = lane < R ? lane : 0, pk = lane < R ? lane : 0;
+            float dq = lane < R ? tile[lane * kRL + (lane + 1 < R ? lane + 1 : 0)] : 0.f; // dist_tour_wrk
+            const int st = two_opt_route_regs(lane, R, r == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
+            if (st != ACO_OK) status = st;
+            const int node = __shfl_sync(kFullMask, v, tq);
+            if (lane < R) {
+                tb[rb + lane] = (uint16_t)node;
+                dt[rb + lane] = dq;
+            }
+        }
+        __syncwarp();
+        __threadfence_block();
+        if (lane == 0) atomicSub(&pend[j], 1);
+    }
+    if (status != ACO_OK && lane == 0) set_status(a.status, status);
+}
+
+template <bool FIN, bool SMAT, bool PACKED, bool REGVIS, bool GTAB = false, bool LSF = false>
 __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int apc, int ant0, unsigned char *smem, uint32_t phase,
-                                  uint32_t pw)
+                                  uint32_t pw, int lsw = 0)
 {
     const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp, T = a.T;
     const int n4 = (n + 3) & ~3;
-    const NNLayout L = nn_layout(n, K, Kp, apc, SMAT, PACKED, GTAB);
+    const NNLayout L = nn_layout(n, K, Kp, apc, SMAT, PACKED, GTAB, LSF ? lsw : 0);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar);
     int *s_dem = reinterpret_cast<int *>(smem + L.dem);
     float *s_d0 = reinterpret_cast<float *>(smem + L.d0);
@@ -297,6 +409,15 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             tma_bulk_g2s(s_mat + (size_t)r * n4, a.total + (size_t)r * ld, n4 * 4, bar);
     if (FIN)
         for (int i = threadIdx.x; i < n; i += blockDim.x) s_d0[i] = a.dist[(size_t)i * ld];
+    if (LSF) { // fused 2-opt bookkeeping starts empty for this item
+        uint16_t *rid_all = reinterpret_cast<uint16_t *>(smem + L.rid);
+        for (int i = threadIdx.x; i < apc * n; i += blockDim.x) rid_all[i] = 0xFFFFu;
+        int *ready_all = reinterpret_cast<int *>(smem + L.ready);
+        for (int i = threadIdx.x; i < L.qcap; i += blockDim.x) ready_all[i] = 0;
+        int *pend_all = reinterpret_cast<int *>(smem + L.pend);
+        for (int i = threadIdx.x; i < 2 * apc; i += blockDim.x) pend_all[i] = 0;
+        if (threadIdx.x < 4) reinterpret_cast<int *>(smem + L.cnt)[threadIdx.x] = 0;
+    }
     const bool ok = mbar_wait(bar, phase);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) set_status(a.status, ACO_ERR_TIMEOUT);
@@ -305,8 +426,36 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
     }
 
     const int ant = ant0 + warp;
+    if (LSF && warp >= apc) {
+        if (warp < apc + lsw) {
+            const int ncw = a.n_ants - ant0 < apc ? a.n_ants - ant0 : apc;
+            fused_ls_warp(a, smem, L, apc, warp - apc, ncw);
+        }
+        return true;
+    }
+    // fused 2-opt: publish route [rb, rb + R) of this ant for the improving warps
+    int *f_cnt = reinterpret_cast<int *>(smem + L.cnt);
+    int *f_pend = reinterpret_cast<int *>(smem + L.pend);
+    auto publish = [&](int r, int rb, int R) {
+        if (threadIdx.x % 32 == 0) {
+            atomicAdd(&f_pend[warp], 1);
+            const int slot = atomicAdd(&f_cnt[0], 1);
+            if (slot < L.qcap) {
+                reinterpret_cast<int2 *>(smem + L.q)[slot] = make_int2(warp | (r << 8), rb | (R << 16));
+                __threadfence_block();
+                atomicExch(reinterpret_cast<int *>(smem + L.ready) + slot, 1);
+            } else {
+                atomicSub(&f_pend[warp], 1); // cannot happen (capacity covers every route)
+                set_status(a.status, ACO_ERR_CAPACITY);
+            }
+        }
+    };
     if (warp < apc && ant < a.n_ants) {
         uint16_t *tbuf = s_tour + warp * 2 * n;
+        uint16_t *f_rid = reinterpret_cast<uint16_t *>(smem + L.rid) + (size_t)warp * n;
+        uint8_t *f_li = reinterpret_cast<uint8_t *>(smem + L.li) + (size_t)warp * n;
+        int f_rb = 0, f_r = 0;
+        (void)f_rid; (void)f_li;
         uint32_t *vism = s_vis + warp * words;
         uint32_t vis = lane == 0 ? 1u : 0u; // register visited set (REGVIS): node 0 = lane 0, bit 0
         if (!REGVIS) {
@@ -405,10 +554,46 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 __syncwarp();
             }
             if (lane == 0) tbuf[step] = (uint16_t)nxt;
+            if (LSF) {
+                if (nxt != 0) {
+                    if (lane == 0) {
+                        f_rid[nxt] = (uint16_t)f_r;
+                        f_li[nxt] = (uint8_t)(step - f_rb < 256 ? step - f_rb : 0);
+                    }
+                } else { // back at the depot: the route [f_rb, step) is complete
+                    publish(f_r, f_rb, step - f_rb);
+                    f_r++;
+                    f_rb = step;
+                }
+            }
             cur = nxt;
         }
         __syncwarp();
         int *tour = a.solutions + (size_t)ant * T;
+        bool use_dt = false;
+        if (LSF) {
+            if (!err) {
+                if (lane == 0) tbuf[step + 1] = 0;
+                publish(f_r, f_rb, step + 1 - f_rb); // the last route ends at the final depot
+            }
+            if (lane == 0) { // this ant is done publishing; wait until its routes are improved
+                __threadfence_block();
+                atomicAdd(&f_cnt[2], 1);
+                uint32_t it = 0;
+                while (ld_volatile(&f_pend[warp]) > 0) {
+                    if (++it > kSpinLimit) {
+                        set_status(a.status, ACO_ERR_TIMEOUT);
+                        break;
+                    }
+                    if (it > 32) __nanosleep(128);
+                }
+                __threadfence_block();
+            }
+            __syncwarp();
+            const bool deferred = ld_volatile(&f_pend[apc + warp]) != 0;
+            use_dt = !deferred;
+            if (lane == 0) a.ls_needed[a.ant_base + ant] = (uint8_t)(!err && deferred ? 1 : 0);
+        }
         if (err) {
             if (lane == 0) {
                 tour[T - 1] = 0;
@@ -420,11 +605,14 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             if (lane == 0) tbuf[step + 1] = 0;
             __syncwarp();
             for (int p = lane; p < size; p += 32) tour[p] = tbuf[p];
-            // tour length: the fp32 sum of the edges in step order (kernel.cl:475,483)
+            // tour length: the fp32 sum of the edges in step order (kernel.cl:475,483); after the
+            // fused 2-opt, of its edge lengths in position order (kernel.cl:534-538)
+            const float *f_dt = reinterpret_cast<const float *>(smem + L.dt) + (size_t)warp * 2 * n;
             float tdist = 0.f;
             for (int base = 0; base < size - 1; base += 32) {
                 const int p = base + lane;
-                const float e = p < size - 1 ? __ldg(a.dist + (size_t)tbuf[p] * ld + tbuf[p + 1]) : 0.f;
+                const float e = p < size - 1 ? (use_dt ? f_dt[p] : __ldg(a.dist + (size_t)tbuf[p] * ld + tbuf[p + 1]))
+                                             : 0.f;
                 const int m = size - 1 - base < 32 ? size - 1 - base : 32;
 #pragma unroll
                 for (int k = 0; k < 32; k++) {
@@ -447,7 +635,7 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
 
 template <bool FIN>
 __global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *args, const int2 *items, int n_items,
-                                                           int *queue, int apc)
+                                                           int *queue, int apc, int lsw)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_item;
@@ -470,7 +658,15 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *
         const ConstructArgs a = args[code.x];
         const int ant0 = code.y;
         bool ok;
-        if (a.gtab) {
+        if (lsw > 0 && a.gtab) { // fused 2-opt, candidate table in global memory
+            ok = a.packed ? construct_nn_item<FIN, false, true, true, true, true>(a, apc, ant0, smem, phase, pw, lsw)
+                          : construct_nn_item<FIN, false, false, true, true, true>(a, apc, ant0, smem, phase, pw, lsw);
+        } else if (lsw > 0) { // fused 2-opt (register visited set, staged tables)
+            if (a.smat) ok = a.packed ? construct_nn_item<FIN, true, true, true, false, true>(a, apc, ant0, smem, phase, pw, lsw)
+                                      : construct_nn_item<FIN, true, false, true, false, true>(a, apc, ant0, smem, phase, pw, lsw);
+            else ok = a.packed ? construct_nn_item<FIN, false, true, true, false, true>(a, apc, ant0, smem, phase, pw, lsw)
+                               : construct_nn_item<FIN, false, false, true, false, true>(a, apc, ant0, smem, phase, pw, lsw);
+        } else if (a.gtab) {
             ok = a.packed ? construct_nn_item<FIN, false, true, false, true>(a, apc, ant0, smem, phase, pw)
                           : construct_nn_item<FIN, false, false, false, true>(a, apc, ant0, smem, phase, pw);
         } else if (a.n <= 1024) {
@@ -514,13 +710,13 @@ size_t construct_parity_smem(int n, int nloc, int kmax, int wpa, int apc, bool s
     return parity_layout(n, nloc, kmax, wpa, apc, stage_total).bytes;
 }
 
-size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool packed, bool global_table)
+size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool packed, bool global_table, int ls_warps)
 {
-    return nn_layout(n, K, Kp, apc, stage_total, packed, global_table).bytes;
+    return nn_layout(n, K, Kp, apc, stage_total, packed, global_table, ls_warps).bytes;
 }
 
 cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue, int apc,
-                                size_t smem, int sm_count, bool finite_maxd, cudaStream_t st)
+                                size_t smem, int sm_count, bool finite_maxd, cudaStream_t st, int ls_warps)
 {
     auto kern = finite_maxd ? construct_nn_kernel<true> : construct_nn_kernel<false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -530,8 +726,10 @@ cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items
     int blocks = sm_count * per_sm;
     if (blocks > n_items) blocks = n_items;
     if (blocks < 1) blocks = 1;
-    const int warps = apc < 8 ? 8 : apc; // helper warps share the staging of each item
-    kern<<<blocks, warps * 32, smem, st>>>(d_args, d_items, n_items, d_queue, apc);
+    int warps = apc < 8 ? 8 : apc; // helper warps share the staging of each item
+    if (ls_warps > 0) warps = apc + ls_warps;
+    if (warps > 16) return cudaErrorInvalidValue;
+    kern<<<blocks, warps * 32, smem, st>>>(d_args, d_items, n_items, d_queue, apc, ls_warps);
     return cudaGetLastError();
 }
 

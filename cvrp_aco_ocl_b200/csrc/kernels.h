@@ -42,6 +42,11 @@ struct ConstructArgs {
     int smat;              // throughput construct: stage the whole total_info matrix
     int packed;            // throughput construct: use cand32 (else nn16 + demand lookups)
     int gtab;              // throughput construct: read the candidate table from global memory (not staged)
+    // fused 2-opt (throughput construct with improving warps): the 2-opt lists, the
+    // pass limit, and per global ant whether the 2-opt kernel still has to run
+    const int *nn_list;    // n x nn_ls
+    int nn_ls, pass_limit, ant_base;
+    uint8_t *ls_needed;    // total ants of the colony
     int *seeds;
     int *solutions;
     float *lens;
@@ -110,12 +115,18 @@ cudaError_t launch_construct_parity(const ConstructArgs &a, int warps_per_ant, i
                                     cudaStream_t st);
 // Throughput construct, persistent: CTAs pull work items {instance, first ant}
 // from *d_queue (reset to 0 by the caller before the launch).
+// ls_warps > 0: each CTA also runs that many 2-opt warps that improve the
+// routes of its ants as soon as they are complete (all instances n <= 1024,
+// candidate tables staged); ants with a route of more than 32 nodes are marked
+// in ls_needed for the 2-opt kernel.
 cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue,
-                                int ants_per_cta, size_t smem, int sm_count, bool finite_maxd, cudaStream_t st);
+                                int ants_per_cta, size_t smem, int sm_count, bool finite_maxd, cudaStream_t st,
+                                int ls_warps = 0);
 // 2-opt: one CTA of `warps` warps per ant; d_ant_inst[g] = instance of global ant g,
 // d_ant_base[b] = first global ant of instance b.
 cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
-                                int total_ants, int warps, size_t smem, cudaStream_t st);
+                                int total_ants, int warps, size_t smem, cudaStream_t st,
+                                const uint8_t *only = nullptr); // only: skip ants whose flag is 0
 cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st);
 // Row passes (heuristic matrix, pheromone init, fused update, candidate gather):
 // one warp per row over all instances; d_row_base[b] = first global row of instance b.
@@ -128,7 +139,7 @@ cudaError_t launch_t0(unsigned long long *t0, cudaStream_t st);
 size_t construct_parity_smem(int n, int nloc, int kmax, int warps_per_ant, int ants_per_block, bool stage_total,
                              bool finite_maxd);
 size_t construct_nn_smem(int n, int K, int Kp, int ants_per_cta, bool stage_total, bool packed,
-                         bool global_table = false);
+                         bool global_table = false, int ls_warps = 0);
 size_t local_search_smem(int n, int warps);
 
 // Tour validation (validate.cu): flags[slot_base[b] + s] = 1 if slot s of

@@ -31,6 +31,7 @@
 
 #include "aco_device.cuh"
 #include "kernels.h"
+#include "two_opt.cuh"
 
 namespace aco {
 
@@ -38,7 +39,6 @@ namespace {
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-constexpr int kRL = 32; // largest route (nodes, depot included) of the register path
 
 struct LsLayout {
     size_t tour, pos, li, rid, dlb, rstart, dt, tiles, lnn, lcnt, rnodes, bytes;
@@ -64,109 +64,6 @@ __host__ __device__ inline LsLayout ls_layout(int n, int T, int warps)
 }
 
 constexpr unsigned FULL = 0xffffffffu;
-
-// ---------------------------------------------------------------------------
-// Register path: routes of at most 32 nodes.
-// ---------------------------------------------------------------------------
-__device__ int two_opt_route_regs(int lane, int R, bool first_route, const float *tile, const uint8_t *lnn,
-                                  const uint8_t *lcnt, int &tq, int &pk, float &dq, int pass_limit)
-{
-    // lane q: tq = local node at position q, dq = dist_tour_wrk of position q;
-    // lane k: pk = position of local node k.  Local node 0 is the depot at position 0.
-    uint32_t dlb = first_route ? 0u : 1u; // bit k: don't-look bit of local node k
-    int passes = 0;
-    bool imp = true;
-    while (imp) {
-        if (pass_limit > 0 && passes >= pass_limit) return ACO_ERR_LS_LIMIT;
-        passes++;
-        imp = false;
-        for (int q1 = 0; q1 < R; q1++) {
-            const int k1 = __shfl_sync(FULL, tq, q1);
-            if ((dlb >> k1) & 1u) continue;
-            const int cnt = lcnt[k1];
-            const int j = lane;
-            const int k2 = j < cnt ? lnn[k1 * kRL + j] : 0;
-            const float d12 = tile[k1 * kRL + k2];
-            const int q2 = __shfl_sync(FULL, pk, k2);
-            bool found = false;
-            int h1 = 0, h2 = 0, h3 = 0, h4 = 0;
-            // successor search (kernel.cl:180-198)
-            {
-                const int ks1 = __shfl_sync(FULL, tq, q1 + 1 < R ? q1 + 1 : 0);
-                const float radius = tile[k1 * kRL + ks1];
-                const int ks2 = __shfl_sync(FULL, tq, q2 + 1 < R ? q2 + 1 : 0);
-                const float dq2 = __shfl_sync(FULL, dq, q2);
-                const bool act = j < cnt;
-                const bool cond = act && __fsub_rn(radius, d12) > kEps;
-                bool okm = false;
-                if (cond) {
-                    const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), tile[ks1 * kRL + ks2]), dq2);
-                    okm = g < -kEps;
-                }
-                const unsigned stop = __ballot_sync(FULL, act && (!cond || okm));
-                if (stop) {
-                    const int f = __ffs(stop) - 1;
-                    if (__shfl_sync(FULL, (int)cond, f)) {
-                        found = true;
-                        h1 = k1;
-                        h2 = ks1;
-                        h3 = __shfl_sync(FULL, k2, f);
-                        h4 = __shfl_sync(FULL, ks2, f);
-                    }
-                }
-            }
-            if (!found) { // predecessor search (kernel.cl:202-230)
-                const int kp1 = __shfl_sync(FULL, tq, q1 > 0 ? q1 - 1 : R - 1);
-                const float radius = tile[kp1 * kRL + k1];
-                const int kpp2 = __shfl_sync(FULL, tq, q2 > 0 ? q2 - 1 : R - 1);
-                const float dqp2 = __shfl_sync(FULL, dq, q2 > 0 ? q2 - 1 : 0);
-                const bool act = j < cnt;
-                const bool cond = act && __fsub_rn(radius, d12) > kEps;
-                bool okm = false;
-                if (cond && !(kpp2 == k1 || kp1 == k2)) {
-                    const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), tile[kp1 * kRL + kpp2]), dqp2);
-                    okm = g < -kEps;
-                }
-                const unsigned stop = __ballot_sync(FULL, act && (!cond || okm));
-                if (stop) {
-                    const int f = __ffs(stop) - 1;
-                    if (__shfl_sync(FULL, (int)cond, f)) {
-                        found = true;
-                        h1 = kp1;
-                        h2 = k1;
-                        h3 = __shfl_sync(FULL, kpp2, f);
-                        h4 = __shfl_sync(FULL, k2, f);
-                    }
-                }
-            }
-            if (!found) {
-                dlb |= 1u << k1; // kernel.cl:232
-                continue;
-            }
-            // exchange (kernel.cl:235-270)
-            imp = true;
-            dlb &= ~((1u << h1) | (1u << h2) | (1u << h3) | (1u << h4));
-            int p1 = __shfl_sync(FULL, pk, h1), p3 = __shfl_sync(FULL, pk, h3);
-            if (p3 < p1) {
-                int t = h1; h1 = h3; h3 = t;
-                t = h2; h2 = h4; h4 = t;
-                t = p1; p1 = p3; p3 = t;
-            }
-            const int i = p1, jj = p3, a = __shfl_sync(FULL, pk, h2);
-            const float d13 = tile[h1 * kRL + h3], d24 = tile[h2 * kRL + h4];
-            // dist_tour_wrk: [i] = d(h1,h3), [jj] = d(h2,h4), (i, jj) reversed
-            const float dsrc = __shfl_sync(FULL, dq, (lane > i && lane < jj) ? i + jj - lane : lane);
-            if (lane == jj) dq = d24; // written after [i], as kernel.cl:249-250
-            else if (lane == i) dq = d13;
-            else if (lane > i && lane < jj) dq = dsrc;
-            // tour positions [a, jj] reversed; positions of the moved nodes mirrored
-            const int tsrc = __shfl_sync(FULL, tq, (lane >= a && lane <= jj) ? a + jj - lane : lane);
-            if (lane >= a && lane <= jj) tq = tsrc;
-            if (pk >= a && pk <= jj) pk = a + jj - pk;
-        }
-    }
-    return ACO_OK;
-}
 
 // ---------------------------------------------------------------------------
 // Generic path: any route length, shared-memory arrays, global distances.
@@ -324,8 +221,9 @@ __device__ int two_opt_route_generic(Route &c, int pass_limit)
 }
 
 __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArgs *args, const int *ant_inst,
-                                                             const int *ant_base)
+                                                             const int *ant_base, const uint8_t *only)
 {
+    if (only && !only[blockIdx.x]) return; // improved already (fused with the construct)
     extern __shared__ __align__(128) unsigned char smem[];
     const int b = __ldg(ant_inst + blockIdx.x);
     const LocalSearchArgs a = args[b];
@@ -458,11 +356,11 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
 size_t local_search_smem(int n, int warps) { return ls_layout(n, 2 * n, warps).bytes; }
 
 cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
-                                int total_ants, int warps, size_t smem, cudaStream_t st)
+                                int total_ants, int warps, size_t smem, cudaStream_t st, const uint8_t *only)
 {
     cudaError_t e = cudaFuncSetAttribute(local_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    local_search_kernel<<<total_ants, warps * 32, smem, st>>>(d_args, d_ant_inst, d_ant_base);
+    local_search_kernel<<<total_ants, warps * 32, smem, st>>>(d_args, d_ant_inst, d_ant_base, only);
     return cudaGetLastError();
 }
 

@@ -68,6 +68,7 @@ int check_params(const aco_params &p, int n)
     if (p.host_prep < 0 || p.host_prep > 1) return ACO_ERR_INVALID;
     if (p.ls_flag != 0 && p.ls_flag != 1 && p.ls_flag != 3) return ACO_ERR_INVALID;
     if (p.ns_rounds < 0 || p.ns_rounds > 1000000) return ACO_ERR_INVALID;
+    if (p.fuse_ls < 0 || p.fuse_ls > 1) return ACO_ERR_INVALID;
     if (!(p.rho > 0.0f && p.rho <= 1.0f)) return ACO_ERR_INVALID;
     if (p.n_ants > 56 * 1024) return ACO_ERR_INVALID; // the statistics kernel holds n_ants lengths in shared memory
     return ACO_OK;

@@ -93,6 +93,9 @@ typedef struct aco_params {
                              it fits (used by the no-candidate fallback); -1 = never, rows are read through L2 */
     int host_prep;        /* 0 = distances and neighbour lists computed on the device when the distance type
                              allows (all but GEO; bit-identical to the host); 1 = on the host */
+    int fuse_ls;          /* throughput mode with 2-opt, n <= 1024: 1 = improve each route inside the construct
+                             kernel as soon as it is complete (same results); 0 = separate 2-opt kernel (default,
+                             faster on the measured workloads) */
     int ns_rounds;        /* random-descent stage after the local search: proposals of the reference's
                              random neighbourhood moves (neighbourSearch.cpp, move.cpp) per ant and iteration,
                              the valid improving ones applied; 0 = off (default) */

@@ -335,3 +335,22 @@ def test_random_descent_stage_vs_oracle(gpu, mode, n_cust, A, ls):
             S.iterate(1); O.run_iteration(throughput=thr)
             compare_state(S, O)
         assert S.validate()[1] == 0
+
+
+@pytest.mark.parametrize("per_route,n_cust,A", [(12.0, 200, 64), (45.0, 200, 40), (8.0, 700, 48)])
+def test_fused_2opt_matches_oracle_and_separate_kernel(gpu, per_route, n_cust, A):
+    """The construct kernel improving routes as they complete (fuse_ls = 1) gives
+    the bits of the separate 2-opt kernel (fuse_ls = 0) and of the oracle; with
+    45 customers a route, routes longer than 32 nodes go to the 2-opt kernel."""
+    inst = I.gen_mixed(700 + n_cust, n_cust, customers_per_route=per_route)
+    S, O = build_pair(inst, A, 256, 1796300000, 91, True, 25, mode=MODE_THROUGHPUT, nn_ants=25, fuse_ls=1)
+    p2 = params_for(inst.n, A, 256, 1796300000, 91, True, 25, mode=MODE_THROUGHPUT, nn_ants=25, fuse_ls=0)
+    prob = problem_of(inst.x, inst.y, inst.demand, inst.capacity)
+    with S, Solver(prob, p2) as S2:
+        S.init(); S2.init(); O.init_aco(throughput=True)
+        compare_state(S, O)
+        for _ in range(3):
+            S.iterate(1); S2.iterate(1); O.run_iteration(throughput=True)
+            compare_state(S, O)
+            a, b = S.solutions(), S2.solutions()
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
