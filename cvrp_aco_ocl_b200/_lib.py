@@ -66,6 +66,7 @@ class AcoParams(ctypes.Structure):
         ("ants_per_block", ctypes.c_int), ("warps_per_ant", ctypes.c_int), ("ls_warps", ctypes.c_int),
         ("stage_matrix", ctypes.c_int), ("host_prep", ctypes.c_int), ("fuse_ls", ctypes.c_int),
         ("ns_rounds", ctypes.c_int),
+        ("ls_ants", ctypes.c_int),
     ]
 
 

@@ -34,6 +34,47 @@ __device__ __forceinline__ float pm_uniform(uint32_t x)
     return __fmul_rn(__int2float_rn((int)x), 4.656612873077392578125e-10f);
 }
 
+// Natural logarithm for the throughput sampler's exponential race, written out
+// so that the host restatement computes the same bits: u = m * 2^e with m in
+// [sqrt(1/2), sqrt(2)), ln(u) = e*ln2 + 2*atanh(s), s = (m-1)/(m+1), the odd
+// series of atanh to s^9 (|s| <= 0.1716: truncation below 2e-9 relative).
+// Defined for u >= 0 (u = 0 gives -127*ln2).
+__device__ __forceinline__ float race_ln(float u)
+{
+    const uint32_t b = __float_as_uint(u);
+    int e = (int)(b >> 23) - 127;
+    float m = __uint_as_float((b & 0x007fffffu) | 0x3f800000u);
+    if (m > 1.41421354f) {
+        m = __fmul_rn(m, 0.5f);
+        e += 1;
+    }
+    const float t = __fsub_rn(m, 1.0f);
+    const float s = __fdiv_rn(t, __fadd_rn(t, 2.0f));
+    const float s2 = __fmul_rn(s, s);
+    float p = __fmaf_rn(s2, 1.0f / 9.0f, 1.0f / 7.0f);
+    p = __fmaf_rn(s2, p, 1.0f / 5.0f);
+    p = __fmaf_rn(s2, p, 1.0f / 3.0f);
+    p = __fmul_rn(s2, p);
+    const float ls = __fmul_rn(2.0f, __fmaf_rn(s, p, s));
+    return __fmaf_rn((float)e, 0.693147182f, ls);
+}
+
+// Rate of a lane's exponential clock: 1 / E with E = -ln(u) ~ Exp(1).  The
+// candidate with the largest weight * rate (smallest E / weight) wins, which
+// selects candidate j with probability weight_j / sum(weight).  u = 1 gives
+// E = +0 and rate +inf.
+__device__ __forceinline__ float race_rate(float u) { return __fdiv_rn(1.0f, __fsub_rn(0.0f, race_ln(u))); }
+
+// Race key of a lane: the bits of weight * rate (non-negative, so ordered as
+// unsigned) with the low 5 bits replaced by 31 - lane, so that one unsigned max
+// reduction yields the winner and equal keys go to the lowest lane; 0 = no
+// candidate.
+__device__ __forceinline__ uint32_t race_key(float w, float rate, int lane)
+{
+    const uint32_t b = __float_as_uint(__fmul_rn(w, rate)) & ~31u;
+    return (b < 32u ? 32u : b) | (uint32_t)(31 - lane);
+}
+
 // Sticky error: the first failing kernel's code wins.
 __device__ __forceinline__ void set_status(int *status, int code)
 {

@@ -412,13 +412,42 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
             }
         }
     }
-    ls_warps = p.ls_warps > 0 ? p.ls_warps : (int)std::max<long long>(1, std::min<long long>(32, max_routes + 2));
-    ls_smem = 0;
-    for (const InstHost &ih : inst) ls_smem = std::max(ls_smem, local_search_smem(ih.n, ls_warps));
-    while (ls_warps > 1 && ls_smem > kSmemBudget) {
-        ls_warps--;
-        ls_smem = 0;
-        for (const InstHost &ih : inst) ls_smem = std::max(ls_smem, local_search_smem(ih.n, ls_warps));
+    {
+        // 2-opt CTA shape: ants per CTA x warps.  Cost model: waves of CTAs over
+        // the SMs x routes per warp (routes per ant estimated by total demand /
+        // capacity); ties go to more warps per ant.  A caller's value is kept.
+        int n_max = 0;
+        for (const InstHost &ih : inst) n_max = std::max(n_max, ih.n);
+        ls_nmax = n_max;
+        long long best_cost = -1;
+        double best_wpa = 0.0;
+        ls_apc = 1;
+        ls_warps = 1;
+        ls_smem = local_search_smem(n_max, 1, 1);
+        for (int apc = 1; apc <= 8; apc++) {
+            if (p.ls_ants > 0 && apc != p.ls_ants) continue;
+            int wcap = 32; // a caller's width is narrowed to what shared memory holds
+            while (wcap > apc && local_search_smem(n_max, apc, wcap) > kSmemBudget) wcap--;
+            for (int w = apc; w <= wcap; w++) {
+                if (p.ls_warps > 0 && w != std::min(p.ls_warps, wcap)) continue;
+                const size_t sm = local_search_smem(n_max, apc, w);
+                if (sm > kSmemBudget) continue;
+                const int res = local_search_occupancy(w, sm);
+                if (res < 1) continue;
+                const long long blocks = (total_ants + apc - 1) / apc;
+                const long long waves = (blocks + (long long)res * sm_count - 1) / ((long long)res * sm_count);
+                const long long cost = waves * ((apc * max_routes + w - 1) / w);
+                const double wpa = (double)w / apc;
+                if (best_cost < 0 || cost < best_cost || (cost == best_cost && wpa > best_wpa)) {
+                    best_cost = cost;
+                    best_wpa = wpa;
+                    ls_apc = apc;
+                    ls_warps = w;
+                    ls_smem = sm;
+                }
+            }
+        }
+        if (best_cost < 0 && (p.ls_flag & 1)) return ACO_ERR_INVALID; // the caller's shape does not fit
     }
     if (p.ls_flag & 2) { // swap stage: as many ants per CTA as their shared arrays allow, up to 8
         int n_max = 0, ld_of_max = 32;
@@ -789,7 +818,7 @@ int Colony::construct(bool fused)
 int Colony::local_search()
 {
     // after a fused construct only the ants it marked still need the 2-opt kernel
-    CK(launch_local_search(largs_d_, ant_inst_d_, ant_base_d_, total_ants, ls_warps, ls_smem, st,
+    CK(launch_local_search(largs_d_, ant_inst_d_, ant_base_d_, total_ants, ls_apc, ls_nmax, ls_warps, ls_smem, st,
                            last_fused_ ? ls_needed_d_ : nullptr));
     last_fused_ = false;
     if (p.ls_flag & 2) CK(launch_swap(cargs_d_, sw_items_d_, sw_items, sw_apc, sw_smem, kSwapLimitPerNode, st));

@@ -99,7 +99,7 @@ public:
     bool cp_stage = false;
     int cn_apc = 1, cn_lsw = 0; // throughput construct: ants per CTA, fused 2-opt warps (0 = separate kernel)
     size_t cn_smem = 0;
-    int ls_warps = 1;
+    int ls_warps = 1, ls_apc = 1, ls_nmax = 0; // 2-opt: warps and ants per CTA, largest instance
     int sw_apc = 1, sw_items = 0; // swap stage: ants per CTA, work items
     size_t sw_smem = 0;
     int ns_apc = 1, ns_items = 0; // random-descent stage

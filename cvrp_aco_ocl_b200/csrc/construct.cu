@@ -16,8 +16,12 @@
 //     turns the tournament into two redux.sync.max reductions.
 //   * value == 0 means "no candidate": return to the depot (kernel.cl:461-465).
 // construct_nn_kernel is the throughput mode (no reference counterpart):
-// warp-per-ant roulette over a nearest-neighbour candidate list staged in
-// shared memory by TMA bulk copies, with warp-shuffle prefix sums.
+// warp-per-ant sampling over a nearest-neighbour candidate list staged in
+// shared memory by TMA bulk copies.  The roulette is run as an exponential
+// race: lane j draws u_j from its own Park-Miller stream and candidate j wins
+// with the largest weight_j / -ln(u_j), which picks j with probability
+// weight_j / sum(weight) like the roulette, in one warp max-reduction instead
+// of a prefix scan (the draws are off the step's dependent chain).
 //
 // Rows of total_info and the lookup tables are staged into shared memory with
 // 1-D cp.async.bulk copies (no cluster multicast) completing on an mbarrier.
@@ -240,7 +244,7 @@ struct NNLayout {
 
 // Shared memory of one 2-opt warp of the fused construct: distance tile,
 // in-route neighbour lists and counts, route node ids.
-constexpr size_t kLsWarpBytes = 32 * 32 * 4 + 32 * 32 + 32 + 64;
+constexpr size_t kLsWarpBytes = 32 * 32 * 4 + 32 * 32 + 32 + 64 + 32 * 32 * 2;
 
 // gtab: the candidate table is read from global memory (L2) instead of being
 // staged (instances whose table does not fit next to the per-ant buffers).
@@ -302,6 +306,7 @@ __device__ void fused_ls_warp(const ConstructArgs &a, unsigned char *smem, const
     uint8_t *lnn = w + 32 * 32 * 4;
     uint8_t *lcnt = lnn + 32 * 32;
     uint16_t *rnode = reinterpret_cast<uint16_t *>(lcnt + 32);
+    uint16_t *nnbuf = rnode + 32;
     int status = ACO_OK;
     for (;;) {
         int t = 0, state = 0; // state: 1 route ready, 2 nothing left, 3 timed out
@@ -336,16 +341,21 @@ __device__ void fused_ls_warp(const ConstructArgs &a, unsigned char *smem, const
             const int v = lane < R ? (int)tb[rb + lane] : 0;
             if (lane < R) rnode[lane] = (uint16_t)v;
             __syncwarp();
+#pragma unroll 8
             for (int x = lane; x < R * kRL; x += 32) {
                 const int k1 = x >> 5, k2 = x & 31;
                 tile[x] = k2 < R ? __ldg(a.dist + (size_t)rnode[k1] * a.ld + rnode[k2]) : 0.f;
+                nnbuf[x] = k2 < a.nn_ls ? (uint16_t)__ldg(a.nn_list + (size_t)rnode[k1] * a.nn_ls + k2) : 0;
             }
+            __syncwarp();
             for (int k = 0; k < R; k++) {
                 const int node = rnode[k];
                 int c = 0;
                 for (int h0 = 0; h0 < a.nn_ls && c < R - 1; h0 += 32) {
                     const int h = h0 + lane;
-                    const int n2 = h < a.nn_ls ? __ldg(a.nn_list + (size_t)node * a.nn_ls + h) : 0;
+                    const int n2 = h >= a.nn_ls ? 0
+                                   : h0 == 0 ? (int)nnbuf[k * kRL + lane]
+                                             : __ldg(a.nn_list + (size_t)node * a.nn_ls + h);
                     const bool in = h < a.nn_ls && n2 != 0 && rid[n2] == r;
                     const unsigned m = __ballot_sync(kFullMask, in);
                     const int slot = c + __popc(m & ((1u << lane) - 1u));
@@ -374,7 +384,7 @@ __device__ void fused_ls_warp(const ConstructArgs &a, unsigned char *smem, const
 
 template <bool FIN, bool SMAT, bool PACKED, bool REGVIS, bool GTAB = false, bool LSF = false>
 __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int apc, int ant0, unsigned char *smem, uint32_t phase,
-                                  uint32_t pw, int lsw = 0)
+                                  int lsw = 0)
 {
     const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp, T = a.T;
     const int n4 = (n + 3) & ~3;
@@ -463,9 +473,9 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             __syncwarp();
         }
         if (lane == 0) tbuf[0] = 0;
+        // lane l draws from the ant's Park-Miller state l (nloc >= 32), one number a step
         int *seedp = a.seeds + (size_t)ant * a.nloc;
-        uint32_t xb = pm_norm(seedp[0]), xl = 0u;
-        float ul = 0.f;
+        uint32_t xs = pm_norm(seedp[lane]);
         int cur = 0, step = 0, vcnt = 1, load = 0, err = 0;
         float rdist = 0.f;
         const int cap = a.capacity;
@@ -476,12 +486,8 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 err = ACO_ERR_STEP_LIMIT;
                 break;
             }
-            if ((step & 31) == 0) { // the next 32 draws of the ant's stream, one per lane
-                xl = pm_mul(xb, pw);
-                ul = pm_uniform(xl);
-                xb = __shfl_sync(FULL, xl, 31);
-            }
-            const float u = __shfl_sync(FULL, ul, step & 31);
+            xs = pm_mul(xs, 16807u);
+            const float rate = race_rate(pm_uniform(xs)); // off the dependent chain of the step
             int c, dc;
             if (PACKED) {
                 const uint32_t pk = s_cand[cur * Kp + jl];
@@ -497,20 +503,11 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             if (FIN && f)
                 f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + c), a.serv_time)),
                               s_d0[c]) <= a.max_dist;
-            const float w = f ? wv : 0.f;
-            float sc = w; // inclusive Kogge-Stone scan across the warp
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const float o = __shfl_up_sync(FULL, sc, off);
-                if (lane >= off) sc = __fadd_rn(sc, o);
-            }
-            const float tw = __shfl_sync(FULL, sc, 31);
+            // exponential race: the largest wv * rate wins (probability wv / sum of wv)
+            const uint32_t hk = __reduce_max_sync(FULL, f && wv > 0.f ? race_key(wv, rate, lane) : 0u);
             int nxt = -1, nd = 0;
-            if (tw > 0.f) {
-                const float r = __fmul_rn(u, tw);
-                unsigned js = __reduce_min_sync(FULL, (w > 0.f && sc > r) ? (unsigned)lane : 32u);
-                if (js == 32u) js = __reduce_max_sync(FULL, w > 0.f ? (unsigned)lane : 0u); // rounding: last positive
-                const uint32_t pick = __shfl_sync(FULL, (uint32_t)c | ((uint32_t)dc << 16), js);
+            if (hk != 0u) {
+                const uint32_t pick = __shfl_sync(FULL, (uint32_t)c | ((uint32_t)dc << 16), 31 - (int)(hk & 31u));
                 nxt = (int)(pick & 0xFFFFu);
                 nd = (int)(pick >> 16);
             } else { // no listed candidate fits: best feasible customer of the full row
@@ -625,10 +622,7 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 a.lens[ant] = tdist;
             }
         }
-        if (step > 0) { // state after the last draw
-            const uint32_t xf = __shfl_sync(FULL, xl, (step - 1) & 31);
-            if (lane == 0) seedp[0] = (int)xf;
-        }
+        if (step > 0) seedp[lane] = (int)xs; // states after the last draw
     }
     return true;
 }
@@ -644,9 +638,6 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *
         mbar_init(bar, 1);
         fence_mbar_init();
     }
-    // 16807^(lane+1) for the batched draws
-    uint32_t pw = 16807u;
-    for (int k = 0; k < (int)(threadIdx.x & 31); k++) pw = pm_mul(pw, 16807u);
     uint32_t phase = 0;
     for (;;) {
         __syncthreads(); // the previous item is done with shared memory
@@ -659,24 +650,24 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *
         const int ant0 = code.y;
         bool ok;
         if (lsw > 0 && a.gtab) { // fused 2-opt, candidate table in global memory
-            ok = a.packed ? construct_nn_item<FIN, false, true, true, true, true>(a, apc, ant0, smem, phase, pw, lsw)
-                          : construct_nn_item<FIN, false, false, true, true, true>(a, apc, ant0, smem, phase, pw, lsw);
+            ok = a.packed ? construct_nn_item<FIN, false, true, true, true, true>(a, apc, ant0, smem, phase, lsw)
+                          : construct_nn_item<FIN, false, false, true, true, true>(a, apc, ant0, smem, phase, lsw);
         } else if (lsw > 0) { // fused 2-opt (register visited set, staged tables)
-            if (a.smat) ok = a.packed ? construct_nn_item<FIN, true, true, true, false, true>(a, apc, ant0, smem, phase, pw, lsw)
-                                      : construct_nn_item<FIN, true, false, true, false, true>(a, apc, ant0, smem, phase, pw, lsw);
-            else ok = a.packed ? construct_nn_item<FIN, false, true, true, false, true>(a, apc, ant0, smem, phase, pw, lsw)
-                               : construct_nn_item<FIN, false, false, true, false, true>(a, apc, ant0, smem, phase, pw, lsw);
+            if (a.smat) ok = a.packed ? construct_nn_item<FIN, true, true, true, false, true>(a, apc, ant0, smem, phase, lsw)
+                                      : construct_nn_item<FIN, true, false, true, false, true>(a, apc, ant0, smem, phase, lsw);
+            else ok = a.packed ? construct_nn_item<FIN, false, true, true, false, true>(a, apc, ant0, smem, phase, lsw)
+                               : construct_nn_item<FIN, false, false, true, false, true>(a, apc, ant0, smem, phase, lsw);
         } else if (a.gtab) {
-            ok = a.packed ? construct_nn_item<FIN, false, true, false, true>(a, apc, ant0, smem, phase, pw)
-                          : construct_nn_item<FIN, false, false, false, true>(a, apc, ant0, smem, phase, pw);
+            ok = a.packed ? construct_nn_item<FIN, false, true, false, true>(a, apc, ant0, smem, phase)
+                          : construct_nn_item<FIN, false, false, false, true>(a, apc, ant0, smem, phase);
         } else if (a.n <= 1024) {
-            if (a.smat) ok = a.packed ? construct_nn_item<FIN, true, true, true>(a, apc, ant0, smem, phase, pw)
-                                      : construct_nn_item<FIN, true, false, true>(a, apc, ant0, smem, phase, pw);
-            else ok = a.packed ? construct_nn_item<FIN, false, true, true>(a, apc, ant0, smem, phase, pw)
-                               : construct_nn_item<FIN, false, false, true>(a, apc, ant0, smem, phase, pw);
+            if (a.smat) ok = a.packed ? construct_nn_item<FIN, true, true, true>(a, apc, ant0, smem, phase)
+                                      : construct_nn_item<FIN, true, false, true>(a, apc, ant0, smem, phase);
+            else ok = a.packed ? construct_nn_item<FIN, false, true, true>(a, apc, ant0, smem, phase)
+                               : construct_nn_item<FIN, false, false, true>(a, apc, ant0, smem, phase);
         } else {
-            ok = a.packed ? construct_nn_item<FIN, false, true, false>(a, apc, ant0, smem, phase, pw)
-                          : construct_nn_item<FIN, false, false, false>(a, apc, ant0, smem, phase, pw);
+            ok = a.packed ? construct_nn_item<FIN, false, true, false>(a, apc, ant0, smem, phase)
+                          : construct_nn_item<FIN, false, false, false>(a, apc, ant0, smem, phase);
         }
         if (!ok) break; // uniform: decided by __syncthreads_or
         phase ^= 1u;

@@ -124,9 +124,12 @@ cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items
                                 int ls_warps = 0);
 // 2-opt: one CTA of `warps` warps per ant; d_ant_inst[g] = instance of global ant g,
 // d_ant_base[b] = first global ant of instance b.
+// 2-opt: CTAs of `ants_per_cta` ants (1..8) and `warps` warps pulling routes;
+// n_max sizes the per-ant shared buffers.  only (after a fused construct):
+// skip ants whose flag is 0 and, in the others, routes of at most 32 nodes.
 cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
-                                int total_ants, int warps, size_t smem, cudaStream_t st,
-                                const uint8_t *only = nullptr); // only: skip ants whose flag is 0
+                                int total_ants, int ants_per_cta, int n_max, int warps, size_t smem, cudaStream_t st,
+                                const uint8_t *only = nullptr);
 cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st);
 // Row passes (heuristic matrix, pheromone init, fused update, candidate gather):
 // one warp per row over all instances; d_row_base[b] = first global row of instance b.
@@ -140,7 +143,9 @@ size_t construct_parity_smem(int n, int nloc, int kmax, int warps_per_ant, int a
                              bool finite_maxd);
 size_t construct_nn_smem(int n, int K, int Kp, int ants_per_cta, bool stage_total, bool packed,
                          bool global_table = false, int ls_warps = 0);
-size_t local_search_smem(int n, int warps);
+size_t local_search_smem(int n_max, int ants_per_cta, int warps);
+// resident 2-opt CTAs per SM for this shape (0 = cannot launch)
+int local_search_occupancy(int warps, size_t smem);
 
 // Tour validation (validate.cu): flags[slot_base[b] + s] = 1 if slot s of
 // instance b (ants, then best-so-far) is a valid tour whose stored length is

@@ -40,13 +40,16 @@ namespace {
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
 
-struct LsLayout {
-    size_t tour, pos, li, rid, dlb, rstart, dt, tiles, lnn, lcnt, rnodes, bytes;
+// Shared memory: one block per ant of the CTA (sized for the colony's largest
+// instance), then one block per warp.
+struct LsAnt {
+    size_t tour, pos, li, rid, dlb, rstart, dt, bytes;
 };
 
-__host__ __device__ inline LsLayout ls_layout(int n, int T, int warps)
+__host__ __device__ inline LsAnt ls_ant_layout(int n)
 {
-    LsLayout L;
+    const int T = 2 * n;
+    LsAnt L;
     size_t o = 0;
     L.tour = o; o = al16(o + (size_t)T * 2);
     L.pos = o; o = al16(o + (size_t)n * 2);
@@ -55,15 +58,21 @@ __host__ __device__ inline LsLayout ls_layout(int n, int T, int warps)
     L.dlb = o; o = al16(o + (size_t)n);
     L.rstart = o; o = al16(o + (size_t)(n + 1) * 2);
     L.dt = o; o = al16(o + (size_t)T * 4);
-    L.tiles = o; o = al16(o + (size_t)warps * kRL * kRL * 4);
-    L.lnn = o; o = al16(o + (size_t)warps * kRL * kRL);
-    L.lcnt = o; o = al16(o + (size_t)warps * kRL);
-    L.rnodes = o; o = al16(o + (size_t)warps * kRL * 2);
     L.bytes = o;
     return L;
 }
 
+// per warp: distance tile; the first 32 list entries of every route node
+// (uint16), overwritten in place by the in-route neighbour lists (uint8: row k
+// lands on bytes of rows <= k/2, already consumed); list counts; route nodes
+constexpr size_t kLsWarp = kRL * kRL * 4 + kRL * 32 * 2 + kRL + kRL * 2;
+constexpr int kMaxLsAnts = 8;
 constexpr unsigned FULL = 0xffffffffu;
+
+__host__ __device__ inline size_t ls_smem_bytes(int n_max, int apc, int warps)
+{
+    return (size_t)apc * ls_ant_layout(n_max).bytes + (size_t)warps * kLsWarp;
+}
 
 // ---------------------------------------------------------------------------
 // Generic path: any route length, shared-memory arrays, global distances.
@@ -221,86 +230,153 @@ __device__ int two_opt_route_generic(Route &c, int pass_limit)
 }
 
 __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArgs *args, const int *ant_inst,
-                                                             const int *ant_base, const uint8_t *only)
+                                                             const int *ant_base, const uint8_t *only, int apc,
+                                                             int n_max, int total_ants)
 {
-    if (only && !only[blockIdx.x]) return; // improved already (fused with the construct)
     extern __shared__ __align__(128) unsigned char smem[];
-    const int b = __ldg(ant_inst + blockIdx.x);
-    const LocalSearchArgs a = args[b];
-    const int ant = blockIdx.x - __ldg(ant_base + b);
-    const int n = a.n, T = a.T;
+    __shared__ int s_inst[kMaxLsAnts], s_ant[kMaxLsAnts], s_size[kMaxLsAnts], s_routes[kMaxLsAnts + 1];
+    __shared__ int s_next;
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const LsLayout L = ls_layout(n, T, W);
-    uint16_t *tour = reinterpret_cast<uint16_t *>(smem + L.tour);
-    uint16_t *pos = reinterpret_cast<uint16_t *>(smem + L.pos);
-    uint8_t *li = reinterpret_cast<uint8_t *>(smem + L.li);
-    uint16_t *rid = reinterpret_cast<uint16_t *>(smem + L.rid);
-    uint8_t *dlb = reinterpret_cast<uint8_t *>(smem + L.dlb);
-    uint16_t *rstart = reinterpret_cast<uint16_t *>(smem + L.rstart);
-    float *dt = reinterpret_cast<float *>(smem + L.dt);
-    float *tile = reinterpret_cast<float *>(smem + L.tiles) + (size_t)warp * kRL * kRL;
-    uint8_t *lnn = reinterpret_cast<uint8_t *>(smem + L.lnn) + (size_t)warp * kRL * kRL;
-    uint8_t *lcnt = reinterpret_cast<uint8_t *>(smem + L.lcnt) + (size_t)warp * kRL;
-    uint16_t *rnode = reinterpret_cast<uint16_t *>(smem + L.rnodes) + (size_t)warp * kRL;
-    __shared__ int s_routes, s_next;
+    const LsAnt AL = ls_ant_layout(n_max);
+    unsigned char *wbase = smem + (size_t)apc * AL.bytes + (size_t)warp * kLsWarp;
+    float *tile = reinterpret_cast<float *>(wbase);
+    uint16_t *nnbuf = reinterpret_cast<uint16_t *>(wbase + kRL * kRL * 4);
+    uint8_t *lnn = reinterpret_cast<uint8_t *>(nnbuf);
+    uint8_t *lcnt = lnn + kRL * 32 * 2;
+    uint16_t *rnode = reinterpret_cast<uint16_t *>(lcnt + kRL);
+    auto ant_ptr = [&](int j, size_t off) { return smem + (size_t)j * AL.bytes + off; };
 
-    int *gtour = a.solutions + (size_t)ant * T;
-    const int size = gtour[T - 1];
-    if (size < 2) return; // a failed construction has nothing to improve (uniform over the CTA)
-
-    // local_search (kernel.cl:517-523) + two_opt_solution set-up (:293-300)
-    for (int p = threadIdx.x; p < size; p += blockDim.x) {
-        const int v = gtour[p];
-        tour[p] = (uint16_t)v;
-        if (v != 0) pos[v] = (uint16_t)p;
+    // the CTA's ants: global ants [blockIdx.x * apc, ... + apc)
+    if (threadIdx.x < apc) {
+        const int j = threadIdx.x, g = blockIdx.x * apc + j;
+        int inst = -1, ant = 0, size = 0;
+        if (g < total_ants && (!only || only[g])) { // `only`: the ants a fused construct left to this kernel
+            inst = __ldg(ant_inst + g);
+            ant = g - __ldg(ant_base + inst);
+            const LocalSearchArgs &a = args[inst];
+            size = a.solutions[(size_t)ant * a.T + a.T - 1];
+            if (size < 2) inst = -1; // a failed construction has nothing to improve
+        }
+        s_inst[j] = inst;
+        s_ant[j] = ant;
+        s_size[j] = inst >= 0 ? size : 0;
     }
-    for (int v = threadIdx.x; v < n; v += blockDim.x) dlb[v] = 0;
     __syncthreads();
-    for (int p = threadIdx.x; p < size - 1; p += blockDim.x)
-        dt[p] = __ldg(a.dist + (size_t)tour[p] * a.ld + tour[p + 1]);
-    if (warp == 0) { // route table: depot positions in order
+
+    // local_search (kernel.cl:517-523) + two_opt_solution set-up (:293-300), per ant
+    for (int j = 0; j < apc; j++) {
+        if (s_inst[j] < 0) continue;
+        const LocalSearchArgs &a = args[s_inst[j]];
+        const int *gtour = a.solutions + (size_t)s_ant[j] * a.T;
+        uint16_t *tour = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.tour));
+        uint16_t *pos = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.pos));
+        uint8_t *dlb = ant_ptr(j, AL.dlb);
+        for (int p = threadIdx.x; p < s_size[j]; p += blockDim.x) {
+            const int v = gtour[p];
+            tour[p] = (uint16_t)v;
+            if (v != 0) pos[v] = (uint16_t)p;
+        }
+        for (int v = threadIdx.x; v < a.n; v += blockDim.x) dlb[v] = 0;
+    }
+    __syncthreads();
+    for (int j = 0; j < apc; j++) {
+        if (s_inst[j] < 0) continue;
+        const LocalSearchArgs &a = args[s_inst[j]];
+        const uint16_t *tour = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.tour));
+        float *dt = reinterpret_cast<float *>(ant_ptr(j, AL.dt));
+        for (int p = threadIdx.x; p < s_size[j] - 1; p += blockDim.x)
+            dt[p] = __ldg(a.dist + (size_t)tour[p] * a.ld + tour[p + 1]);
+    }
+    if (warp < apc) { // route table of ant `warp`: depot positions in order
+        const int j = warp;
         int count = 0;
-        for (int base = 0; base < size; base += 32) {
-            const int p = base + lane;
-            const bool dep = p < size && tour[p] == 0;
-            const unsigned m = __ballot_sync(FULL, dep);
-            if (dep) rstart[count + __popc(m & ((1u << lane) - 1u))] = (uint16_t)p;
-            count += __popc(m);
+        if (s_inst[j] >= 0) {
+            const uint16_t *tour = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.tour));
+            uint16_t *rstart = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.rstart));
+            const int size = s_size[j];
+            for (int base = 0; base < size; base += 32) {
+                const int p = base + lane;
+                const bool dep = p < size && tour[p] == 0;
+                const unsigned m = __ballot_sync(FULL, dep);
+                if (dep) rstart[count + __popc(m & ((1u << lane) - 1u))] = (uint16_t)p;
+                count += __popc(m);
+            }
+            count -= 1;
         }
-        if (lane == 0) {
-            s_routes = count - 1;
-            s_next = W;
-        }
+        if (lane == 0) s_routes[j] = count;
     }
     __syncthreads();
-    const int routes = s_routes;
-    for (int r = warp; r < routes; r += W) // route id and local index of every customer
+    if (threadIdx.x == 0) { // routes of ant j are flattened after those of ants < j
+        int acc = 0;
+        for (int j = 0; j < apc; j++) {
+            const int c = s_routes[j];
+            s_routes[j] = acc;
+            acc += c;
+        }
+        s_routes[apc] = acc;
+        s_next = W;
+    }
+    __syncthreads();
+    const int total_routes = s_routes[apc];
+    auto locate = [&](int f, int &j, int &r) { // flattened route f -> (ant j, route r)
+        j = 0;
+        while (j + 1 < apc && s_routes[j + 1] <= f) j++;
+        r = f - s_routes[j];
+    };
+    for (int f = warp; f < total_routes; f += W) { // route id and local index of every customer
+        int j, r;
+        locate(f, j, r);
+        const uint16_t *tour = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.tour));
+        const uint16_t *rstart = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.rstart));
+        uint16_t *rid = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.rid));
+        uint8_t *li = ant_ptr(j, AL.li);
         for (int p = rstart[r] + 1 + lane; p < rstart[r + 1]; p += 32) {
             rid[tour[p]] = (uint16_t)r;
             li[tour[p]] = (uint8_t)(p - rstart[r] < 256 ? p - rstart[r] : 0);
         }
+    }
     __syncthreads();
 
-    int status = ACO_OK;
-    for (int r = warp; r < routes;) {
+    int status = ACO_OK, status_inst = 0;
+    for (int f = warp; f < total_routes;) {
+        int j, r;
+        locate(f, j, r);
+        const LocalSearchArgs a = args[s_inst[j]];
+        uint16_t *tour = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.tour));
+        uint16_t *pos = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.pos));
+        uint8_t *li = ant_ptr(j, AL.li);
+        uint16_t *rid = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.rid));
+        uint8_t *dlb = ant_ptr(j, AL.dlb);
+        const uint16_t *rstart = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.rstart));
+        float *dt = reinterpret_cast<float *>(ant_ptr(j, AL.dt));
         const int rb = rstart[r], re = rstart[r + 1] - 1, R = re - rb + 1;
-        int st;
-        if (R <= kRL) {
+        int st = ACO_OK;
+        if (R <= kRL && only) {
+            // after a fused construct the routes of at most 32 nodes are improved
+            // already; only the longer ones of a flagged ant are left here
+        } else if (R <= kRL) {
             // route-local state: node ids, distance tile, in-route neighbour lists
             const int v = lane < R ? (int)tour[rb + lane] : 0;
             if (lane < R) rnode[lane] = (uint16_t)v;
             __syncwarp();
+            // the distance tile and the first 32 list entries of every route node,
+            // loads issued ahead of their uses
+#pragma unroll 8
             for (int e = lane; e < R * kRL; e += 32) {
                 const int k1 = e >> 5, k2 = e & 31;
                 tile[e] = k2 < R ? __ldg(a.dist + (size_t)rnode[k1] * a.ld + rnode[k2]) : 0.f;
+                nnbuf[e] = k2 < a.nn_ls ? (uint16_t)__ldg(a.nn_list + (size_t)rnode[k1] * a.nn_ls + k2) : 0;
             }
+            __syncwarp();
             for (int k = 0; k < R; k++) {
                 const int node = rnode[k];
                 int cnt = 0;
                 for (int h0 = 0; h0 < a.nn_ls && cnt < R - 1; h0 += 32) {
                     const int h = h0 + lane;
-                    const int n2 = h < a.nn_ls ? __ldg(a.nn_list + (size_t)node * a.nn_ls + h) : 0;
+                    const int n2 = h >= a.nn_ls ? 0
+                                   : h0 == 0 ? (int)nnbuf[k * kRL + lane]
+                                             : __ldg(a.nn_list + (size_t)node * a.nn_ls + h);
                     const bool in = h < a.nn_ls && n2 != 0 && rid[n2] == r;
                     const unsigned m = __ballot_sync(FULL, in);
                     const int slot = cnt + __popc(m & ((1u << lane) - 1u));
@@ -327,16 +403,27 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
             c.r = r; c.rb = rb; c.re = re; c.dlb0 = r > 0;
             st = two_opt_route_generic(c, a.pass_limit);
         }
-        if (st != ACO_OK && status == ACO_OK) status = st;
+        if (st != ACO_OK && status == ACO_OK) {
+            status = st;
+            status_inst = s_inst[j];
+        }
         int nxt = 0;
         if (lane == 0) nxt = atomicAdd(&s_next, 1);
-        r = __shfl_sync(FULL, nxt, 0);
+        f = __shfl_sync(FULL, nxt, 0);
     }
-    if (status != ACO_OK && lane == 0) set_status(a.status, status);
+    if (status != ACO_OK && lane == 0) set_status(args[status_inst].status, status);
     __syncthreads();
 
-    for (int p = threadIdx.x; p < size; p += blockDim.x) gtour[p] = tour[p]; // kernel.cl:530-532
-    if (warp == 0) { // kernel.cl:534-538: fp32 sum of dist_tour_wrk in position order
+    for (int j = 0; j < apc; j++) {
+        if (s_inst[j] < 0) continue;
+        const LocalSearchArgs &a = args[s_inst[j]];
+        int *gtour = a.solutions + (size_t)s_ant[j] * a.T;
+        const uint16_t *tour = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.tour));
+        for (int p = threadIdx.x; p < s_size[j]; p += blockDim.x) gtour[p] = tour[p]; // kernel.cl:530-532
+    }
+    if (warp < apc && s_inst[warp] >= 0) { // kernel.cl:534-538: fp32 sum of dist_tour_wrk in position order
+        const int j = warp, size = s_size[j];
+        const float *dt = reinterpret_cast<const float *>(ant_ptr(j, AL.dt));
         float len = 0.f;
         for (int base = 0; base < size - 1; base += 32) {
             const float e = base + lane < size - 1 ? dt[base + lane] : 0.f;
@@ -347,20 +434,34 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
                 if (k < m) len = __fadd_rn(len, x);
             }
         }
-        if (lane == 0) a.lens[ant] = len;
+        if (lane == 0) args[s_inst[j]].lens[s_ant[j]] = len;
     }
 }
 
 } // namespace
 
-size_t local_search_smem(int n, int warps) { return ls_layout(n, 2 * n, warps).bytes; }
+size_t local_search_smem(int n_max, int ants_per_cta, int warps) { return ls_smem_bytes(n_max, ants_per_cta, warps); }
+
+int local_search_occupancy(int warps, size_t smem)
+{
+    if (cudaFuncSetAttribute(local_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, local_search_kernel, warps * 32, smem) != cudaSuccess)
+        return 0;
+    return blocks;
+}
 
 cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
-                                int total_ants, int warps, size_t smem, cudaStream_t st, const uint8_t *only)
+                                int total_ants, int ants_per_cta, int n_max, int warps, size_t smem, cudaStream_t st,
+                                const uint8_t *only)
 {
+    if (ants_per_cta < 1 || ants_per_cta > kMaxLsAnts || warps < ants_per_cta) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(local_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    local_search_kernel<<<total_ants, warps * 32, smem, st>>>(d_args, d_ant_inst, d_ant_base, only);
+    const int blocks = (total_ants + ants_per_cta - 1) / ants_per_cta;
+    local_search_kernel<<<blocks, warps * 32, smem, st>>>(d_args, d_ant_inst, d_ant_base, only, ants_per_cta, n_max,
+                                                          total_ants);
     return cudaGetLastError();
 }
 

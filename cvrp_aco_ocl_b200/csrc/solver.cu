@@ -69,6 +69,7 @@ int check_params(const aco_params &p, int n)
     if (p.ls_flag != 0 && p.ls_flag != 1 && p.ls_flag != 3) return ACO_ERR_INVALID;
     if (p.ns_rounds < 0 || p.ns_rounds > 1000000) return ACO_ERR_INVALID;
     if (p.fuse_ls < 0 || p.fuse_ls > 1) return ACO_ERR_INVALID;
+    if (p.ls_ants < 0 || p.ls_ants > 8) return ACO_ERR_INVALID;
     if (!(p.rho > 0.0f && p.rho <= 1.0f)) return ACO_ERR_INVALID;
     if (p.n_ants > 56 * 1024) return ACO_ERR_INVALID; // the statistics kernel holds n_ants lengths in shared memory
     return ACO_OK;
@@ -768,22 +769,30 @@ int autotune(const InstanceSpec *specs, int count, const aco_params &p0, int ite
         }
     }
     if (!any) return ACO_ERR_INVALID;
-    // 2-opt CTA width with the chosen construct
-    if (p0.ls_flag && p0.ls_warps == 0) {
+    // 2-opt CTA shape (ants x warps) with the chosen construct
+    if (p0.ls_flag && (p0.ls_warps == 0 || p0.ls_ants == 0)) {
         float best_l = best_ph[1];
-        int best_w = 0;
-        for (int w : {4, 8, 16, 32}) {
-            aco_params q = best;
-            q.ls_warps = w;
-            float ph[4];
-            if (time_config(specs, count, q, iters, ph) != ACO_OK) continue;
-            if (ph[1] < best_l) {
-                best_l = ph[1];
-                best_w = w;
-                std::memcpy(best_ph, ph, sizeof(ph));
-                best_ph[0] = best_c;
+        int best_a = p0.ls_ants, best_w = p0.ls_warps;
+        for (int an : {1, 2, 4}) {
+            if (p0.ls_ants != 0 && an != p0.ls_ants) continue;
+            for (int w : {8, 12, 16, 24, 32}) {
+                if (p0.ls_warps != 0 && w != p0.ls_warps) continue;
+                if (w < an) continue;
+                aco_params q = best;
+                q.ls_ants = an;
+                q.ls_warps = w;
+                float ph[4];
+                if (time_config(specs, count, q, iters, ph) != ACO_OK) continue;
+                if (ph[1] < best_l) {
+                    best_l = ph[1];
+                    best_a = an;
+                    best_w = w;
+                    std::memcpy(best_ph, ph, sizeof(ph));
+                    best_ph[0] = best_c;
+                }
             }
         }
+        best.ls_ants = best_a;
         best.ls_warps = best_w;
     }
     *out = best;

@@ -30,6 +30,16 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
 {
     // lane q: tq = local node at position q, dq = dist_tour_wrk of position q;
     // lane k: pk = position of local node k.  Local node 0 is the depot at position 0.
+    //
+    // The scan visits positions q1 = 0, 1, ..., R-1 and skips a node whose
+    // don't-look bit is set.  `open` holds one bit per position whose node's bit
+    // is clear, rebuilt whenever a move changes the tour or the bits, so the next
+    // position to examine is a bit operation away.  For each examined node the
+    // successor and the predecessor searches (kernel.cl:180-198, 202-230) are
+    // evaluated together; the predecessor result is used only when the successor
+    // search finds no move, as in the sequential code.
+    const unsigned FULLM = 0xffffffffu;
+    const unsigned rmask = R >= 32 ? FULLM : ((1u << R) - 1u);
     uint32_t dlb = first_route ? 0u : 1u; // bit k: don't-look bit of local node k
     int passes = 0;
     bool imp = true;
@@ -37,89 +47,81 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
         if (pass_limit > 0 && passes >= pass_limit) return ACO_ERR_LS_LIMIT;
         passes++;
         imp = false;
-        for (int q1 = 0; q1 < R; q1++) {
-            const int k1 = __shfl_sync(kFullMask, tq, q1);
-            if ((dlb >> k1) & 1u) continue;
+        uint32_t open = __ballot_sync(FULLM, lane < R && !((dlb >> tq) & 1u)) & rmask;
+        int q1 = -1;
+        for (;;) {
+            const uint32_t ahead = q1 < 0 ? open : (q1 >= 31 ? 0u : (open & ~((2u << q1) - 1u))); // positions > q1
+            if (!ahead) break;
+            q1 = __ffs(ahead) - 1;
+            // every shuffle below is independent of the others at its level
+            const int k1 = __shfl_sync(FULLM, tq, q1);
+            const int ks1 = __shfl_sync(FULLM, tq, q1 + 1 < R ? q1 + 1 : 0);
+            const int kp1 = __shfl_sync(FULLM, tq, q1 > 0 ? q1 - 1 : R - 1);
             const int cnt = lcnt[k1];
             const int j = lane;
-            const int k2 = j < cnt ? lnn[k1 * kRL + j] : 0;
+            const bool act = j < cnt;
+            const int k2 = act ? lnn[k1 * kRL + j] : 0;
             const float d12 = tile[k1 * kRL + k2];
-            const int q2 = __shfl_sync(kFullMask, pk, k2);
-            bool found = false;
-            int h1 = 0, h2 = 0, h3 = 0, h4 = 0;
-            // successor search (kernel.cl:180-198)
-            {
-                const int ks1 = __shfl_sync(kFullMask, tq, q1 + 1 < R ? q1 + 1 : 0);
-                const float radius = tile[k1 * kRL + ks1];
-                const int ks2 = __shfl_sync(kFullMask, tq, q2 + 1 < R ? q2 + 1 : 0);
-                const float dq2 = __shfl_sync(kFullMask, dq, q2);
-                const bool act = j < cnt;
-                const bool cond = act && __fsub_rn(radius, d12) > kEps;
-                bool okm = false;
-                if (cond) {
-                    const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), tile[ks1 * kRL + ks2]), dq2);
-                    okm = g < -kEps;
-                }
-                const unsigned stop = __ballot_sync(kFullMask, act && (!cond || okm));
-                if (stop) {
-                    const int f = __ffs(stop) - 1;
-                    if (__shfl_sync(kFullMask, (int)cond, f)) {
-                        found = true;
-                        h1 = k1;
-                        h2 = ks1;
-                        h3 = __shfl_sync(kFullMask, k2, f);
-                        h4 = __shfl_sync(kFullMask, ks2, f);
-                    }
-                }
+            const float rs = tile[k1 * kRL + ks1];  // successor radius
+            const float rp = tile[kp1 * kRL + k1];  // predecessor radius
+            const int q2 = __shfl_sync(FULLM, pk, k2);
+            const int ks2 = __shfl_sync(FULLM, tq, q2 + 1 < R ? q2 + 1 : 0);
+            const int kpp2 = __shfl_sync(FULLM, tq, q2 > 0 ? q2 - 1 : R - 1);
+            const float dq2 = __shfl_sync(FULLM, dq, q2);
+            const float dqp2 = __shfl_sync(FULLM, dq, q2 > 0 ? q2 - 1 : 0);
+            const bool sc = act && __fsub_rn(rs, d12) > kEps;
+            const bool pc = act && __fsub_rn(rp, d12) > kEps;
+            bool sok = false, pok = false;
+            if (sc) {
+                const float g = __fsub_rn(__fadd_rn(__fadd_rn(-rs, d12), tile[ks1 * kRL + ks2]), dq2);
+                sok = g < -kEps;
             }
-            if (!found) { // predecessor search (kernel.cl:202-230)
-                const int kp1 = __shfl_sync(kFullMask, tq, q1 > 0 ? q1 - 1 : R - 1);
-                const float radius = tile[kp1 * kRL + k1];
-                const int kpp2 = __shfl_sync(kFullMask, tq, q2 > 0 ? q2 - 1 : R - 1);
-                const float dqp2 = __shfl_sync(kFullMask, dq, q2 > 0 ? q2 - 1 : 0);
-                const bool act = j < cnt;
-                const bool cond = act && __fsub_rn(radius, d12) > kEps;
-                bool okm = false;
-                if (cond && !(kpp2 == k1 || kp1 == k2)) {
-                    const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), tile[kp1 * kRL + kpp2]), dqp2);
-                    okm = g < -kEps;
-                }
-                const unsigned stop = __ballot_sync(kFullMask, act && (!cond || okm));
-                if (stop) {
-                    const int f = __ffs(stop) - 1;
-                    if (__shfl_sync(kFullMask, (int)cond, f)) {
-                        found = true;
-                        h1 = kp1;
-                        h2 = k1;
-                        h3 = __shfl_sync(kFullMask, kpp2, f);
-                        h4 = __shfl_sync(kFullMask, k2, f);
-                    }
-                }
+            if (pc && !(kpp2 == k1 || kp1 == k2)) {
+                const float g = __fsub_rn(__fadd_rn(__fadd_rn(-rp, d12), tile[kp1 * kRL + kpp2]), dqp2);
+                pok = g < -kEps;
             }
-            if (!found) {
+            const unsigned sstop = __ballot_sync(FULLM, act && (!sc || sok));
+            const unsigned pstop = __ballot_sync(FULLM, act && (!pc || pok));
+            const int sf = sstop ? __ffs(sstop) - 1 : 0, pf = pstop ? __ffs(pstop) - 1 : 0;
+            const bool sfound = sstop && __shfl_sync(FULLM, (int)sc, sf);
+            const bool pfound = pstop && __shfl_sync(FULLM, (int)pc, pf);
+            int h1, h2, h3, h4;
+            if (sfound) {
+                h1 = k1;
+                h2 = ks1;
+                h3 = __shfl_sync(FULLM, k2, sf);
+                h4 = __shfl_sync(FULLM, ks2, sf);
+            } else if (pfound) {
+                h1 = kp1;
+                h2 = k1;
+                h3 = __shfl_sync(FULLM, kpp2, pf);
+                h4 = __shfl_sync(FULLM, k2, pf);
+            } else {
                 dlb |= 1u << k1; // kernel.cl:232
+                open &= ~(1u << q1);
                 continue;
             }
             // exchange (kernel.cl:235-270)
             imp = true;
             dlb &= ~((1u << h1) | (1u << h2) | (1u << h3) | (1u << h4));
-            int p1 = __shfl_sync(kFullMask, pk, h1), p3 = __shfl_sync(kFullMask, pk, h3);
+            int p1 = __shfl_sync(FULLM, pk, h1), p3 = __shfl_sync(FULLM, pk, h3);
             if (p3 < p1) {
                 int t = h1; h1 = h3; h3 = t;
                 t = h2; h2 = h4; h4 = t;
                 t = p1; p1 = p3; p3 = t;
             }
-            const int i = p1, jj = p3, a = __shfl_sync(kFullMask, pk, h2);
+            const int i = p1, jj = p3, a = __shfl_sync(FULLM, pk, h2);
             const float d13 = tile[h1 * kRL + h3], d24 = tile[h2 * kRL + h4];
             // dist_tour_wrk: [i] = d(h1,h3), [jj] = d(h2,h4), (i, jj) reversed
-            const float dsrc = __shfl_sync(kFullMask, dq, (lane > i && lane < jj) ? i + jj - lane : lane);
+            const float dsrc = __shfl_sync(FULLM, dq, (lane > i && lane < jj) ? i + jj - lane : lane);
             if (lane == jj) dq = d24; // written after [i], as kernel.cl:249-250
             else if (lane == i) dq = d13;
             else if (lane > i && lane < jj) dq = dsrc;
             // tour positions [a, jj] reversed; positions of the moved nodes mirrored
-            const int tsrc = __shfl_sync(kFullMask, tq, (lane >= a && lane <= jj) ? a + jj - lane : lane);
+            const int tsrc = __shfl_sync(FULLM, tq, (lane >= a && lane <= jj) ? a + jj - lane : lane);
             if (lane >= a && lane <= jj) tq = tsrc;
             if (pk >= a && pk <= jj) pk = a + jj - pk;
+            open = __ballot_sync(FULLM, lane < R && !((dlb >> tq) & 1u)) & rmask; // the tour and bits changed
         }
     }
     return ACO_OK;

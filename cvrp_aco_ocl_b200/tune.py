@@ -2,7 +2,7 @@
 
 ``aco_autotune`` / ``aco_batch_autotune`` (C ABI) time the launch shapes on
 the device -- ants per construct CTA, matrix staging (throughput) or warps per
-ant (parity), warps per 2-opt CTA -- and return the fastest.  Every shape
+ant (parity), ants and warps per 2-opt CTA -- and return the fastest.  Every shape
 computes the same result bit for bit, so the choice is a pure speed question.
 This module runs them over a ladder of sizes, stores the winners as a JSON
 table keyed by mode, node-count range and ant count, and fills the ``0 =
@@ -26,7 +26,7 @@ from typing import Dict, List, Optional, Sequence, Tuple
 from . import _lib
 from ._lib import AcoInstance, AcoParams, check, lib
 
-SHAPE_FIELDS = ("ants_per_block", "warps_per_ant", "ls_warps", "stage_matrix")
+SHAPE_FIELDS = ("ants_per_block", "warps_per_ant", "ls_warps", "stage_matrix", "ls_ants")
 
 
 @dataclasses.dataclass
@@ -41,6 +41,7 @@ class TuneEntry:
     stage_matrix: int
     ms_per_iter: float
     nn_ants: int = 0  # list length the entry was timed with (0 = not recorded)
+    ls_ants: int = 0  # ants per 2-opt CTA (0 = the library's default)
 
 
 class TuneTable:
@@ -144,11 +145,11 @@ def build_table(sizes: Sequence[int], ants: int, mode: int = _lib.MODE_THROUGHPU
         t0 = time.perf_counter()
         out, ms = autotune(prob, p, iters)
         e = TuneEntry(mode, lo, hi, ants, out.ants_per_block, out.warps_per_ant, out.ls_warps, out.stage_matrix,
-                      ms, p.nn_ants)
+                      ms, p.nn_ants, out.ls_ants)
         table.add(e)
         if log:
             log(f"n={n} [{lo},{hi}] ants={ants}: apc={e.ants_per_block} wpa={e.warps_per_ant} "
-                f"ls_warps={e.ls_warps} stage={e.stage_matrix} {ms:.3f} ms/iter ({time.perf_counter() - t0:.1f} s)")
+                f"ls_warps={e.ls_warps} ls_ants={e.ls_ants} stage={e.stage_matrix} {ms:.3f} ms/iter ({time.perf_counter() - t0:.1f} s)")
     return table
 
 

@@ -99,6 +99,7 @@ typedef struct aco_params {
     int ns_rounds;        /* random-descent stage after the local search: proposals of the reference's
                              random neighbourhood moves (neighbourSearch.cpp, move.cpp) per ant and iteration,
                              the valid improving ones applied; 0 = off (default) */
+    int ls_ants;          /* 0 = autotuned; else ants per 2-opt CTA (1..8), whose routes its warps share */
 } aco_params;
 
 /* One best-so-far record {iteration, length, seconds since init} (problem.h:62-66). */

@@ -846,12 +846,43 @@ int orc_run_aco_iteration(orc_state *s, int n_threads)
 
 /* ---------------------------------------------------------------------- */
 /* Throughput mode: this project's candidate-list sampler (no reference    */
-/* counterpart).  One uniform per step from the ant's lane-0 Park-Miller   */
-/* state; the first nn_ants entries of the NN list are the candidates;     */
-/* roulette over their choice_info by a 32-wide Kogge-Stone inclusive scan  */
-/* (fp32, the order a warp computes it); full-row argmax fallback over all  */
-/* feasible customers when no candidate has weight; depot return otherwise. */
+/* counterpart).  Lane j (0..31) of an ant owns its Park-Miller state j and */
+/* draws u_j every step; the first nn_ants entries of the NN list are the  */
+/* candidates, and the feasible one with the largest choice_info / -ln(u_j) */
+/* wins (exponential race: the roulette's probabilities), keyed as the     */
+/* device does it; full-row argmax fallback over all feasible customers    */
+/* when no candidate has weight; depot return otherwise.                   */
 /* ---------------------------------------------------------------------- */
+static float f_of_bits(uint32_t b) { float f; memcpy(&f, &b, 4); return f; }
+static uint32_t bits_of_f(float f) { uint32_t b; memcpy(&b, &f, 4); return b; }
+
+/* ln(u) = e*ln2 + 2*atanh((m-1)/(m+1)), m in [sqrt(1/2), sqrt(2)), odd series
+ * of atanh to s^9 -- the device's race_ln operation for operation. */
+float orc_race_ln(float u)
+{
+    const uint32_t b = bits_of_f(u);
+    int e = (int)(b >> 23) - 127;
+    float m = f_of_bits((b & 0x007fffffu) | 0x3f800000u);
+    if (m > 1.41421354f) { m = m * 0.5f; e += 1; }
+    const float t = m - 1.0f;
+    const float s = t / (t + 2.0f);
+    const float s2 = s * s;
+    float p = fmaf(s2, 1.0f / 9.0f, 1.0f / 7.0f);
+    p = fmaf(s2, p, 1.0f / 5.0f);
+    p = fmaf(s2, p, 1.0f / 3.0f);
+    p = s2 * p;
+    const float ls = 2.0f * fmaf(s, p, s);
+    return fmaf((float)e, 0.693147182f, ls);
+}
+
+/* The device's race_key: bits of w / -ln(u), low 5 bits = 31 - lane. */
+static uint32_t race_key(float w, float u, int lane)
+{
+    const float rate = 1.0f / (0.0f - orc_race_ln(u));
+    const uint32_t b = bits_of_f(w * rate) & ~31u;
+    return (b < 32u ? 32u : b) | (uint32_t)(31 - lane);
+}
+
 static int construct_nn_one(const orc_state *s, int ant, const int *nnl, int K,
                             unsigned char *visited, float *dist0)
 {
@@ -866,39 +897,21 @@ static int construct_nn_one(const orc_state *s, int ant, const int *nnl, int K,
     tour[0] = 0;
     while (visited_cnt < n) {
         if (step >= T - 3) { tour[T - 1] = 0; s->lens[ant] = INFINITY; return ORC_ERR_STEP_LIMIT; }
-        float u = orc_ran01(seed);
-        float wv[32], sc[32];
-        int cnd[32];
-        for (int j = 0; j < 32; j++) {
-            wv[j] = 0.0f; cnd[j] = 0;
-            if (j < K) {
-                int c = nnl[(size_t)cur * K + j];
-                cnd[j] = c;
-                const float dc = dist[(size_t)cur * n + c];
-                if (!visited[c] && route_load + s->demand[c] <= s->capacity &&
-                    route_dist + (dc + s->serv_time) + dist0[c] <= s->max_dist)
-                    wv[j] = total[(size_t)cur * n + c];
-            }
-            sc[j] = wv[j];
-        }
-        for (int off = 1; off < 32; off <<= 1) {
-            float prev[32];
-            for (int j = 0; j < 32; j++) prev[j] = sc[j];
-            for (int j = off; j < 32; j++) sc[j] = prev[j] + prev[j - off];
-        }
-        float tw = sc[31];
+        float u[32];
+        for (int j = 0; j < 32; j++) u[j] = orc_ran01(&seed[j]);
+        uint32_t hk = 0;
         int nxt = -1;
-        if (tw > 0.0f) {
-            float r = u * tw;
-            int last = -1;
-            for (int j = 0; j < 32; j++) {
-                if (wv[j] > 0.0f) {
-                    last = j;
-                    if (sc[j] > r) { nxt = cnd[j]; break; }
-                }
+        for (int j = 0; j < K; j++) {
+            const int c = nnl[(size_t)cur * K + j];
+            const float dc = dist[(size_t)cur * n + c];
+            const float w = total[(size_t)cur * n + c];
+            if (!visited[c] && route_load + s->demand[c] <= s->capacity &&
+                route_dist + (dc + s->serv_time) + dist0[c] <= s->max_dist && w > 0.0f) {
+                const uint32_t key = race_key(w, u[j], j);
+                if (key > hk) { hk = key; nxt = c; }
             }
-            if (nxt < 0) nxt = cnd[last];
-        } else {
+        }
+        if (hk == 0) {
             float bv = -1.0f;
             for (int i = 1; i < n; i++) {
                 const float di = dist[(size_t)cur * n + i];
