@@ -67,6 +67,7 @@ class AcoParams(ctypes.Structure):
         ("stage_matrix", ctypes.c_int), ("host_prep", ctypes.c_int), ("fuse_ls", ctypes.c_int),
         ("ns_rounds", ctypes.c_int),
         ("ls_ants", ctypes.c_int),
+        ("draw_warps", ctypes.c_int),
     ]
 
 

@@ -366,24 +366,28 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         if (p.ants_per_block > 0) cn_apc = std::min(16, p.ants_per_block);
         else if (count == 1) cn_apc = std::max(1, std::min(8, (inst[0].A + sm_count - 1) / sm_count));
         else cn_apc = std::max(1, std::min(16, total_ants / (sm_count * 2)));
+        // helper draw warps while the construct is latency bound (few ants per SM)
+        cn_draw = p.draw_warps > 0 || (p.draw_warps == 0 && total_ants <= 4 * sm_count);
+        if (cn_draw) cn_apc = std::min(cn_apc, 8);
         // shared-memory plan of every instance for `apc` ants per CTA and `lsw`
         // fused 2-opt warps (lsw > 0 needs the tables staged)
         auto plan = [&](int apc, int lsw) {
+            const bool draw = cn_draw && lsw == 0 && apc <= 8;
             size_t mx = 0;
             for (InstHost &ih : inst) {
                 bool packable = true;
                 for (int i = 0; i < ih.n; i++)
                     if (ih.demand[i] < 0 || ih.demand[i] > 0xFFFF) packable = false;
                 ih.smat = p.stage_matrix >= 0 && ih.n <= 1024 && packable &&
-                          construct_nn_smem(ih.n, ih.K, ih.Kp, apc, true, true, false, lsw) <= kSmemBudget;
+                          construct_nn_smem(ih.n, ih.K, ih.Kp, apc, true, true, false, lsw, draw) <= kSmemBudget;
                 ih.packed =
-                    packable && construct_nn_smem(ih.n, ih.K, ih.Kp, apc, ih.smat, true, false, lsw) <= kSmemBudget;
+                    packable && construct_nn_smem(ih.n, ih.K, ih.Kp, apc, ih.smat, true, false, lsw, draw) <= kSmemBudget;
                 ih.gtab = false;
-                size_t need = construct_nn_smem(ih.n, ih.K, ih.Kp, apc, ih.smat, ih.packed, false, lsw);
+                size_t need = construct_nn_smem(ih.n, ih.K, ih.Kp, apc, ih.smat, ih.packed, false, lsw, draw);
                 if (need > kSmemBudget) {
                     ih.gtab = true; // the candidate table stays in global memory (read through L2)
                     ih.packed = packable;
-                    need = construct_nn_smem(ih.n, ih.K, ih.Kp, apc, false, ih.packed, true, lsw);
+                    need = construct_nn_smem(ih.n, ih.K, ih.Kp, apc, false, ih.packed, true, lsw, draw);
                 }
                 if (need > kSmemBudget) return false;
                 mx = std::max(mx, need);
@@ -411,6 +415,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
                 else return ACO_ERR_INVALID; // candidate table of this size cannot be staged
             }
         }
+        cn_draw = cn_draw && cn_lsw == 0 && cn_apc <= 8; // as the last plan sized the shared memory
     }
     {
         // 2-opt CTA shape: ants per CTA x warps.  Cost model: waves of CTAs over
@@ -811,7 +816,8 @@ int Colony::construct(bool fused)
     CK(cudaMemsetAsync(queue_d_, 0, sizeof(int), st));
     const int lsw = fused && p.ls_flag ? cn_lsw : 0;
     last_fused_ = lsw > 0;
-    CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st, lsw));
+    CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st, lsw,
+                           cn_draw));
     return ACO_OK;
 }
 

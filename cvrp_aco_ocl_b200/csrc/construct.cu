@@ -228,19 +228,25 @@ __global__ void __launch_bounds__(512) construct_parity_kernel(ConstructArgs a)
 // candidate choice_info (chc) and -- when it fits (smat) -- the whole
 // total_info matrix into shared memory with TMA bulk copies, then runs one
 // warp per ant.  Per ant:
-//   * the Park-Miller draws are made 32 steps at a time, one per lane
-//     (x_{s+j+1} = x_s * 16807^(j+1) mod m), and read with one shuffle per step;
+//   * lane l draws from the ant's Park-Miller state l, one number a step, and
+//     turns it into the rate of its exponential clock (race_rate);
+//   * with helper warps (draw), a second warp per ant makes those draws and
+//     rates 16 steps ahead into a double-buffered shared ring, handing over at
+//     a two-warp named barrier every 16 steps, so the ant's warp keeps only the
+//     dependent chain of the step: candidate row, visited bit, key, one redux;
 //   * with n <= 1024 the visited set lives in registers (lane l holds bit j for
 //     node l + 32j): a candidate's bit is one shuffle away, the update needs no
 //     memory operation, and the full-row fallback tests its own bits;
-//   * the 5-step shuffle scan and a redux over lane ids select the candidate;
 //   * the tour goes to a shared buffer and its length is summed after the last
 //     step, in step order.
 // ---------------------------------------------------------------------------
 struct NNLayout {
-    size_t bar, dem, d0, cand, chc, vis, tour, mat, rid, li, dt, pend, cnt, q, ready, ls, bytes;
+    size_t bar, dem, d0, cand, chc, vis, tour, mat, rid, li, dt, pend, cnt, q, ready, ls, ring, flag, bytes;
     int qcap;
 };
+
+// Helper-warp draws: steps per hand-over (the ring holds two such chunks per ant).
+constexpr int kDrawChunk = 16;
 
 // Shared memory of one 2-opt warp of the fused construct: distance tile,
 // in-route neighbour lists and counts, route node ids.
@@ -251,7 +257,7 @@ constexpr size_t kLsWarpBytes = 32 * 32 * 4 + 32 * 32 + 32 + 64 + 32 * 32 * 2;
 // lsw > 0: the fused 2-opt (lsw improving warps): per ant the route id and
 // local index of every node and the edge lengths, the route queue.
 __host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, bool smat, bool packed, bool gtab,
-                                              int lsw = 0)
+                                              int lsw = 0, bool draw = false)
 {
     const size_t n4 = (size_t)((n + 3) & ~3);
     const size_t words = (size_t)((n + 31) / 32);
@@ -277,6 +283,11 @@ __host__ __device__ inline NNLayout nn_layout(int n, int K, int Kp, int apc, boo
         L.q = o; o = al128(o + (size_t)L.qcap * 8);
         L.ready = o; o = al128(o + (size_t)L.qcap * 4);
         L.ls = o; o = al128(o + (size_t)lsw * kLsWarpBytes);
+    }
+    L.ring = L.flag = o;
+    if (draw) { // per ant: two chunks of rates, two hand-over flags
+        L.ring = o; o = al128(o + (size_t)apc * 2 * kDrawChunk * 32 * 4);
+        L.flag = o; o = al128(o + (size_t)apc * 2 * 4);
     }
     L.bytes = o;
     (void)K;
@@ -382,13 +393,46 @@ __device__ void fused_ls_warp(const ConstructArgs &a, unsigned char *smem, const
     if (status != ACO_OK && lane == 0) set_status(a.status, status);
 }
 
-template <bool FIN, bool SMAT, bool PACKED, bool REGVIS, bool GTAB = false, bool LSF = false>
+// Barrier `id` shared by exactly two warps (an ant's warp and its helper).
+__device__ __forceinline__ void pair_barrier(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
+
+// 16807^e mod (2^31 - 1): the jump of a Park-Miller state over e draws.
+__device__ __forceinline__ uint32_t pm_pow16807(int e)
+{
+    uint32_t r = 1u, b = 16807u;
+    for (; e > 0; e >>= 1) {
+        if (e & 1) r = pm_mul(r, b);
+        b = pm_mul(b, b);
+    }
+    return r;
+}
+
+// Helper warp of one ant: the race rates of chunk c go to ring half c & 1; at
+// hand-over c both warps meet at the pair barrier, after which the ant's warp
+// has set flag[c & 1] (1 = the ant is done, 0 = continue).  The ant's warp
+// reads flag-free: it only waits at the same barriers.
+__device__ __forceinline__ void draw_warp(const int *seedp, float *ring, const int *flag, int bar_id, int lane)
+{
+    uint32_t xs = pm_norm(seedp[lane]);
+    for (int c = 0;; c++) {
+        float *buf = ring + (c & 1) * kDrawChunk * 32;
+#pragma unroll 4
+        for (int k = 0; k < kDrawChunk; k++) {
+            xs = pm_mul(xs, 16807u);
+            buf[k * 32 + lane] = race_rate(pm_uniform(xs));
+        }
+        pair_barrier(bar_id);
+        if (*reinterpret_cast<const volatile int *>(flag + (c & 1))) break;
+    }
+}
+
+template <bool FIN, bool SMAT, bool PACKED, bool REGVIS, bool GTAB = false, bool LSF = false, bool DRAW = false>
 __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int apc, int ant0, unsigned char *smem, uint32_t phase,
                                   int lsw = 0)
 {
     const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp, T = a.T;
     const int n4 = (n + 3) & ~3;
-    const NNLayout L = nn_layout(n, K, Kp, apc, SMAT, PACKED, GTAB, LSF ? lsw : 0);
+    const NNLayout L = nn_layout(n, K, Kp, apc, SMAT, PACKED, GTAB, LSF ? lsw : 0, DRAW);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar);
     int *s_dem = reinterpret_cast<int *>(smem + L.dem);
     float *s_d0 = reinterpret_cast<float *>(smem + L.d0);
@@ -436,6 +480,13 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
     }
 
     const int ant = ant0 + warp;
+    float *ring = reinterpret_cast<float *>(smem + L.ring) + (size_t)(DRAW ? warp % apc : 0) * 2 * kDrawChunk * 32;
+    int *hflag = reinterpret_cast<int *>(smem + L.flag) + (DRAW ? warp % apc : 0) * 2;
+    if (DRAW && warp >= apc) { // helper warps: warp apc + j draws for ant j
+        if (warp < 2 * apc && ant0 + (warp - apc) < a.n_ants)
+            draw_warp(a.seeds + (size_t)(ant0 + warp - apc) * a.nloc, ring, hflag, 1 + warp - apc, lane);
+        return true;
+    }
     if (LSF && warp >= apc) {
         if (warp < apc + lsw) {
             const int ncw = a.n_ants - ant0 < apc ? a.n_ants - ant0 : apc;
@@ -476,6 +527,13 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
         // lane l draws from the ant's Park-Miller state l (nloc >= 32), one number a step
         int *seedp = a.seeds + (size_t)ant * a.nloc;
         uint32_t xs = pm_norm(seedp[lane]);
+        int hand = 0; // hand-overs passed (helper-warp draws)
+        if (DRAW) {   // hand-over 0: the helper has filled chunk 0
+            if (lane == 0) hflag[0] = 0;
+            __syncwarp();
+            pair_barrier(1 + warp);
+            hand = 1;
+        }
         int cur = 0, step = 0, vcnt = 1, load = 0, err = 0;
         float rdist = 0.f;
         const int cap = a.capacity;
@@ -486,8 +544,20 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 err = ACO_ERR_STEP_LIMIT;
                 break;
             }
-            xs = pm_mul(xs, 16807u);
-            const float rate = race_rate(pm_uniform(xs)); // off the dependent chain of the step
+            float rate;
+            if (DRAW) {
+                const int sc = step & (kDrawChunk - 1);
+                if (sc == 0 && step > 0) { // next chunk: hand-over `hand`, continue
+                    if (lane == 0) hflag[hand & 1] = 0;
+                    __syncwarp();
+                    pair_barrier(1 + warp);
+                    hand++;
+                }
+                rate = ring[((hand - 1) & 1) * kDrawChunk * 32 + sc * 32 + lane];
+            } else {
+                xs = pm_mul(xs, 16807u);
+                rate = race_rate(pm_uniform(xs)); // off the dependent chain of the step
+            }
             int c, dc;
             if (PACKED) {
                 const uint32_t pk = s_cand[cur * Kp + jl];
@@ -565,6 +635,11 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             }
             cur = nxt;
         }
+        if (DRAW) { // last hand-over: the helper stops
+            if (lane == 0) hflag[hand & 1] = 1;
+            __syncwarp();
+            pair_barrier(1 + warp);
+        }
         __syncwarp();
         int *tour = a.solutions + (size_t)ant * T;
         bool use_dt = false;
@@ -622,14 +697,36 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 a.lens[ant] = tdist;
             }
         }
-        if (step > 0) seedp[lane] = (int)xs; // states after the last draw
+        if (step > 0) // states after the last draw (the helper may have drawn further)
+            seedp[lane] = (int)(DRAW ? pm_mul(xs, pm_pow16807(step)) : xs);
     }
     return true;
 }
 
-template <bool FIN>
-__global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *args, const int2 *items, int n_items,
-                                                           int *queue, int apc, int lsw)
+// The item without fused 2-opt: candidate table staged or in global memory,
+// register or shared visited set, with or without helper-warp draws.
+template <bool FIN, bool DRAW>
+__device__ __forceinline__ bool construct_nn_plain(const ConstructArgs &a, int apc, int ant0, unsigned char *smem,
+                                                   uint32_t phase)
+{
+    if (a.gtab)
+        return a.packed ? construct_nn_item<FIN, false, true, false, true, false, DRAW>(a, apc, ant0, smem, phase)
+                        : construct_nn_item<FIN, false, false, false, true, false, DRAW>(a, apc, ant0, smem, phase);
+    if (a.n <= 1024) {
+        if (a.smat)
+            return a.packed ? construct_nn_item<FIN, true, true, true, false, false, DRAW>(a, apc, ant0, smem, phase)
+                            : construct_nn_item<FIN, true, false, true, false, false, DRAW>(a, apc, ant0, smem, phase);
+        return a.packed ? construct_nn_item<FIN, false, true, true, false, false, DRAW>(a, apc, ant0, smem, phase)
+                        : construct_nn_item<FIN, false, false, true, false, false, DRAW>(a, apc, ant0, smem, phase);
+    }
+    return a.packed ? construct_nn_item<FIN, false, true, false, false, false, DRAW>(a, apc, ant0, smem, phase)
+                    : construct_nn_item<FIN, false, false, false, false, false, DRAW>(a, apc, ant0, smem, phase);
+}
+
+// KIND: 0 = plain, 1 = helper-warp draws, 2 = fused 2-opt (lsw improving warps)
+template <bool FIN, int KIND>
+__device__ __forceinline__ void construct_nn_body(const ConstructArgs *args, const int2 *items, int n_items, int *queue,
+                                                  int apc, int lsw)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_item;
@@ -649,29 +746,36 @@ __global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *
         const ConstructArgs a = args[code.x];
         const int ant0 = code.y;
         bool ok;
-        if (lsw > 0 && a.gtab) { // fused 2-opt, candidate table in global memory
+        if (KIND == 2 && a.gtab) { // fused 2-opt, candidate table in global memory
             ok = a.packed ? construct_nn_item<FIN, false, true, true, true, true>(a, apc, ant0, smem, phase, lsw)
                           : construct_nn_item<FIN, false, false, true, true, true>(a, apc, ant0, smem, phase, lsw);
-        } else if (lsw > 0) { // fused 2-opt (register visited set, staged tables)
+        } else if (KIND == 2) { // fused 2-opt (register visited set, staged tables)
             if (a.smat) ok = a.packed ? construct_nn_item<FIN, true, true, true, false, true>(a, apc, ant0, smem, phase, lsw)
                                       : construct_nn_item<FIN, true, false, true, false, true>(a, apc, ant0, smem, phase, lsw);
             else ok = a.packed ? construct_nn_item<FIN, false, true, true, false, true>(a, apc, ant0, smem, phase, lsw)
                                : construct_nn_item<FIN, false, false, true, false, true>(a, apc, ant0, smem, phase, lsw);
-        } else if (a.gtab) {
-            ok = a.packed ? construct_nn_item<FIN, false, true, false, true>(a, apc, ant0, smem, phase)
-                          : construct_nn_item<FIN, false, false, false, true>(a, apc, ant0, smem, phase);
-        } else if (a.n <= 1024) {
-            if (a.smat) ok = a.packed ? construct_nn_item<FIN, true, true, true>(a, apc, ant0, smem, phase)
-                                      : construct_nn_item<FIN, true, false, true>(a, apc, ant0, smem, phase);
-            else ok = a.packed ? construct_nn_item<FIN, false, true, true>(a, apc, ant0, smem, phase)
-                               : construct_nn_item<FIN, false, false, true>(a, apc, ant0, smem, phase);
         } else {
-            ok = a.packed ? construct_nn_item<FIN, false, true, false>(a, apc, ant0, smem, phase)
-                          : construct_nn_item<FIN, false, false, false>(a, apc, ant0, smem, phase);
+            ok = construct_nn_plain<FIN, KIND == 1>(a, apc, ant0, smem, phase);
         }
         if (!ok) break; // uniform: decided by __syncthreads_or
         phase ^= 1u;
     }
+}
+
+template <bool FIN, int KIND>
+__global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *args, const int2 *items, int n_items,
+                                                           int *queue, int apc, int lsw)
+{
+    construct_nn_body<FIN, KIND>(args, items, n_items, queue, apc, lsw);
+}
+
+// The helper-warp variant runs one CTA per SM (few ants, latency bound): its
+// registers are not squeezed for a second CTA.
+template <bool FIN>
+__global__ void __launch_bounds__(512, 1) construct_nn_draw_kernel(const ConstructArgs *args, const int2 *items,
+                                                                   int n_items, int *queue, int apc, int lsw)
+{
+    construct_nn_body<FIN, 1>(args, items, n_items, queue, apc, lsw);
 }
 
 template <int WPA, bool FIN, bool SMAT>
@@ -701,15 +805,19 @@ size_t construct_parity_smem(int n, int nloc, int kmax, int wpa, int apc, bool s
     return parity_layout(n, nloc, kmax, wpa, apc, stage_total).bytes;
 }
 
-size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool packed, bool global_table, int ls_warps)
+size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool packed, bool global_table, int ls_warps,
+                         bool draw)
 {
-    return nn_layout(n, K, Kp, apc, stage_total, packed, global_table, ls_warps).bytes;
+    return nn_layout(n, K, Kp, apc, stage_total, packed, global_table, ls_warps, draw && ls_warps == 0).bytes;
 }
 
 cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue, int apc,
-                                size_t smem, int sm_count, bool finite_maxd, cudaStream_t st, int ls_warps)
+                                size_t smem, int sm_count, bool finite_maxd, cudaStream_t st, int ls_warps, bool draw)
 {
-    auto kern = finite_maxd ? construct_nn_kernel<true> : construct_nn_kernel<false>;
+    if (ls_warps > 0) draw = false;
+    auto kern = ls_warps > 0 ? (finite_maxd ? construct_nn_kernel<true, 2> : construct_nn_kernel<false, 2>)
+                : draw       ? (finite_maxd ? construct_nn_draw_kernel<true> : construct_nn_draw_kernel<false>)
+                             : (finite_maxd ? construct_nn_kernel<true, 0> : construct_nn_kernel<false, 0>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = (int)(228 * 1024 / (smem + 1024));
@@ -718,6 +826,7 @@ cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items
     if (blocks > n_items) blocks = n_items;
     if (blocks < 1) blocks = 1;
     int warps = apc < 8 ? 8 : apc; // helper warps share the staging of each item
+    if (draw && warps < 2 * apc) warps = 2 * apc;
     if (ls_warps > 0) warps = apc + ls_warps;
     if (warps > 16) return cudaErrorInvalidValue;
     kern<<<blocks, warps * 32, smem, st>>>(d_args, d_items, n_items, d_queue, apc, ls_warps);

@@ -121,7 +121,7 @@ cudaError_t launch_construct_parity(const ConstructArgs &a, int warps_per_ant, i
 // in ls_needed for the 2-opt kernel.
 cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue,
                                 int ants_per_cta, size_t smem, int sm_count, bool finite_maxd, cudaStream_t st,
-                                int ls_warps = 0);
+                                int ls_warps = 0, bool draw = false);
 // 2-opt: one CTA of `warps` warps per ant; d_ant_inst[g] = instance of global ant g,
 // d_ant_base[b] = first global ant of instance b.
 // 2-opt: CTAs of `ants_per_cta` ants (1..8) and `warps` warps pulling routes;
@@ -141,8 +141,10 @@ cudaError_t launch_t0(unsigned long long *t0, cudaStream_t st);
 // the 227 KB per-CTA limit).
 size_t construct_parity_smem(int n, int nloc, int kmax, int warps_per_ant, int ants_per_block, bool stage_total,
                              bool finite_maxd);
+// draw: a helper warp per ant makes the race draws ahead (ants_per_cta <= 8;
+// ignored with ls_warps > 0)
 size_t construct_nn_smem(int n, int K, int Kp, int ants_per_cta, bool stage_total, bool packed,
-                         bool global_table = false, int ls_warps = 0);
+                         bool global_table = false, int ls_warps = 0, bool draw = false);
 size_t local_search_smem(int n_max, int ants_per_cta, int warps);
 // resident 2-opt CTAs per SM for this shape (0 = cannot launch)
 int local_search_occupancy(int warps, size_t smem);

@@ -100,6 +100,9 @@ typedef struct aco_params {
                              random neighbourhood moves (neighbourSearch.cpp, move.cpp) per ant and iteration,
                              the valid improving ones applied; 0 = off (default) */
     int ls_ants;          /* 0 = autotuned; else ants per 2-opt CTA (1..8), whose routes its warps share */
+    int draw_warps;       /* throughput construct: 1 = a helper warp per ant makes the ant's draws ahead of it
+                             (at most 8 ants per CTA), -1 = the ant's warp draws, 0 = automatic (helper warps
+                             while there are at most 4 ants per SM); same results either way */
 } aco_params;
 
 /* One best-so-far record {iteration, length, seconds since init} (problem.h:62-66). */

@@ -119,9 +119,11 @@ def test_full_iterations_vs_oracle(gpu, n_cust, A, nloc, ls, nn_ls):
         assert np.array_equal(S.elites(), O.elites)
 
 
-def test_throughput_mode_vs_oracle(gpu):
+@pytest.mark.parametrize("draw", [-1, 1])  # the ant's warp draws / a helper warp draws ahead
+def test_throughput_mode_vs_oracle(gpu, draw):
     inst = I.gen_mixed(5, 200)
-    S, O = build_pair(inst, 100, 256, 1796300000, 4321, True, 25, mode=MODE_THROUGHPUT, nn_ants=25)
+    S, O = build_pair(inst, 100, 256, 1796300000, 4321, True, 25, mode=MODE_THROUGHPUT, nn_ants=25,
+                      draw_warps=draw)
     with S:
         S.init(); O.init_aco(throughput=True)
         compare_state(S, O)
@@ -130,9 +132,33 @@ def test_throughput_mode_vs_oracle(gpu):
             compare_state(S, O)
 
 
-def test_throughput_large_no_smem_matrix(gpu):
+@pytest.mark.parametrize("draw", [-1, 1])
+def test_throughput_route_length_limit_vs_oracle(gpu, draw):
+    """max_distance and service time: the candidate test adds the route-length
+    check (finite-limit kernels) in both draw arrangements."""
+    inst = I.gen_mixed(23, 150)
+    dist = oracle.compute_distances(inst.x, inst.y)
+    A, nloc, T0, rs = 64, 256, 1796300000, 515
+    maxd, serv = float(np.max(dist[0]) * 2.6), 3.0
+    prob = problem_of(inst.x, inst.y, inst.demand, inst.capacity, max_distance=maxd, service_time=serv)
+    p = params_for(inst.n, A, nloc, T0, rs, True, 25, mode=MODE_THROUGHPUT, nn_ants=25, draw_warps=draw)
+    nn = oracle.compute_nn_lists(dist, 25, 25)
+    seeds, _ = oracle.make_seeds(T0, rs, A, nloc)
+    O = oracle.Oracle(dist, inst.demand, inst.capacity, A, nloc, nn, seeds, ls_flag=True, nn_ants_list=nn,
+                      max_dist=maxd, serv_time=serv, n_threads=8, ls_pass_limit=4096)
+    with Solver(prob, p) as S:
+        S.init(); O.init_aco(throughput=True)
+        compare_state(S, O)
+        for _ in range(2):
+            S.iterate(1); O.run_iteration(throughput=True)
+            compare_state(S, O)
+        assert S.validate()[1] == 0
+
+
+@pytest.mark.parametrize("draw", [-1, 1])
+def test_throughput_large_no_smem_matrix(gpu, draw):
     inst = I.gen_large(11, 1000)
-    S, O = build_pair(inst, 48, 256, 1796300000, 99, True, 30, mode=MODE_THROUGHPUT, nn_ants=30)
+    S, O = build_pair(inst, 48, 256, 1796300000, 99, True, 30, mode=MODE_THROUGHPUT, nn_ants=30, draw_warps=draw)
     with S:
         S.init(); O.init_aco(throughput=True)
         compare_state(S, O)
@@ -281,11 +307,12 @@ def test_integer_exponents_and_many_ranks(gpu, mode):
         assert np.array_equal(S.elites(), O.elites)
 
 
-def test_throughput_candidate_table_in_global_memory(gpu):
+@pytest.mark.parametrize("draw", [-1, 1])
+def test_throughput_candidate_table_in_global_memory(gpu, draw):
     """n=1201 with 25-candidate lists: the table does not fit in shared memory
     and is read through L2; results stay bit-exact."""
     inst = I.gen_large(17, 1200)
-    S, O = build_pair(inst, 32, 256, 1796300000, 8, True, 25, mode=MODE_THROUGHPUT, nn_ants=25)
+    S, O = build_pair(inst, 32, 256, 1796300000, 8, True, 25, mode=MODE_THROUGHPUT, nn_ants=25, draw_warps=draw)
     with S:
         S.init(); O.init_aco(throughput=True)
         compare_state(S, O)
