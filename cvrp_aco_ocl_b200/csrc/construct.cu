@@ -583,20 +583,32 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             } else { // no listed candidate fits: best feasible customer of the full row
                 uint32_t bk = 0u, bi = 0xffffffffu;
                 const float *row = SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld;
-#pragma unroll 8
-                for (int k = 0; k < words; k++) { // branch-free: every lane tests its own nodes
-                    const int i = lane + 32 * k;
-                    const int ic = i < n ? i : 0;
-                    const uint32_t vk = REGVIS ? vis : vism[k];
-                    bool ff = i > 0 && i < n && !((vk >> (REGVIS ? k : lane)) & 1u) && load + s_dem[ic] <= cap;
-                    if (FIN)
-                        ff = ff && __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + ic),
-                                                                        a.serv_time)),
-                                             s_d0[ic]) <= a.max_dist;
-                    const uint32_t kk = ff ? __float_as_uint(row[ic]) + 1u : 0u;
-                    const bool better = kk > bk;
-                    bk = better ? kk : bk;
-                    bi = better ? (uint32_t)i : bi;
+                constexpr int G = FIN ? 4 : 8;
+                for (int k0 = 0; k0 < words; k0 += G) { // branch-free: every lane tests its own nodes
+                    // G nodes a lane at a time, all loads first (indices clamped into range)
+                    float rv[G], dv[G];
+                    int dm[G];
+#pragma unroll
+                    for (int u = 0; u < G; u++) {
+                        const int i = lane + 32 * (k0 + u);
+                        const int ic = i < n ? i : 0;
+                        rv[u] = row[ic];
+                        dm[u] = s_dem[ic];
+                        if (FIN) dv[u] = __ldg(a.dist + (size_t)cur * ld + ic);
+                    }
+#pragma unroll
+                    for (int u = 0; u < G; u++) {
+                        const int k = k0 + u, i = lane + 32 * k;
+                        const uint32_t vk = REGVIS ? vis : (k < words ? vism[k] : ~0u);
+                        bool ff = i > 0 && i < n && !((vk >> (REGVIS ? (k & 31) : lane)) & 1u) && load + dm[u] <= cap;
+                        if (FIN)
+                            ff = ff && __fadd_rn(__fadd_rn(rdist, __fadd_rn(dv[u], a.serv_time)), s_d0[i < n ? i : 0]) <=
+                                           a.max_dist;
+                        const uint32_t kk = ff ? __float_as_uint(rv[u]) + 1u : 0u;
+                        const bool better = kk > bk; // strictly: the lowest k of a lane wins ties
+                        bk = better ? kk : bk;
+                        bi = better ? (uint32_t)i : bi;
+                    }
                 }
                 const uint32_t hk = __reduce_max_sync(FULL, bk);
                 if (hk != 0u) {
