@@ -264,7 +264,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         o.xy = ih.device_prep ? take((size_t)2 * ih.n4 * 4) : 0;
         o.nnfull = ih.device_prep ? take((size_t)ih.n * std::max(1, ih.depth) * 4) : 0;
     }
-    const size_t o_status = take(4), o_t0 = take(8), o_queue = take(4);
+    const size_t o_status = take(4), o_t0 = take(8), o_queue = take(8); // construct queue: next item, CTAs done
     total_ants = 0;
     total_rows = 0;
     ld_max = 32;
@@ -419,8 +419,9 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     }
     {
         // 2-opt CTA shape: ants per CTA x warps.  Cost model: waves of CTAs over
-        // the SMs x routes per warp (routes per ant estimated by total demand /
-        // capacity); ties go to more warps per ant.  A caller's value is kept.
+        // the SMs x (routes per warp + 1 for the CTA's set-up and write-back),
+        // routes per ant estimated by total demand / capacity; ties go to more
+        // warps per ant.  A caller's value is kept.
         int n_max = 0;
         for (const InstHost &ih : inst) n_max = std::max(n_max, ih.n);
         ls_nmax = n_max;
@@ -441,7 +442,8 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
                 if (res < 1) continue;
                 const long long blocks = (total_ants + apc - 1) / apc;
                 const long long waves = (blocks + (long long)res * sm_count - 1) / ((long long)res * sm_count);
-                const long long cost = waves * ((apc * max_routes + w - 1) / w);
+                // + 1: the per-CTA set-up and write-back cost about one route
+                const long long cost = waves * ((apc * max_routes + w - 1) / w + 1);
                 const double wpa = (double)w / apc;
                 if (best_cost < 0 || cost < best_cost || (cost == best_cost && wpa > best_wpa)) {
                     best_cost = cost;
@@ -813,8 +815,7 @@ int Colony::construct(bool fused)
         CK(launch_construct_parity(cargs_h_[0], cp_wpa, cp_apc, cp_stage, st));
         return ACO_OK;
     }
-    CK(cudaMemsetAsync(queue_d_, 0, sizeof(int), st));
-    const int lsw = fused && p.ls_flag ? cn_lsw : 0;
+    const int lsw = fused && p.ls_flag ? cn_lsw : 0; // the queue starts at 0 (zeroed arena, rewound by the kernel)
     last_fused_ = lsw > 0;
     CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st, lsw,
                            cn_draw));

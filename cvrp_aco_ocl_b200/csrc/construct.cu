@@ -772,6 +772,15 @@ __device__ __forceinline__ void construct_nn_body(const ConstructArgs *args, con
         if (!ok) break; // uniform: decided by __syncthreads_or
         phase ^= 1u;
     }
+    // the last CTA to finish rewinds the queue for the next launch: every CTA
+    // has taken its final ticket before it counts itself out
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(queue + 1, 1) == (int)gridDim.x - 1) {
+            queue[0] = 0;
+            queue[1] = 0;
+        }
+    }
 }
 
 template <bool FIN, int KIND>

@@ -114,7 +114,8 @@ enum RowMode {
 cudaError_t launch_construct_parity(const ConstructArgs &a, int warps_per_ant, int ants_per_block, bool stage_total,
                                     cudaStream_t st);
 // Throughput construct, persistent: CTAs pull work items {instance, first ant}
-// from *d_queue (reset to 0 by the caller before the launch).
+// from d_queue[0]; d_queue[1] counts finished CTAs.  Both start at 0 and the
+// last CTA to finish sets them back to 0, so consecutive launches need no reset.
 // ls_warps > 0: each CTA also runs that many 2-opt warps that improve the
 // routes of its ants as soon as they are complete (all instances n <= 1024,
 // candidate tables staged); ants with a route of more than 32 nodes are marked

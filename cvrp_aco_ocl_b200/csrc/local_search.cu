@@ -62,10 +62,9 @@ __host__ __device__ inline LsAnt ls_ant_layout(int n)
     return L;
 }
 
-// per warp: distance tile; the first 32 list entries of every route node
-// (uint16), overwritten in place by the in-route neighbour lists (uint8: row k
-// lands on bytes of rows <= k/2, already consumed); list counts; route nodes
-constexpr size_t kLsWarp = kRL * kRL * 4 + kRL * 32 * 2 + kRL + kRL * 2;
+// per warp: distance tile, in-route neighbour lists (local indices), list counts
+constexpr size_t kLsWarp = kRL * kRL * 4 + kRL * kRL + kRL;
+constexpr int kLsRows = 8; // tile rows loaded per round
 constexpr int kMaxLsAnts = 8;
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -241,10 +240,8 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
     const LsAnt AL = ls_ant_layout(n_max);
     unsigned char *wbase = smem + (size_t)apc * AL.bytes + (size_t)warp * kLsWarp;
     float *tile = reinterpret_cast<float *>(wbase);
-    uint16_t *nnbuf = reinterpret_cast<uint16_t *>(wbase + kRL * kRL * 4);
-    uint8_t *lnn = reinterpret_cast<uint8_t *>(nnbuf);
-    uint8_t *lcnt = lnn + kRL * 32 * 2;
-    uint16_t *rnode = reinterpret_cast<uint16_t *>(lcnt + kRL);
+    uint8_t *lnn = wbase + kRL * kRL * 4;
+    uint8_t *lcnt = lnn + kRL * kRL;
     auto ant_ptr = [&](int j, size_t off) { return smem + (size_t)j * AL.bytes + off; };
 
     // the CTA's ants: global ants [blockIdx.x * apc, ... + apc)
@@ -356,34 +353,46 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
             // after a fused construct the routes of at most 32 nodes are improved
             // already; only the longer ones of a flagged ant are left here
         } else if (R <= kRL) {
-            // route-local state: node ids, distance tile, in-route neighbour lists
+            // route-local state: the distance tile (row k1 = distances from route
+            // node k1, lane k2 its column) and every route node's neighbour list
+            // filtered to the route, in list order.  Lane q holds route node q; row
+            // nodes come by shuffle, so the loads of a round of kLsRows rows depend
+            // on nothing in shared memory and are all in flight together.
             const int v = lane < R ? (int)tour[rb + lane] : 0;
-            if (lane < R) rnode[lane] = (uint16_t)v;
-            __syncwarp();
-            // the distance tile and the first 32 list entries of every route node,
-            // loads issued ahead of their uses
-#pragma unroll 8
-            for (int e = lane; e < R * kRL; e += 32) {
-                const int k1 = e >> 5, k2 = e & 31;
-                tile[e] = k2 < R ? __ldg(a.dist + (size_t)rnode[k1] * a.ld + rnode[k2]) : 0.f;
-                nnbuf[e] = k2 < a.nn_ls ? (uint16_t)__ldg(a.nn_list + (size_t)rnode[k1] * a.nn_ls + k2) : 0;
-            }
-            __syncwarp();
-            for (int k = 0; k < R; k++) {
-                const int node = rnode[k];
-                int cnt = 0;
-                for (int h0 = 0; h0 < a.nn_ls && cnt < R - 1; h0 += 32) {
-                    const int h = h0 + lane;
-                    const int n2 = h >= a.nn_ls ? 0
-                                   : h0 == 0 ? (int)nnbuf[k * kRL + lane]
-                                             : __ldg(a.nn_list + (size_t)node * a.nn_ls + h);
-                    const bool in = h < a.nn_ls && n2 != 0 && rid[n2] == r;
-                    const unsigned m = __ballot_sync(FULL, in);
-                    const int slot = cnt + __popc(m & ((1u << lane) - 1u));
-                    if (in && slot < kRL) lnn[k * kRL + slot] = li[n2];
-                    cnt += __popc(m);
+            for (int k0 = 0; k0 < R; k0 += kLsRows) {
+                float d[kLsRows];
+                int nb[kLsRows];
+#pragma unroll
+                for (int u = 0; u < kLsRows; u++) {
+                    const int k1 = k0 + u;
+                    const int node1 = __shfl_sync(FULL, v, k1 & 31);
+                    d[u] = (k1 < R && lane < R) ? __ldg(a.dist + (size_t)node1 * a.ld + v) : 0.f;
+                    nb[u] = (k1 < R && lane < a.nn_ls) ? __ldg(a.nn_list + (size_t)node1 * a.nn_ls + lane) : 0;
                 }
-                if (lane == 0) lcnt[k] = (uint8_t)(cnt < R - 1 ? cnt : R - 1);
+#pragma unroll
+                for (int u = 0; u < kLsRows; u++) {
+                    const int k1 = k0 + u;
+                    if (k1 >= R) break; // warp-uniform
+                    tile[k1 * kRL + lane] = d[u];
+                    const int n2 = nb[u];
+                    const bool in = n2 != 0 && rid[n2] == r;
+                    const unsigned m = __ballot_sync(FULL, in);
+                    const int slot = __popc(m & ((1u << lane) - 1u));
+                    if (in && slot < kRL) lnn[k1 * kRL + slot] = li[n2];
+                    int cnt = __popc(m);
+                    // lists deeper than 32: the rest while the route may still gain entries
+                    const int node1 = __shfl_sync(FULL, v, k1 & 31);
+                    for (int h0 = 32; h0 < a.nn_ls && cnt < R - 1; h0 += 32) {
+                        const int h = h0 + lane;
+                        const int n3 = h < a.nn_ls ? __ldg(a.nn_list + (size_t)node1 * a.nn_ls + h) : 0;
+                        const bool in3 = n3 != 0 && rid[n3] == r;
+                        const unsigned m3 = __ballot_sync(FULL, in3);
+                        const int slot3 = cnt + __popc(m3 & ((1u << lane) - 1u));
+                        if (in3 && slot3 < kRL) lnn[k1 * kRL + slot3] = li[n3];
+                        cnt += __popc(m3);
+                    }
+                    if (lane == 0) lcnt[k1] = (uint8_t)(cnt < R - 1 ? cnt : R - 1);
+                }
             }
             __syncwarp();
             int tq = lane < R ? lane : 0;

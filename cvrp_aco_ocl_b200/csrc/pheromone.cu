@@ -48,13 +48,22 @@ __device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v
 
 __global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, int do_elites)
 {
-    extern __shared__ float s_hb[]; // help_b[n_ants] of get_elites
+    extern __shared__ float s_len[]; // lens[0..A) of this iteration
     __shared__ unsigned long long red[32];
-    __shared__ int s_best, s_flag;
-    __shared__ float s_minval;
+    __shared__ int s_best, s_flag, s_elite[32], s_size[32];
+    __shared__ int s_rank[1024]; // keys below each entry (get_elites, one pass)
+    __shared__ float s_minval, s_bsf;
+    __shared__ const int *s_tour[32];
     const StatsArgs a = args[blockIdx.x];
-    const int A = a.n_ants, T = a.T, tid = threadIdx.x, bs = blockDim.x;
+    const int A = a.n_ants, T = a.T, tid = threadIdx.x, bs = blockDim.x, R = a.ras_ranks;
     const int lg = a.log2_nloc;
+    // every global value the kernel needs is loaded up front, in parallel
+    if (tid == 0) {
+        s_bsf = a.lens[A];
+        s_elite[0] = A;
+    }
+    for (int k = tid; k < A; k += bs) s_len[k] = a.lens[k];
+    __syncthreads();
     const int iter = *a.iteration;
 
     // iteration best: min over (length, work-group, bit-reversed lane).  Phase 0
@@ -65,7 +74,7 @@ __global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, int 
     for (int k = tid; k < A; k += bs) {
         const unsigned g = (unsigned)k >> lg, lid = (unsigned)k & ((1u << lg) - 1u);
         const unsigned rank = (g << lg) | (lg ? (__brev(lid) >> (32 - lg)) : 0u);
-        const unsigned long long key = ((unsigned long long)__float_as_uint(a.lens[k]) << 32) | rank;
+        const unsigned long long key = ((unsigned long long)__float_as_uint(s_len[k]) << 32) | rank;
         best = key < best ? key : best;
     }
     best = block_min_u64(best, red);
@@ -73,14 +82,47 @@ __global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, int 
         const unsigned rank = (unsigned)(best & 0xffffffffu);
         const unsigned g = rank >> lg, br = rank & ((1u << lg) - 1u);
         const int idx = (int)((g << lg) | (lg ? (__brev(br) >> (32 - lg)) : 0u));
-        const float minval = a.lens[idx];
+        const float minval = s_len[idx];
         a.solutions[(size_t)T * (A + 1)] = idx;
         s_best = idx;
         s_minval = minval;
-        s_flag = __fsub_rn(minval, a.lens[A]) < -kEps; // kernel.cl:660
+        s_flag = __fsub_rn(minval, s_bsf) < -kEps; // kernel.cl:660
+    }
+    // get_elites (kernel.cl:717-741): elite 0 is the best-so-far slot, then
+    // ras_ranks-1 rounds of "first minimum, knocked out to +inf".  The finite
+    // lengths come out in (length, index) order; once they are used up every
+    // entry is +inf and each further round takes index 0.  With all lengths in
+    // one pass of the block, each entry's rank is the number of keys below its
+    // own, and the first R-1 finite ranks place themselves.
+    if (do_elites && A <= bs) {
+        // P threads per entry, each counting the keys below it in one slice of the entries
+        const int P = A > 0 ? (bs / A < 8 ? bs / A : 8) : 1;
+        const int slice = (A + P - 1) / P;
+        for (int k = tid; k < A; k += bs) s_rank[k] = 0;
+        __syncthreads();
+        if (tid < A * P) {
+            const int k = tid / P, j0 = (tid - k * P) * slice;
+            const int j1 = j0 + slice < A ? j0 + slice : A;
+            const uint32_t bk = __float_as_uint(s_len[k]);
+            int c = 0;
+            for (int jb = j0; jb < j1; jb += 8) { // eight keys a round, loads first
+                uint32_t bj[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) bj[u] = jb + u < j1 ? __float_as_uint(s_len[jb + u]) : 0xffffffffu;
+#pragma unroll
+                for (int u = 0; u < 8; u++) c += (bj[u] < bk || (bj[u] == bk && jb + u < k)) ? 1 : 0;
+            }
+            if (c) atomicAdd(&s_rank[k], c);
+        }
+        int fin = 0;
+        if (tid < A) fin = __float_as_uint(s_len[tid]) < 0x7f800000u;
+        const int nfin = __syncthreads_count(fin);
+        if (fin && s_rank[tid] < R - 1) s_elite[1 + s_rank[tid]] = tid;
+        if (tid >= 1 + nfin && tid < R) s_elite[tid] = 0;
     }
     __syncthreads();
-    if (s_flag) { // update_best_so_far (kernel.cl:551-585)
+    const bool flag = s_flag;
+    if (flag) { // update_best_so_far (kernel.cl:551-585)
         const int *it = a.solutions + (size_t)T * s_best;
         int *bt = a.solutions + (size_t)T * A;
         const int size = it[T - 1];
@@ -102,39 +144,59 @@ __global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, int 
         }
     }
     if (do_elites) {
-        // get_elites (kernel.cl:717-741): elite 0 is the best-so-far slot, then
-        // ras_ranks-1 first-occurrence minima with knock-out.
-        for (int k = tid; k < A; k += bs) s_hb[k] = a.lens[k];
-        if (tid == 0) a.elites[0] = A;
-        __syncthreads();
-        for (int r = 1; r < a.ras_ranks; r++) {
-            unsigned long long m = ~0ull;
-            for (int k = tid; k < A; k += bs) {
-                const unsigned long long key = ((unsigned long long)__float_as_uint(s_hb[k]) << 32) | (unsigned)k;
-                m = key < m ? key : m;
+        if (A > bs) { // many ants: the knock-out rounds as written
+            for (int r = 1; r < R; r++) {
+                unsigned long long m = ~0ull;
+                for (int k = tid; k < A; k += bs) {
+                    const unsigned long long key = ((unsigned long long)__float_as_uint(s_len[k]) << 32) | (unsigned)k;
+                    m = key < m ? key : m;
+                }
+                m = block_min_u64(m, red);
+                if (tid == 0) {
+                    const int target = A > 0 ? (int)(m & 0xffffffffu) : 0;
+                    s_len[target] = __int_as_float(0x7f800000);
+                    s_elite[r] = target;
+                }
+                __syncthreads();
             }
-            m = block_min_u64(m, red);
-            if (tid == 0) {
-                const int target = A > 0 ? (int)(m & 0xffffffffu) : 0;
-                s_hb[target] = __int_as_float(0x7f800000);
-                a.elites[r] = target;
-            }
-            __syncthreads();
+        }
+        // deposit weights (kernel.cl:767-768) and the elite tours: elite 0 reads
+        // the iteration best directly when it has just become the best-so-far
+        if (tid < R) {
+            const int e = s_elite[tid];
+            a.elites[tid] = e;
+            const int src = (tid == 0 && flag) ? s_best : e;
+            const float len = tid == 0 ? (flag ? s_minval : s_bsf) : a.lens[e];
+            a.d_tau[tid] = __fdiv_rn((float)(R - tid), len);
+            const int *tour = a.solutions + (size_t)T * src;
+            s_tour[tid] = tour;
+            s_size[tid] = __ldg(tour + T - 1);
         }
         // deposit list: successor of every customer in each elite tour and the
         // depot -> customer edges as a per-customer bit mask.
-        const int n = a.n, R = a.ras_ranks;
+        const int n = a.n;
         for (int e = tid; e < R * n; e += bs) a.succ[e] = -1;
         for (int e = tid; e < n; e += bs) a.depmask[e] = 0u;
-        if (tid < R) a.d_tau[tid] = __fdiv_rn((float)(R - tid), a.lens[a.elites[tid]]); // kernel.cl:767-768
         __syncthreads();
-        for (int r = 0; r < R; r++) {
-            const int *tour = a.solutions + (size_t)T * a.elites[r];
-            const int size = tour[T - 1];
-            for (int k = tid; k < size - 1; k += bs) {
-                const int u = tour[k], v = tour[k + 1];
-                if (u != 0) a.succ[(size_t)r * n + u] = v;
-                else atomicOr(&a.depmask[v], 1u << r);
+        // all elites at once: item e = (r, k), edge k of elite r's tour; four
+        // items a thread at a time with their loads issued first
+        const int items = R * (T - 1);
+        for (int e0 = tid; e0 < items; e0 += 4 * bs) {
+            int uu[4], vv[4], rr[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int e = e0 + q * bs;
+                const int r = e < items ? e / (T - 1) : 0, k = e - r * (T - 1);
+                rr[q] = e < items && k < s_size[r] - 1 ? r : -1;
+                const int *tour = s_tour[r];
+                uu[q] = rr[q] >= 0 ? __ldg(tour + k) : 0;
+                vv[q] = rr[q] >= 0 ? __ldg(tour + k + 1) : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (rr[q] < 0) continue;
+                if (uu[q] != 0) a.succ[(size_t)rr[q] * n + uu[q]] = vv[q];
+                else atomicOr(&a.depmask[vv[q]], 1u << rr[q]);
             }
         }
     }
@@ -379,6 +441,11 @@ cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, siz
         cudaError_t e = cudaFuncSetAttribute(stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
+    // the construct and 2-opt kernels before it run with the largest shared
+    // memory carve-out; asking for the same avoids reconfiguring the SMs
+    cudaError_t e = cudaFuncSetAttribute(stats_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     stats_kernel<<<n_inst, 1024, smem, st>>>(d_args, do_elites);
     return cudaGetLastError();
 }

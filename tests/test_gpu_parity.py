@@ -155,6 +155,28 @@ def test_throughput_route_length_limit_vs_oracle(gpu, draw):
         assert S.validate()[1] == 0
 
 
+@pytest.mark.parametrize("A,ranks", [(1100, 8), (4, 6), (1, 3)])
+def test_elites_many_and_few_ants(gpu, A, ranks):
+    """get_elites with more ants than one pass of the statistics block (knock-out
+    rounds) and with fewer ants than ranks (rounds past the last finite length
+    take index 0)."""
+    inst = I.gen_mixed(31, 40)
+    n = inst.n
+    dist = oracle.compute_distances(inst.x, inst.y)
+    nn = oracle.compute_nn_lists(dist, 20, 20)
+    seeds, _ = oracle.make_seeds(1796300000, 77, A, 256)
+    prob = problem_of(inst.x, inst.y, inst.demand, inst.capacity)
+    p = params_for(n, A, 256, 1796300000, 77, True, 20, mode=MODE_THROUGHPUT, nn_ants=20, ras_ranks=ranks)
+    O = oracle.Oracle(dist, inst.demand, inst.capacity, A, 256, nn, seeds, ls_flag=True, nn_ants_list=nn,
+                      ras_ranks=ranks, n_threads=8, ls_pass_limit=4096)
+    with Solver(prob, p) as S:
+        S.init(); O.init_aco(throughput=True)
+        compare_state(S, O)
+        for _ in range(2):
+            S.iterate(1); O.run_iteration(throughput=True)
+            compare_state(S, O)
+
+
 @pytest.mark.parametrize("draw", [-1, 1])
 def test_throughput_large_no_smem_matrix(gpu, draw):
     inst = I.gen_large(11, 1000)
