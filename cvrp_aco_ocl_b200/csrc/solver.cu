@@ -530,7 +530,8 @@ int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *
     const bool thr = c.p.mode == ACO_MODE_THROUGHPUT;
     if (ants_per_block) *ants_per_block = thr ? c.cn_apc : c.cp_apc;
     if (warps_per_ant) *warps_per_ant = thr ? 1 : c.cp_wpa;
-    if (staging_flags) *staging_flags = (thr ? (c.inst[0].smat ? 1 : 0) : (c.cp_stage ? 1 : 0)) | 2;
+    if (staging_flags)
+        *staging_flags = (thr ? (c.inst[0].smat ? 1 : 0) : (c.cp_stage ? 1 : 0)) | 2 | (thr && c.cn_draw ? 4 : 0);
     return ACO_OK;
 }
 

@@ -213,7 +213,8 @@ int aco_enqueue_iterations(aco_solver *s, int n_iter);
 int aco_time_phases(aco_solver *s, int n_iter, float *ms4);
 /* the kernel configuration the solver picked: ants per CTA and warps per ant of
  * construct, and whether matrices are staged in shared memory (bit 0: total_info
- * in construct, bit 1: NN lists in 2-opt). */
+ * in construct, bit 1: NN lists in 2-opt); bit 2: the throughput construct runs
+ * with helper draw warps (construct_nn_draw_kernel). */
 int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *staging_flags);
 
 /* ---- validation and output -------------------------------------------------
