@@ -426,6 +426,81 @@ __device__ __forceinline__ void draw_warp(const int *seedp, float *ring, const i
     }
 }
 
+// Smallest demand among the unvisited customers of an ant (warp-wide result).
+template <bool REGVIS>
+__device__ __forceinline__ int min_open_demand(const int *s_dem, uint32_t vis, const uint32_t *vism, int n, int words,
+                                               int lane)
+{
+    int m = 0x7fffffff;
+    for (int k = 0; k < words; k++) {
+        const int i = lane + 32 * k;
+        const uint32_t vk = REGVIS ? vis : vism[k];
+        if (i > 0 && i < n && !((vk >> (REGVIS ? k : lane)) & 1u)) m = min(m, s_dem[i]);
+    }
+    return (int)__reduce_min_sync(0xffffffffu, (unsigned)m);
+}
+
+// The feasible customer of the full row with the largest total_info (ties:
+// lowest index), -1 if none: the step's path when no listed candidate fits.
+template <bool FIN, bool REGVIS>
+__device__ __forceinline__ int best_of_row(const float *row, const int *s_dem, const float *s_d0, const float *drow,
+                                           uint32_t vis, const uint32_t *vism, int n, int words, int lane, int load,
+                                           int cap, float rdist, float serv, float maxd)
+{
+    const unsigned FULL = 0xffffffffu;
+    uint32_t bk = 0u, bi = 0xffffffffu;
+    constexpr int G = FIN ? 4 : 8;
+    for (int k0 = 0; k0 < words; k0 += G) { // branch-free: every lane tests its own nodes
+        // G nodes a lane at a time, all loads first (indices clamped into range)
+        float rv[G], dv[G];
+        int dm[G];
+#pragma unroll
+        for (int u = 0; u < G; u++) {
+            const int i = lane + 32 * (k0 + u);
+            const int ic = i < n ? i : 0;
+            rv[u] = row[ic];
+            dm[u] = s_dem[ic];
+            if (FIN) dv[u] = __ldg(drow + ic);
+        }
+#pragma unroll
+        for (int u = 0; u < G; u++) {
+            const int k = k0 + u, i = lane + 32 * k;
+            const uint32_t vk = REGVIS ? vis : (k < words ? vism[k] : ~0u);
+            bool ff = i > 0 && i < n && !((vk >> (REGVIS ? (k & 31) : lane)) & 1u) && load + dm[u] <= cap;
+            if (FIN) ff = ff && __fadd_rn(__fadd_rn(rdist, __fadd_rn(dv[u], serv)), s_d0[i < n ? i : 0]) <= maxd;
+            const uint32_t kk = ff ? __float_as_uint(rv[u]) + 1u : 0u;
+            const bool better = kk > bk; // strictly: the lowest k of a lane wins ties
+            bk = better ? kk : bk;
+            bi = better ? (uint32_t)i : bi;
+        }
+    }
+    const uint32_t hk = __reduce_max_sync(FULL, bk);
+    if (hk == 0u) return -1;
+    return (int)__reduce_min_sync(FULL, bk == hk ? bi : 0xffffffffu);
+}
+
+struct FallbackPick {
+    int nxt, mind; // nxt -1: no customer fits
+};
+
+// best_of_row out of line, for the kernel without helper warps (many ants per
+// SM), with a shortcut: mind is the smallest demand among unvisited customers
+// (refreshed here when stale); when even it does not fit, no customer does and
+// the row is not scanned.  Measured: the shortcut and the call pay off there,
+// while in the helper-warp kernel (one ant warp per SMSP, latency bound) the
+// plain inline scan is faster, so that kernel keeps it.
+template <bool FIN, bool REGVIS>
+__device__ __noinline__ FallbackPick fallback_pick(const float *row, const int *s_dem, const float *s_d0,
+                                                   const float *drow, uint32_t vis, const uint32_t *vism, int n,
+                                                   int words, int lane, int load, int cap, float rdist, float serv,
+                                                   float maxd, int mind, bool stale)
+{
+    if (stale) mind = min_open_demand<REGVIS>(s_dem, vis, vism, n, words, lane);
+    if (mind > cap - load) return {-1, mind};
+    return {best_of_row<FIN, REGVIS>(row, s_dem, s_d0, drow, vis, vism, n, words, lane, load, cap, rdist, serv, maxd),
+            mind};
+}
+
 template <bool FIN, bool SMAT, bool PACKED, bool REGVIS, bool GTAB = false, bool LSF = false, bool DRAW = false>
 __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int apc, int ant0, unsigned char *smem, uint32_t phase,
                                   int lsw = 0)
@@ -524,6 +599,11 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             __syncwarp();
         }
         if (lane == 0) tbuf[0] = 0;
+        // smallest demand among the unvisited customers (fallback_pick): visits
+        // only raise it, so it is refreshed lazily, on the fallback path, after
+        // the customer holding it has been visited
+        int mind = DRAW ? 0 : min_open_demand<REGVIS>(s_dem, vis, vism, n, words, lane);
+        bool mind_stale = false;
         // lane l draws from the ant's Park-Miller state l (nloc >= 32), one number a step
         int *seedp = a.seeds + (size_t)ant * a.nloc;
         uint32_t xs = pm_norm(seedp[lane]);
@@ -580,41 +660,19 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 const uint32_t pick = __shfl_sync(FULL, (uint32_t)c | ((uint32_t)dc << 16), 31 - (int)(hk & 31u));
                 nxt = (int)(pick & 0xFFFFu);
                 nd = (int)(pick >> 16);
-            } else { // no listed candidate fits: best feasible customer of the full row
-                uint32_t bk = 0u, bi = 0xffffffffu;
-                const float *row = SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld;
-                constexpr int G = FIN ? 4 : 8;
-                for (int k0 = 0; k0 < words; k0 += G) { // branch-free: every lane tests its own nodes
-                    // G nodes a lane at a time, all loads first (indices clamped into range)
-                    float rv[G], dv[G];
-                    int dm[G];
-#pragma unroll
-                    for (int u = 0; u < G; u++) {
-                        const int i = lane + 32 * (k0 + u);
-                        const int ic = i < n ? i : 0;
-                        rv[u] = row[ic];
-                        dm[u] = s_dem[ic];
-                        if (FIN) dv[u] = __ldg(a.dist + (size_t)cur * ld + ic);
-                    }
-#pragma unroll
-                    for (int u = 0; u < G; u++) {
-                        const int k = k0 + u, i = lane + 32 * k;
-                        const uint32_t vk = REGVIS ? vis : (k < words ? vism[k] : ~0u);
-                        bool ff = i > 0 && i < n && !((vk >> (REGVIS ? (k & 31) : lane)) & 1u) && load + dm[u] <= cap;
-                        if (FIN)
-                            ff = ff && __fadd_rn(__fadd_rn(rdist, __fadd_rn(dv[u], a.serv_time)), s_d0[i < n ? i : 0]) <=
-                                           a.max_dist;
-                        const uint32_t kk = ff ? __float_as_uint(rv[u]) + 1u : 0u;
-                        const bool better = kk > bk; // strictly: the lowest k of a lane wins ties
-                        bk = better ? kk : bk;
-                        bi = better ? (uint32_t)i : bi;
-                    }
-                }
-                const uint32_t hk = __reduce_max_sync(FULL, bk);
-                if (hk != 0u) {
-                    nxt = (int)__reduce_min_sync(FULL, bk == hk ? bi : 0xffffffffu);
-                    nd = s_dem[nxt];
-                }
+            } else if (DRAW) {
+                nxt = best_of_row<FIN, REGVIS>(SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld, s_dem, s_d0,
+                                               a.dist + (size_t)cur * ld, vis, vism, n, words, lane, load, cap, rdist,
+                                               a.serv_time, a.max_dist);
+                if (nxt >= 0) nd = s_dem[nxt];
+            } else {
+                const FallbackPick fp = fallback_pick<FIN, REGVIS>(
+                    SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld, s_dem, s_d0, a.dist + (size_t)cur * ld, vis,
+                    vism, n, words, lane, load, cap, rdist, a.serv_time, a.max_dist, mind, mind_stale);
+                mind = fp.mind;
+                mind_stale = false;
+                nxt = fp.nxt;
+                if (nxt >= 0) nd = s_dem[nxt];
             }
             step++;
             if (nxt < 0) {
@@ -632,6 +690,7 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 if (lane == 0) vism[nxt >> 5] |= 1u << (nxt & 31);
                 __syncwarp();
             }
+            if (!DRAW) mind_stale |= nxt != 0 && nd == mind; // the smallest may have gone
             if (lane == 0) tbuf[step] = (uint16_t)nxt;
             if (LSF) {
                 if (nxt != 0) {
