@@ -68,6 +68,7 @@ class AcoParams(ctypes.Structure):
         ("ns_rounds", ctypes.c_int),
         ("ls_ants", ctypes.c_int),
         ("draw_warps", ctypes.c_int),
+        ("route_ls", ctypes.c_int),
     ]
 
 

@@ -29,6 +29,7 @@ namespace {
 
 // 227 KB per CTA minus room for the kernels' static shared memory
 constexpr size_t kSmemBudget = 226 * 1024;
+constexpr int kRouteWarps = 16; // warps per CTA of the route-level 2-opt
 constexpr int kSwapLimitPerNode = 64; // accepted swaps per node and tour before ACO_ERR_LS_LIMIT
 
 int exp_as_int(float e)
@@ -285,6 +286,31 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     const size_t o_sw_items = take((size_t)total_ants * sizeof(int2));
     const size_t o_ns_items = take((size_t)total_ants * sizeof(int2));
     const size_t o_ls_needed = take((size_t)total_ants);
+    // route list of the route-level 2-opt: throughput mode with 2-opt, instances
+    // whose distance matrix is symmetric (it sums tour lengths from the matrix)
+    {
+        int n_max = 0;
+        bool sym = true;
+        long long cap = 0;
+        for (const InstHost &ih : inst) {
+            n_max = std::max(n_max, ih.n);
+            cap += (long long)ih.A * std::min(ih.n - 1, 64);
+            if (!ih.device_prep) // coordinate formulas are symmetric; a given matrix is checked
+                for (int i = 0; i < ih.n && sym; i++)
+                    for (int j = 0; j < i; j++)
+                        if (ih.dist[(size_t)i * ih.n + j] != ih.dist[(size_t)j * ih.n + i]) {
+                            sym = false;
+                            break;
+                        }
+        }
+        // measured: with few ants per SM the per-ant kernel is as fast (the slowest
+        // route sets the time either way) and the list costs the construct a pass
+        use_routes_ = p.mode == ACO_MODE_THROUGHPUT && (p.ls_flag & 1) && sym && n_max <= 4096 &&
+                      cap < (1ll << 30) && (p.route_ls > 0 || (p.route_ls == 0 && total_ants > 4 * sm_count));
+        route_cap_ = use_routes_ ? (int)cap : 0;
+    }
+    const size_t o_rdesc = take((size_t)route_cap_ * sizeof(int2)), o_rctr = take(16);
+    const size_t o_rrem = take((size_t)total_ants * 4);
 
     void *arena = nullptr;
     if (res->pool && cudaMallocFromPoolAsync(&arena, off, res->pool, st) == cudaSuccess) {
@@ -334,6 +360,9 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     sw_items_d_ = (int2 *)(base + o_sw_items);
     ns_items_d_ = (int2 *)(base + o_ns_items);
     ls_needed_d_ = (uint8_t *)(base + o_ls_needed);
+    route_desc_d_ = (int2 *)(base + o_rdesc);
+    route_ctr_d_ = (int *)(base + o_rctr);
+    route_rem_d_ = (int *)(base + o_rrem);
 
     // ---- configuration (shared-memory budgets over the largest instance)
     const bool throughput = p.mode == ACO_MODE_THROUGHPUT;
@@ -578,6 +607,10 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         c.smat = ih.smat ? 1 : 0; c.packed = ih.packed ? 1 : 0; c.gtab = ih.gtab ? 1 : 0;
         c.nn_list = ih.nnls_d; c.nn_ls = ih.nn_ls; c.pass_limit = p.ls_pass_limit; c.ant_base = ant_base[b];
         c.ls_needed = ls_needed_d_;
+        c.route_desc = use_routes_ ? route_desc_d_ : nullptr;
+        c.route_ctr = route_ctr_d_;
+        c.route_rem = route_rem_d_;
+        c.route_cap = route_cap_;
         c.seeds = ih.seeds_d; c.solutions = ih.sol_d; c.lens = ih.lens_d; c.status = status_d;
         LocalSearchArgs &l = largs[b];
         l = LocalSearchArgs{};
@@ -817,6 +850,10 @@ int Colony::construct(bool fused)
     }
     const int lsw = fused && p.ls_flag ? cn_lsw : 0; // the queue starts at 0 (zeroed arena, rewound by the kernel)
     last_fused_ = lsw > 0;
+    // the route list is rewound by the 2-opt kernel that consumes it; a second
+    // construct without one in between starts it afresh
+    if (use_routes_ && lsw == 0 && routes_pending_) CK(cudaMemsetAsync(route_ctr_d_, 0, 16, st));
+    routes_pending_ = use_routes_ && lsw == 0;
     CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st, lsw,
                            cn_draw));
     return ACO_OK;
@@ -824,9 +861,15 @@ int Colony::construct(bool fused)
 
 int Colony::local_search()
 {
-    // after a fused construct only the ants it marked still need the 2-opt kernel
+    // after a fused construct or the route-level kernel, only the ants marked
+    // in ls_needed still need the per-ant kernel
+    const bool routes = routes_pending_;
+    if (routes)
+        CK(launch_route_opt(largs_d_, ant_inst_d_, ant_base_d_, route_desc_d_, route_ctr_d_, route_cap_, route_rem_d_,
+                            ls_needed_d_, ls_nmax, kRouteWarps, sm_count, st));
+    routes_pending_ = false;
     CK(launch_local_search(largs_d_, ant_inst_d_, ant_base_d_, total_ants, ls_apc, ls_nmax, ls_warps, ls_smem, st,
-                           last_fused_ ? ls_needed_d_ : nullptr));
+                           last_fused_ || routes ? ls_needed_d_ : nullptr));
     last_fused_ = false;
     if (p.ls_flag & 2) CK(launch_swap(cargs_d_, sw_items_d_, sw_items, sw_apc, sw_smem, kSwapLimitPerNode, st));
     return ACO_OK;

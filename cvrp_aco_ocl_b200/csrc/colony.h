@@ -120,6 +120,12 @@ private:
     unsigned long long *t0_d_ = nullptr;
     int2 *items_d_ = nullptr, *sw_items_d_ = nullptr, *ns_items_d_ = nullptr;
     uint8_t *ls_needed_d_ = nullptr;
+    // route-level 2-opt (throughput mode, symmetric distances): the construct's
+    // route list, its counters and the listed routes left per ant
+    bool use_routes_ = false, routes_pending_ = false;
+    int route_cap_ = 0;
+    int2 *route_desc_d_ = nullptr;
+    int *route_ctr_d_ = nullptr, *route_rem_d_ = nullptr;
     bool last_fused_ = false;
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
     int *row_base_d_ = nullptr, *zero_base_d_ = nullptr;

@@ -426,6 +426,55 @@ __device__ __forceinline__ void draw_warp(const int *seedp, float *ring, const i
     }
 }
 
+// The route list entries of one finished ant (warp-wide): route r is the
+// positions [depot r, depot r+1) of its tour; routes of at most 32 nodes are
+// listed for the route-level 2-opt, longer ones flag the ant for the per-ant
+// kernel (and so does a full list, for all of its routes).
+__device__ __forceinline__ void emit_routes(const ConstructArgs &a, const uint16_t *tbuf, int size, int g, int lane)
+{
+    const unsigned FULL = 0xffffffffu;
+    int nshort = 0, prev = 0;
+    bool longr = false;
+    for (int base = 0; base < size; base += 32) { // count
+        const int p = base + lane;
+        unsigned m = __ballot_sync(FULL, p >= 1 && p < size && tbuf[p < size ? p : 0] == 0);
+        while (m) {
+            const int q = base + __ffs(m) - 1;
+            m &= m - 1;
+            if (q - prev <= 32) nshort++;
+            else longr = true;
+            prev = q;
+        }
+    }
+    int rbase = 0;
+    if (lane == 0 && nshort > 0) rbase = atomicAdd(a.route_ctr, nshort);
+    rbase = __shfl_sync(FULL, rbase, 0);
+    const bool fits = rbase + nshort <= a.route_cap;
+    if (fits && nshort > 0) { // write
+        int k = 0;
+        prev = 0;
+        for (int base = 0; base < size; base += 32) {
+            const int p = base + lane;
+            unsigned m = __ballot_sync(FULL, p >= 1 && p < size && tbuf[p < size ? p : 0] == 0);
+            while (m) {
+                const int q = base + __ffs(m) - 1;
+                m &= m - 1;
+                if (q - prev <= 32) {
+                    if (lane == (k & 31)) a.route_desc[rbase + k] = make_int2(g, prev | ((q - prev) << 20));
+                    k++;
+                }
+                prev = q;
+            }
+        }
+    }
+    if (!fits) // entries of this reservation below the capacity are read: mark them empty
+        for (int k = lane; k < nshort && rbase + k < a.route_cap; k += 32) a.route_desc[rbase + k] = make_int2(-1, 0);
+    if (lane == 0) {
+        a.route_rem[g] = fits ? nshort : 0;
+        a.ls_needed[g] = (uint8_t)(!fits ? 2 : (longr ? 1 : 0));
+    }
+}
+
 // Smallest demand among the unvisited customers of an ant (warp-wide result).
 template <bool REGVIS>
 __device__ __forceinline__ int min_open_demand(const int *s_dem, uint32_t vis, const uint32_t *vism, int n, int words,
@@ -742,6 +791,10 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 tour[T - 1] = 0;
                 a.lens[ant] = __int_as_float(0x7f800000);
                 set_status(a.status, err);
+                if (!LSF && a.route_desc) {
+                    a.route_rem[a.ant_base + ant] = 0;
+                    a.ls_needed[a.ant_base + ant] = 0;
+                }
             }
         } else {
             const int size = step + 2;
@@ -767,6 +820,7 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 tour[T - 1] = size;
                 a.lens[ant] = tdist;
             }
+            if (!LSF && a.route_desc) emit_routes(a, tbuf, size, a.ant_base + ant, lane);
         }
         if (step > 0) // states after the last draw (the helper may have drawn further)
             seedp[lane] = (int)(DRAW ? pm_mul(xs, pm_pow16807(step)) : xs);

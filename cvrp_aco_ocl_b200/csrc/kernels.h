@@ -47,6 +47,14 @@ struct ConstructArgs {
     const int *nn_list;    // n x nn_ls
     int nn_ls, pass_limit, ant_base;
     uint8_t *ls_needed;    // total ants of the colony
+    // route list for the route-level 2-opt (null: not used): every route of at
+    // most 32 nodes as {global ant, first position | nodes << 20}; route_ctr[0]
+    // counts the entries (capacity route_cap), route_rem[g] the entries of ant g.
+    // ls_needed[g]: 1 = the ant also has longer routes, 2 = none of its routes
+    // listed (the list was full) -- the per-ant kernel does those.
+    int2 *route_desc;
+    int *route_ctr, *route_rem;
+    int route_cap;
     int *seeds;
     int *solutions;
     float *lens;
@@ -125,6 +133,12 @@ cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items
                                 int ls_warps = 0, bool draw = false);
 // 2-opt: one CTA of `warps` warps per ant; d_ant_inst[g] = instance of global ant g,
 // d_ant_base[b] = first global ant of instance b.
+// Route-level 2-opt over the construct's route list (d_ctr: {entries, next,
+// CTAs done}, rewound by the kernel); a persistent grid of `warps`-warp CTAs.
+size_t route_opt_smem(int n_max, int warps);
+cudaError_t launch_route_opt(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
+                             const int2 *d_desc, int *d_ctr, int cap, int *d_rem, const uint8_t *d_flagged, int n_max,
+                             int warps, int sm_count, cudaStream_t st);
 // 2-opt: CTAs of `ants_per_cta` ants (1..8) and `warps` warps pulling routes;
 // n_max sizes the per-ant shared buffers.  only (after a fused construct):
 // skip ants whose flag is 0 and, in the others, routes of at most 32 nodes.

@@ -234,6 +234,7 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_inst[kMaxLsAnts], s_ant[kMaxLsAnts], s_size[kMaxLsAnts], s_routes[kMaxLsAnts + 1];
+    __shared__ int s_only[kMaxLsAnts]; // 1: the short routes of this ant are done already
     __shared__ int s_next;
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -257,6 +258,7 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
         }
         s_inst[j] = inst;
         s_ant[j] = ant;
+        s_only[j] = only && g < total_ants ? only[g] : 0;
         s_size[j] = inst >= 0 ? size : 0;
     }
     __syncthreads();
@@ -349,9 +351,9 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
         float *dt = reinterpret_cast<float *>(ant_ptr(j, AL.dt));
         const int rb = rstart[r], re = rstart[r + 1] - 1, R = re - rb + 1;
         int st = ACO_OK;
-        if (R <= kRL && only) {
-            // after a fused construct the routes of at most 32 nodes are improved
-            // already; only the longer ones of a flagged ant are left here
+        if (R <= kRL && s_only[j] == 1) {
+            // routes of at most 32 nodes improved already (fused construct or
+            // route-level kernel); only the longer ones of this ant are left here
         } else if (R <= kRL) {
             // route-local state: the distance tile (row k1 = distances from route
             // node k1, lane k2 its column) and every route node's neighbour list
@@ -449,6 +451,131 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
 
 } // namespace
 
+// ---------------------------------------------------------------------------
+// Route-level 2-opt (throughput construct): every route of at most 32 nodes
+// of every ant is one entry of the list the construct kernel wrote, and the
+// warps of a persistent grid take entries from a counter, so the routes of
+// one ant spread over all SMs instead of queueing in one CTA.  A route needs
+// no state of its ant beyond its own nodes: its membership test is a per-warp
+// node -> local index map in shared memory, set for the route and cleared
+// after it.  The warp that improves an ant's last listed route sums the ant's
+// tour length (kernel.cl:534-538) from the distances of its final tour edges,
+// which equal the 2-opt's edge lengths for a symmetric matrix (the only case
+// this kernel is used for); ants flagged for the per-ant kernel get their
+// length there.
+// ---------------------------------------------------------------------------
+constexpr int kRouteRows = 4; // tile rows loaded per round (register budget of two CTAs per SM)
+
+__host__ __device__ inline size_t route_warp_bytes(int n_max)
+{
+    return kRL * kRL * 4 + kRL * kRL + kRL + al16((size_t)n_max);
+}
+
+__global__ void __launch_bounds__(512, 2) route_opt_kernel(const LocalSearchArgs *args, const int *ant_inst,
+                                                           const int *ant_base, const int2 *desc, int *ctr, int cap,
+                                                           int *rem, const uint8_t *flagged, int n_max)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *wbase = smem + (size_t)warp * route_warp_bytes(n_max);
+    float *tile = reinterpret_cast<float *>(wbase);
+    uint8_t *lnn = wbase + kRL * kRL * 4;
+    uint8_t *lcnt = lnn + kRL * kRL;
+    uint8_t *loc = lcnt + kRL; // node -> local index (0: not in the route)
+    for (int i = lane; i < n_max; i += 32) loc[i] = 0;
+    __syncwarp();
+    const int total = min(ctr[0], cap);
+    for (;;) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(&ctr[1], 1);
+        idx = __shfl_sync(FULL, idx, 0);
+        if (idx >= total) break;
+        const int2 d = desc[idx];
+        if (d.x < 0) continue; // an empty entry
+        const int g = d.x, rb = d.y & 0xFFFFF, R = d.y >> 20;
+        const int b = __ldg(ant_inst + g), ant = g - __ldg(ant_base + b);
+        const LocalSearchArgs a = args[b];
+        int *gt = a.solutions + (size_t)ant * a.T;
+        const int v = lane < R ? gt[rb + lane] : 0;
+        if (lane >= 1 && lane < R) loc[v] = (uint8_t)lane; // customers only (kernel.cl:293-300)
+        __syncwarp();
+        for (int k0 = 0; k0 < R; k0 += kRouteRows) {
+            float dd[kRouteRows];
+            int nb[kRouteRows];
+#pragma unroll
+            for (int u = 0; u < kRouteRows; u++) {
+                const int k1 = k0 + u;
+                const int node1 = __shfl_sync(FULL, v, k1 & 31);
+                dd[u] = (k1 < R && lane < R) ? __ldg(a.dist + (size_t)node1 * a.ld + v) : 0.f;
+                nb[u] = (k1 < R && lane < a.nn_ls) ? __ldg(a.nn_list + (size_t)node1 * a.nn_ls + lane) : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < kRouteRows; u++) {
+                const int k1 = k0 + u;
+                if (k1 >= R) break; // warp-uniform
+                tile[k1 * kRL + lane] = dd[u];
+                const int n2 = nb[u];
+                const int l2 = n2 != 0 ? loc[n2] : 0;
+                const unsigned m = __ballot_sync(FULL, l2 != 0);
+                const int slot = __popc(m & ((1u << lane) - 1u));
+                if (l2 != 0 && slot < kRL) lnn[k1 * kRL + slot] = (uint8_t)l2;
+                int cnt = __popc(m);
+                const int node1 = __shfl_sync(FULL, v, k1 & 31);
+                for (int h0 = 32; h0 < a.nn_ls && cnt < R - 1; h0 += 32) { // lists deeper than 32
+                    const int h = h0 + lane;
+                    const int n3 = h < a.nn_ls ? __ldg(a.nn_list + (size_t)node1 * a.nn_ls + h) : 0;
+                    const int l3 = n3 != 0 ? loc[n3] : 0;
+                    const unsigned m3 = __ballot_sync(FULL, l3 != 0);
+                    const int slot3 = cnt + __popc(m3 & ((1u << lane) - 1u));
+                    if (l3 != 0 && slot3 < kRL) lnn[k1 * kRL + slot3] = (uint8_t)l3;
+                    cnt += __popc(m3);
+                }
+                if (lane == 0) lcnt[k1] = (uint8_t)(cnt < R - 1 ? cnt : R - 1);
+            }
+        }
+        __syncwarp();
+        // edge lengths: position q -> q+1, the last one back to the next depot (node 0 = local 0)
+        int tq = lane < R ? lane : 0, pk = lane < R ? lane : 0;
+        float dq = lane < R ? tile[lane * kRL + (lane + 1 < R ? lane + 1 : 0)] : 0.f;
+        const int st = two_opt_route_regs(lane, R, rb == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
+        if (st != ACO_OK && lane == 0) set_status(a.status, st);
+        const int node = __shfl_sync(FULL, v, tq);
+        if (lane < R) gt[rb + lane] = node;
+        if (lane >= 1 && lane < R) loc[v] = 0;
+        __syncwarp();
+        __threadfence();
+        int last = 0;
+        if (lane == 0) last = atomicSub(rem + g, 1) == 1;
+        last = __shfl_sync(FULL, last, 0);
+        if (last && !flagged[g]) { // every route of the ant is final: its length
+            __threadfence();
+            const int size = __ldcg(gt + a.T - 1);
+            float len = 0.f;
+            for (int base = 0; base < size - 1; base += 32) {
+                const int p = base + lane;
+                const float e = p < size - 1 ? __ldg(a.dist + (size_t)__ldcg(gt + p) * a.ld + __ldcg(gt + p + 1)) : 0.f;
+                const int m = size - 1 - base < 32 ? size - 1 - base : 32;
+#pragma unroll
+                for (int k = 0; k < 32; k++) {
+                    const float x = __shfl_sync(FULL, e, k);
+                    if (k < m) len = __fadd_rn(len, x);
+                }
+            }
+            if (lane == 0) a.lens[ant] = len;
+        }
+    }
+    // the last CTA to finish rewinds the list for the next iteration
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctr[2], 1) == (int)gridDim.x - 1) {
+            ctr[0] = 0;
+            ctr[1] = 0;
+            ctr[2] = 0;
+        }
+    }
+}
+
 size_t local_search_smem(int n_max, int ants_per_cta, int warps) { return ls_smem_bytes(n_max, ants_per_cta, warps); }
 
 int local_search_occupancy(int warps, size_t smem)
@@ -459,6 +586,24 @@ int local_search_occupancy(int warps, size_t smem)
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, local_search_kernel, warps * 32, smem) != cudaSuccess)
         return 0;
     return blocks;
+}
+
+size_t route_opt_smem(int n_max, int warps) { return (size_t)warps * route_warp_bytes(n_max); }
+
+cudaError_t launch_route_opt(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
+                             const int2 *d_desc, int *d_ctr, int cap, int *d_rem, const uint8_t *d_flagged, int n_max,
+                             int warps, int sm_count, cudaStream_t st)
+{
+    const size_t smem = route_opt_smem(n_max, warps);
+    cudaError_t e = cudaFuncSetAttribute(route_opt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, route_opt_kernel, warps * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    route_opt_kernel<<<sm_count * per_sm, warps * 32, smem, st>>>(d_args, d_ant_inst, d_ant_base, d_desc, d_ctr, cap,
+                                                                   d_rem, d_flagged, n_max);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,

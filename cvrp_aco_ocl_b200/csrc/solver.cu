@@ -71,6 +71,7 @@ int check_params(const aco_params &p, int n)
     if (p.fuse_ls < 0 || p.fuse_ls > 1) return ACO_ERR_INVALID;
     if (p.ls_ants < 0 || p.ls_ants > 8) return ACO_ERR_INVALID;
     if (p.draw_warps < -1 || p.draw_warps > 1) return ACO_ERR_INVALID;
+    if (p.route_ls < -1 || p.route_ls > 1) return ACO_ERR_INVALID;
     if (!(p.rho > 0.0f && p.rho <= 1.0f)) return ACO_ERR_INVALID;
     if (p.n_ants > 56 * 1024) return ACO_ERR_INVALID; // the statistics kernel holds n_ants lengths in shared memory
     return ACO_OK;

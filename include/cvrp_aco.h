@@ -45,7 +45,7 @@ extern "C" {
 enum { ACO_DIST_EUC_2D = 0, ACO_DIST_CEIL_2D = 1, ACO_DIST_GEO = 2, ACO_DIST_ATT = 3 }; /* problem.h:36-38 */
 enum {
     ACO_MODE_PARITY = 0,     /* full-row I-Roulette with the reference's RNG stream: bit-exact */
-    ACO_MODE_THROUGHPUT = 1  /* nearest-neighbour candidate lists + prefix-sum roulette */
+    ACO_MODE_THROUGHPUT = 1  /* nearest-neighbour candidate lists, roulette probabilities drawn as an exponential race */
 };
 
 /* Instance: the fields of Problem the path reads (problem.h:82-99).  Either
@@ -103,6 +103,10 @@ typedef struct aco_params {
     int draw_warps;       /* throughput construct: 1 = a helper warp per ant makes the ant's draws ahead of it
                              (at most 8 ants per CTA), -1 = the ant's warp draws, 0 = automatic (helper warps
                              while there are at most 4 ants per SM); same results either way */
+    int route_ls;         /* throughput mode with 2-opt, symmetric distances: 1 = the construct lists every route
+                             of at most 32 nodes and one persistent kernel improves them all, spread over the SMs;
+                             -1 = one CTA per group of ants; 0 = automatic (the list above 4 ants per SM); same
+                             results either way */
 } aco_params;
 
 /* One best-so-far record {iteration, length, seconds since init} (problem.h:62-66). */

@@ -74,6 +74,22 @@ def test_batch_members_match_single_solvers(gpu, sizes, A):
                 assert_same(B, b, S)
 
 
+def test_batch_route_level_2opt_matches_single_solvers(gpu):
+    # the route list spans all instances of the batch; members still run exactly
+    # the single solver's iteration (per-ant 2-opt kernel)
+    probs = mixed_problems(420, [40, 120, 200, 75, 333])
+    A, rs0 = 40, 777
+    p = batch_params(max(pr.num_node for pr in probs), A, rs0, route_ls=1)
+    with Batch(probs, p) as B:
+        B.init()
+        B.iterate(3)
+        for b, pr in enumerate(probs):
+            with Solver(pr, batch_params(pr.num_node, A, rs0 + b, route_ls=-1)) as S:
+                S.init()
+                S.iterate(3)
+                assert_same(B, b, S)
+
+
 def test_batch_member_matches_oracle(gpu):
     probs = mixed_problems(77, [150, 60, 90])
     A = 32

@@ -155,6 +155,27 @@ def test_throughput_route_length_limit_vs_oracle(gpu, draw):
         assert S.validate()[1] == 0
 
 
+@pytest.mark.parametrize("per_route,n_cust,A", [(12.0, 200, 100), (45.0, 200, 40), (2.0, 150, 24)])
+def test_route_level_2opt_vs_oracle(gpu, per_route, n_cust, A):
+    """route_ls = 1: the construct lists the routes of at most 32 nodes and one
+    persistent kernel improves them; longer routes (45 customers a route) and
+    ants whose routes overflow the list (about 80 routes an ant against 64 list
+    entries an ant) go to the per-ant kernel.  Same bits as the oracle and as
+    the per-ant kernel alone."""
+    inst = I.gen_mixed(900 + n_cust, n_cust, customers_per_route=per_route)
+    S, O = build_pair(inst, A, 256, 1796300000, 93, True, 25, mode=MODE_THROUGHPUT, nn_ants=25, route_ls=1)
+    p2 = params_for(inst.n, A, 256, 1796300000, 93, True, 25, mode=MODE_THROUGHPUT, nn_ants=25, route_ls=-1)
+    prob = problem_of(inst.x, inst.y, inst.demand, inst.capacity)
+    with S, Solver(prob, p2) as S2:
+        S.init(); S2.init(); O.init_aco(throughput=True)
+        compare_state(S, O)
+        for _ in range(3):
+            S.iterate(1); S2.iterate(1); O.run_iteration(throughput=True)
+            compare_state(S, O)
+            a, b = S.solutions(), S2.solutions()
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
 @pytest.mark.parametrize("A,ranks", [(1100, 8), (4, 6), (1, 3)])
 def test_elites_many_and_few_ants(gpu, A, ranks):
     """get_elites with more ants than one pass of the statistics block (knock-out
