@@ -30,7 +30,7 @@ EXPORTED = [
     "aco_pheromone_update", "aco_pheromone_init", "aco_get_best", "aco_get_bsf_records",
     "aco_get_solutions", "aco_get_pheromone", "aco_get_seeds", "aco_get_elites", "aco_get_iteration",
     "aco_set_state", "aco_status", "aco_strerror", "aco_get_stream", "aco_launches_per_iteration",
-    "aco_time_iterations", "aco_enqueue_iterations", "aco_time_phases", "aco_get_config",
+    "aco_time_iterations", "aco_enqueue_iterations", "aco_enqueue_lengths", "aco_read_lengths", "aco_time_phases", "aco_get_config",
     "aco_pheromone_update_noalloc", "aco_batch_create", "aco_batch_init", "aco_batch_iterate",
     "aco_batch_enqueue_iterations", "aco_batch_status", "aco_batch_size", "aco_batch_get_best",
     "aco_batch_get_solutions", "aco_batch_get_pheromone", "aco_batch_time_phases", "aco_batch_get_stream",
@@ -119,6 +119,8 @@ def lib() -> ctypes.CDLL:
         L.aco_get_stream.restype = vp
         L.aco_time_iterations.argtypes = [vp, ip, ctypes.POINTER(fp)]
         L.aco_enqueue_iterations.argtypes = [vp, ip]
+        L.aco_enqueue_lengths.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.aco_read_lengths.argtypes = [vp, ctypes.c_longlong, vp, ctypes.c_size_t]
         L.aco_time_phases.argtypes = [vp, ip, vp]
         L.aco_pheromone_update_noalloc.argtypes = [ip, ip, ip, ip, fp, fp, fp, vp, vp, vp, vp, vp, vp, vp]
         L.aco_batch_create.argtypes = [ctypes.POINTER(AcoInstance), ip, ctypes.POINTER(AcoParams), ctypes.POINTER(vp)]

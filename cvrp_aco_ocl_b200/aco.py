@@ -341,6 +341,20 @@ class Solver:
     def enqueue(self, n_iter: int = 1):
         check(lib().aco_enqueue_iterations(self.h, n_iter), "aco_enqueue_iterations")
 
+    def enqueue_lengths(self) -> int:
+        """Queue a copy of the A+1 tour lengths as they stand after the work
+        queued so far; returns a ticket for read_lengths (at most 4 outstanding)."""
+        t = ctypes.c_longlong()
+        check(lib().aco_enqueue_lengths(self.h, ctypes.byref(t)), "aco_enqueue_lengths")
+        return t.value
+
+    def read_lengths(self, ticket: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Wait for the copy of `ticket` only and return the lengths."""
+        if out is None:
+            out = np.empty(self.A + 1, np.float32)
+        check(lib().aco_read_lengths(self.h, ticket, ptr(out), out.size), "aco_read_lengths")
+        return out
+
     def time_phases(self, n_iter: int) -> np.ndarray:
         ms = np.zeros(4, np.float32)
         check(lib().aco_time_phases(self.h, n_iter, ptr(ms)), "aco_time_phases")

@@ -31,8 +31,27 @@
 
 using namespace aco;
 
+// Pipelined length readback: a ring of pinned host slots, each filled by a
+// stream-ordered copy and marked by an event, so a caller can queue the next
+// iteration before waiting for the lengths of the previous one.
+constexpr int kLenSlots = 4;
+
 struct aco_solver {
     Colony c;
+    float *len_ring = nullptr; // kLenSlots x (A + 2) pinned words: A + 1 lengths, the status word
+    cudaEvent_t len_ev[kLenSlots] = {};
+    long long len_ticket[kLenSlots] = {-1, -1, -1, -1};
+    long long next_ticket = 0;
+    ~aco_solver()
+    {
+        if (len_ring) {
+            c.set_device();
+            cudaStreamSynchronize(c.st);
+            for (int k = 0; k < kLenSlots; k++)
+                if (len_ev[k]) cudaEventDestroy(len_ev[k]);
+            cudaFreeHost(len_ring);
+        }
+    }
 };
 
 struct aco_batch {
@@ -333,6 +352,50 @@ int aco_enqueue_iterations(aco_solver *s, int n_iter)
 {
     if (!s || n_iter < 0) return ACO_ERR_INVALID;
     return s->c.enqueue(n_iter);
+}
+
+int aco_enqueue_lengths(aco_solver *s, long long *ticket)
+{
+    if (!s || !ticket) return ACO_ERR_INVALID;
+    Colony &c = s->c;
+    if (!c.initialized) return ACO_ERR_STATE;
+    if (c.set_device() != ACO_OK) return ACO_ERR_CUDA;
+    const int A = c.inst[0].A;
+    if (!s->len_ring) { // first use: the ring and its events
+        if (cudaMallocHost(&s->len_ring, sizeof(float) * (size_t)(A + 2) * kLenSlots) != cudaSuccess) {
+            s->len_ring = nullptr;
+            return ACO_ERR_NOMEM;
+        }
+        for (int k = 0; k < kLenSlots; k++)
+            CK(cudaEventCreateWithFlags(&s->len_ev[k], cudaEventDisableTiming));
+    }
+    const long long t = s->next_ticket;
+    const int slot = (int)(t % kLenSlots);
+    float *dst = s->len_ring + (size_t)slot * (A + 2);
+    CK(cudaMemcpyAsync(dst, c.inst[0].lens_d, sizeof(float) * (A + 1), cudaMemcpyDeviceToHost, c.st));
+    CK(cudaMemcpyAsync(dst + A + 1, c.status_d, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+    CK(cudaEventRecord(s->len_ev[slot], c.st));
+    s->len_ticket[slot] = t;
+    s->next_ticket = t + 1;
+    *ticket = t;
+    return ACO_OK;
+}
+
+int aco_read_lengths(aco_solver *s, long long ticket, float *lens, size_t cap)
+{
+    if (!s || !lens || ticket < 0) return ACO_ERR_INVALID;
+    Colony &c = s->c;
+    const int slot = (int)(ticket % kLenSlots);
+    if (!s->len_ring || s->len_ticket[slot] != ticket) return ACO_ERR_STATE; // never queued, or overwritten
+    const int A = c.inst[0].A;
+    if (cap < (size_t)(A + 1)) return ACO_ERR_CAPACITY;
+    if (c.set_device() != ACO_OK) return ACO_ERR_CUDA;
+    CK(cudaEventSynchronize(s->len_ev[slot]));
+    const float *src = s->len_ring + (size_t)slot * (A + 2);
+    std::memcpy(lens, src, sizeof(float) * (A + 1));
+    int status;
+    std::memcpy(&status, src + A + 1, sizeof(int));
+    return status; // the device status word when the copy was queued
 }
 
 int aco_run(aco_solver *s, float optimum, int *iterations_done)

@@ -211,6 +211,17 @@ int aco_time_iterations(aco_solver *s, int n_iter, float *ms);
 /* enqueue n_iter iterations on the solver's stream and return without waiting
  * (aco_status waits and reports); lets a caller bracket them with its own events. */
 int aco_enqueue_iterations(aco_solver *s, int n_iter);
+/* Pipelined readback of the A+1 tour lengths (ants, then best-so-far) as the
+ * stream stands after the work queued so far: aco_enqueue_lengths queues a copy
+ * into one of 4 solver-owned pinned slots and returns a ticket; aco_read_lengths
+ * waits for that copy only, writes the lengths to `lens` (cap >= A+1) and
+ * returns the device status.  A caller can queue iteration k+1 before reading
+ * iteration k, so the GPU does not idle during the host's readback (the
+ * reference reads back after every iteration, g_aco.cpp:407-417).  At most 4
+ * tickets are outstanding; an older one reads ACO_ERR_STATE.  No reference
+ * counterpart. */
+int aco_enqueue_lengths(aco_solver *s, long long *ticket);
+int aco_read_lengths(aco_solver *s, long long ticket, float *lens, size_t cap);
 /* n_iter iterations launched phase by phase with CUDA events between the
  * phases: ms[0] construct, ms[1] 2-opt, ms[2] statistics, ms[3] pheromone pass
  * (device milliseconds summed over the iterations). */

@@ -157,3 +157,25 @@ def test_batch_rejects_parity_mode_and_large_instances(gpu):
     big = mixed_problems(2, [1100])
     with pytest.raises(AcoError):
         Batch(big, batch_params(1101, 8, 1))
+
+
+def test_pipelined_length_readback(gpu):
+    # iteration k+1 is queued before the lengths of iteration k are read; every
+    # read returns exactly the lengths a synchronous read gives after that iteration
+    pr = mixed_problems(61, [150])[0]
+    A = 64
+    p = batch_params(pr.num_node, A, 5)
+    with Solver(pr, p) as S, Solver(pr, batch_params(pr.num_node, A, 5)) as R:
+        S.init(); R.init()
+        tickets = []
+        for k in range(6):
+            S.enqueue(1)
+            tickets.append(S.enqueue_lengths())
+        want = []
+        for k in range(6):
+            R.iterate(1)
+            want.append(R.solutions()[1])
+        for k, t in enumerate(tickets[-4:]):  # four slots: the newest four tickets are readable
+            assert np.array_equal(S.read_lengths(t), want[2 + k])
+        with pytest.raises(AcoError):
+            S.read_lengths(tickets[0])  # overwritten
