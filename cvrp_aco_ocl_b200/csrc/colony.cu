@@ -47,6 +47,40 @@ int ilog2(int v)
 
 size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Uploads collected into one host blob; flush() copies it to a temporary
+// device buffer in one transfer and scatters the pieces with one kernel.
+struct Staging {
+    std::vector<unsigned char> blob;
+    std::vector<ScatterPiece> pieces;
+    void add(void *dst, const void *src, size_t bytes)
+    {
+        if (bytes == 0) return;
+        const size_t off = (blob.size() + 15) & ~(size_t)15;
+        blob.resize(off + bytes);
+        std::memcpy(blob.data() + off, src, bytes);
+        pieces.push_back(ScatterPiece{(unsigned long long)(uintptr_t)dst, (unsigned long long)off,
+                                      (unsigned long long)bytes});
+    }
+    cudaError_t flush(cudaMemPool_t pool, int sm_count, cudaStream_t st)
+    {
+        if (pieces.empty()) return cudaSuccess;
+        const size_t poff = (blob.size() + 15) & ~(size_t)15;
+        blob.resize(poff + pieces.size() * sizeof(ScatterPiece));
+        std::memcpy(blob.data() + poff, pieces.data(), pieces.size() * sizeof(ScatterPiece));
+        void *d = nullptr;
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(&d, blob.size(), pool, st) : cudaMallocAsync(&d, blob.size(), st);
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpyAsync(d, blob.data(), blob.size(), cudaMemcpyHostToDevice, st); // pageable: staged on return
+        if (e == cudaSuccess)
+            e = launch_scatter(reinterpret_cast<const ScatterPiece *>(static_cast<unsigned char *>(d) + poff),
+                               (int)pieces.size(), static_cast<const unsigned char *>(d), poff, sm_count, st);
+        const cudaError_t f = cudaFreeAsync(d, st);
+        blob.clear();
+        pieces.clear();
+        return e != cudaSuccess ? e : f;
+    }
+};
+
 // Per-instance host preparation: distances, feasibility, NN lists.
 int prep_instance(const InstanceSpec &sp, const aco_params &p, InstHost &ih)
 {
@@ -539,18 +573,25 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     std::vector<UpdateArgs> uargs(count);
     const int ai = exp_as_int(p.alpha), bi = exp_as_int(p.beta);
     bool ok = true;
-    auto up = [&](void *dst, const void *src, size_t bytes) {
-        ok = ok && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
-    };
-    for (int b = 0; b < count; b++) {
+    // host -> device uploads are staged into one blob: one copy and one scatter
+    // kernel per flush instead of a pageable copy per array
+    Staging stage;
+    auto up = [&](void *dst, const void *src, size_t bytes) { stage.add(dst, src, bytes); };
+    for (int b = 0; b < count; b++) { // what the device preprocessing reads
         InstHost &ih = inst[b];
-        const int n = ih.n;
         std::vector<int> dem4(ih.n4, 0);
         std::copy(ih.demand.begin(), ih.demand.end(), dem4.begin());
         up(ih.dem_d, dem4.data(), dem4.size() * 4);
+        if (ih.device_prep) {
+            up(ih.xy_d, ih.x, (size_t)ih.n * 4);
+            up(ih.xy_d + ih.n4, ih.y, (size_t)ih.n * 4);
+        }
+    }
+    ok = ok && stage.flush(res->pool, sm_count, st) == cudaSuccess;
+    for (int b = 0; b < count; b++) {
+        InstHost &ih = inst[b];
+        const int n = ih.n;
         if (ih.device_prep) { // distances, lists and tables on the device (prep.cu)
-            up(ih.xy_d, ih.x, (size_t)n * 4);
-            up(ih.xy_d + ih.n4, ih.y, (size_t)n * 4);
             ok = ok && launch_dist(n, ih.xy_d, ih.xy_d + ih.n4, ih.dist_type, ih.dist_d, ih.ld, sm_count, st) ==
                            cudaSuccess;
             if (ih.depth > 0) {
@@ -643,6 +684,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     up(items_d_, items.data(), items.size() * sizeof(int2));
     up(sw_items_d_, swi.data(), swi.size() * sizeof(int2));
     up(ns_items_d_, nsi.data(), nsi.size() * sizeof(int2));
+    ok = ok && stage.flush(res->pool, sm_count, st) == cudaSuccess;
     if (!ok) return ACO_ERR_CUDA;
     rc = run_rows(ROW_HEUR, 0.f);
     if (rc != ACO_OK) return rc;

@@ -119,6 +119,14 @@ enum RowMode {
 
 // Launchers (stream-ordered; return cudaGetLastError()).  `d_*args` point to
 // arrays of argument blocks in device memory, one per instance.
+// Staged host -> device uploads: the pieces of one blob copied to their
+// destinations by one kernel.
+struct ScatterPiece {
+    unsigned long long dst, src_off, bytes;
+};
+cudaError_t launch_scatter(const ScatterPiece *d_pieces, int count, const unsigned char *d_blob,
+                           unsigned long long total_bytes, int sm_count, cudaStream_t st);
+
 cudaError_t launch_construct_parity(const ConstructArgs &a, int warps_per_ant, int ants_per_block, bool stage_total,
                                     cudaStream_t st);
 // Throughput construct, persistent: CTAs pull work items {instance, first ant}

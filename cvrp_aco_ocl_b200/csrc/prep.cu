@@ -9,7 +9,7 @@
 // device reproduces the host bits.  GEO goes through cos/acos, whose last bits
 // differ between math libraries; it stays on the host.
 //
-// Lists: one thread per row runs the reference's quicksort (middle pivot
+// Lists: one warp per row stages it and its first lane runs the reference's quicksort (middle pivot
 // swapped to the left end, Lomuto partition with strict <, both halves
 // recursed) on its row in shared memory.  Only positions below the list depth
 // are needed, so ranges starting at or beyond it are skipped; the ranges are
@@ -50,19 +50,9 @@ __global__ void dist_kernel(int n, const float *x, const float *y, int type, flo
 
 constexpr int kStack = 40;
 
-__global__ void nn_kernel(int n, const float *dist, int ld, int depth, int rows_per_cta, int *nn, int *status)
+// The reference's quicksort (utilities.cpp:246-266) on one row, stopping below `depth`.
+__device__ void sort_row(float *v, int *idx, int n, int depth, int *status)
 {
-    extern __shared__ __align__(16) unsigned char sm[];
-    const int row = blockIdx.x * rows_per_cta + threadIdx.x;
-    if (threadIdx.x >= rows_per_cta || row >= n) return;
-    float *v = reinterpret_cast<float *>(sm) + (size_t)threadIdx.x * 2 * n;
-    int *idx = reinterpret_cast<int *>(v + n);
-    for (int i = 0; i < n; i++) {
-        v[i] = dist[(size_t)row * ld + i];
-        idx[i] = i;
-    }
-    v[row] = __int_as_float(0x7f800000); // the node itself and the depot never make the list
-    v[0] = __int_as_float(0x7f800000);
     int sl[kStack], sr[kStack], top = 0;
     sl[0] = 0;
     sr[0] = n - 1;
@@ -98,8 +88,32 @@ __global__ void nn_kernel(int n, const float *dist, int ld, int depth, int rows_
             sl[top] = last + 1; sr[top] = r; top++;
         }
     }
-    for (int i = 0; i < depth; i++) nn[(size_t)row * depth + i] = idx[i];
 }
+
+// One warp per row: the lanes stage the row, lane 0 runs the sort alone (no
+// divergence between rows sorted by the same warp), the lanes write the list.
+__global__ void nn_kernel(int n, const float *dist, int ld, int depth, int rows_per_cta, int *nn, int *status)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row = blockIdx.x * rows_per_cta + w;
+    if (w >= rows_per_cta || row >= n) return;
+    float *v = reinterpret_cast<float *>(sm) + (size_t)w * 2 * n;
+    int *idx = reinterpret_cast<int *>(v + n);
+    for (int i = lane; i < n; i += 32) {
+        v[i] = dist[(size_t)row * ld + i];
+        idx[i] = i;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        v[row] = __int_as_float(0x7f800000); // the node itself and the depot never make the list
+        v[0] = __int_as_float(0x7f800000);
+        sort_row(v, idx, n, depth, status);
+    }
+    __syncwarp();
+    for (int i = lane; i < depth; i += 32) nn[(size_t)row * depth + i] = idx[i];
+}
+
 
 // Candidate and 2-opt tables from the lists: nn16 / cand32 (first K, padded
 // with node 0 to Kp) and the 2-opt list (first nn_ls).
@@ -141,12 +155,48 @@ cudaError_t launch_dist(int n, const float *x, const float *y, int dist_type, fl
 
 cudaError_t launch_nn(int n, const float *dist, int ld, int depth, int *nn, int *status, cudaStream_t st)
 {
-    const int rows = (int)nn_rows_per_cta(n);
+    int rows = (int)nn_rows_per_cta(n);
     if (rows < 1) return cudaErrorInvalidValue;
+    if (rows > 8) rows = 8; // warps (rows) per CTA
     const size_t smem = (size_t)rows * 8 * n;
     cudaError_t e = cudaFuncSetAttribute(nn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    nn_kernel<<<(n + rows - 1) / rows, 32, smem, st>>>(n, dist, ld, depth, rows, nn, status);
+    nn_kernel<<<(n + rows - 1) / rows, 32 * rows, smem, st>>>(n, dist, ld, depth, rows, nn, status);
+    return cudaGetLastError();
+}
+
+// Scatter of staged uploads: piece k copies bytes [src_off, src_off + bytes)
+// of the blob to dst.  The whole grid works on one piece after another, so a
+// large piece (the seeds) spreads over every CTA.
+__global__ void scatter_kernel(const ScatterPiece *pieces, int count, const unsigned char *blob)
+{
+    const unsigned long long t0 = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (int k = 0; k < count; k++) {
+        const ScatterPiece pc = pieces[k];
+        unsigned char *dst = reinterpret_cast<unsigned char *>(pc.dst);
+        const unsigned char *src = blob + pc.src_off;
+        const unsigned long long b = pc.bytes;
+        if (((pc.dst | pc.src_off | b) & 15ull) == 0) {
+            for (unsigned long long i = t0; i < b / 16; i += stride)
+                reinterpret_cast<uint4 *>(dst)[i] = reinterpret_cast<const uint4 *>(src)[i];
+        } else if (((pc.dst | pc.src_off | b) & 3ull) == 0) {
+            for (unsigned long long i = t0; i < b / 4; i += stride)
+                reinterpret_cast<uint32_t *>(dst)[i] = reinterpret_cast<const uint32_t *>(src)[i];
+        } else {
+            for (unsigned long long i = t0; i < b; i += stride) dst[i] = src[i];
+        }
+    }
+}
+
+cudaError_t launch_scatter(const ScatterPiece *d_pieces, int count, const unsigned char *d_blob,
+                           unsigned long long total_bytes, int sm_count, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    unsigned long long blocks = (total_bytes / 16 + 255) / 256;
+    if (blocks > (unsigned long long)sm_count * 4) blocks = (unsigned long long)sm_count * 4;
+    if (blocks < 1) blocks = 1;
+    scatter_kernel<<<(unsigned)blocks, 256, 0, st>>>(d_pieces, count, d_blob);
     return cudaGetLastError();
 }
 
