@@ -263,43 +263,52 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
     }
     __syncthreads();
 
-    // local_search (kernel.cl:517-523) + two_opt_solution set-up (:293-300), per ant
+    // local_search (kernel.cl:517-523) + two_opt_solution set-up (:293-300): the
+    // tours are staged by the whole CTA, then warp j makes one pass over ant j's:
+    // node positions, depot positions (route table) and every customer's route id
+    // and index inside its route, from one ballot per 32 positions.  Edge lengths
+    // (dist_tour_wrk) are filled per route: by the register path from its tile,
+    // by the others from the matrix.
     for (int j = 0; j < apc; j++) {
         if (s_inst[j] < 0) continue;
         const LocalSearchArgs &a = args[s_inst[j]];
         const int *gtour = a.solutions + (size_t)s_ant[j] * a.T;
         uint16_t *tour = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.tour));
-        uint16_t *pos = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.pos));
         uint8_t *dlb = ant_ptr(j, AL.dlb);
-        for (int p = threadIdx.x; p < s_size[j]; p += blockDim.x) {
-            const int v = gtour[p];
-            tour[p] = (uint16_t)v;
-            if (v != 0) pos[v] = (uint16_t)p;
-        }
+        for (int p = threadIdx.x; p < s_size[j]; p += blockDim.x) tour[p] = (uint16_t)gtour[p];
         for (int v = threadIdx.x; v < a.n; v += blockDim.x) dlb[v] = 0;
     }
     __syncthreads();
-    for (int j = 0; j < apc; j++) {
-        if (s_inst[j] < 0) continue;
-        const LocalSearchArgs &a = args[s_inst[j]];
-        const uint16_t *tour = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.tour));
-        float *dt = reinterpret_cast<float *>(ant_ptr(j, AL.dt));
-        for (int p = threadIdx.x; p < s_size[j] - 1; p += blockDim.x)
-            dt[p] = __ldg(a.dist + (size_t)tour[p] * a.ld + tour[p + 1]);
-    }
-    if (warp < apc) { // route table of ant `warp`: depot positions in order
+    if (warp < apc) {
         const int j = warp;
         int count = 0;
         if (s_inst[j] >= 0) {
             const uint16_t *tour = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.tour));
+            uint16_t *pos = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.pos));
             uint16_t *rstart = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.rstart));
+            uint16_t *rid = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.rid));
+            uint8_t *li = ant_ptr(j, AL.li);
             const int size = s_size[j];
+            int last = 0; // position of the last depot before this chunk
             for (int base = 0; base < size; base += 32) {
                 const int p = base + lane;
-                const bool dep = p < size && tour[p] == 0;
+                const int v = p < size ? (int)tour[p] : -1;
+                const bool dep = v == 0;
                 const unsigned m = __ballot_sync(FULL, dep);
-                if (dep) rstart[count + __popc(m & ((1u << lane) - 1u))] = (uint16_t)p;
+                const unsigned lt = m & ((1u << lane) - 1u);
+                if (p < size) {
+                    if (dep) {
+                        rstart[count + __popc(lt)] = (uint16_t)p;
+                    } else {
+                        const int r = count + __popc(lt) - 1;     // depots before p, less the first
+                        const int rb = lt ? base + 31 - __clz(lt) : last; // the depot opening p's route
+                        pos[v] = (uint16_t)p;
+                        rid[v] = (uint16_t)r;
+                        li[v] = (uint8_t)(p - rb < 256 ? p - rb : 0);
+                    }
+                }
                 count += __popc(m);
+                if (m) last = base + 31 - __clz(m);
             }
             count -= 1;
         }
@@ -323,19 +332,6 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
         while (j + 1 < apc && s_routes[j + 1] <= f) j++;
         r = f - s_routes[j];
     };
-    for (int f = warp; f < total_routes; f += W) { // route id and local index of every customer
-        int j, r;
-        locate(f, j, r);
-        const uint16_t *tour = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.tour));
-        const uint16_t *rstart = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.rstart));
-        uint16_t *rid = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.rid));
-        uint8_t *li = ant_ptr(j, AL.li);
-        for (int p = rstart[r] + 1 + lane; p < rstart[r + 1]; p += 32) {
-            rid[tour[p]] = (uint16_t)r;
-            li[tour[p]] = (uint8_t)(p - rstart[r] < 256 ? p - rstart[r] : 0);
-        }
-    }
-    __syncthreads();
 
     int status = ACO_OK, status_inst = 0;
     for (int f = warp; f < total_routes;) {
@@ -353,7 +349,9 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
         int st = ACO_OK;
         if (R <= kRL && s_only[j] == 1) {
             // routes of at most 32 nodes improved already (fused construct or
-            // route-level kernel); only the longer ones of this ant are left here
+            // route-level kernel); only the longer ones of this ant are left
+            // here.  Their edge lengths still enter the tour length.
+            for (int p = rb + lane; p <= re; p += 32) dt[p] = __ldg(a.dist + (size_t)tour[p] * a.ld + tour[p + 1]);
         } else if (R <= kRL) {
             // route-local state: the distance tile (row k1 = distances from route
             // node k1, lane k2 its column) and every route node's neighbour list
@@ -399,7 +397,8 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
             __syncwarp();
             int tq = lane < R ? lane : 0;
             int pk = lane < R ? lane : 0;
-            float dq = lane < R ? dt[rb + lane] : 0.f;
+            // edge lengths: position q -> q+1, the last one back to the next depot (node 0 = local 0)
+            float dq = lane < R ? tile[lane * kRL + (lane + 1 < R ? lane + 1 : 0)] : 0.f;
             st = two_opt_route_regs(lane, R, r == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
             const int node = __shfl_sync(FULL, v, tq);
             if (lane < R) {
@@ -408,6 +407,8 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
             }
             __syncwarp();
         } else {
+            for (int p = rb + lane; p <= re; p += 32) dt[p] = __ldg(a.dist + (size_t)tour[p] * a.ld + tour[p + 1]);
+            __syncwarp();
             Route c;
             c.tour = tour; c.pos = pos; c.rid = rid; c.dlb = dlb; c.dt = dt;
             c.dist = a.dist; c.nn = a.nn_list; c.ld = a.ld; c.nn_ls = a.nn_ls; c.lane = lane;
