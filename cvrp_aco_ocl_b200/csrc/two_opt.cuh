@@ -40,6 +40,18 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
     // search finds no move, as in the sequential code.
     const unsigned FULLM = 0xffffffffu;
     const unsigned rmask = R >= 32 ? FULLM : ((1u << R) - 1u);
+    // lane k, by local node: the nodes after and before it on the tour, and the
+    // dist_tour_wrk entries at its position and the one before (position 0: its
+    // own), rebuilt after every move
+    int nsucc, npred;
+    float dout, din;
+    auto by_node = [&]() {
+        nsucc = __shfl_sync(FULLM, tq, pk + 1 < R ? pk + 1 : 0);
+        npred = __shfl_sync(FULLM, tq, pk > 0 ? pk - 1 : R - 1);
+        dout = __shfl_sync(FULLM, dq, pk);
+        din = __shfl_sync(FULLM, dq, pk > 0 ? pk - 1 : 0);
+    };
+    by_node();
     uint32_t dlb = first_route ? 0u : 1u; // bit k: don't-look bit of local node k
     int passes = 0;
     bool imp = true;
@@ -64,11 +76,11 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
             const float d12 = tile[k1 * kRL + k2];
             const float rs = tile[k1 * kRL + ks1];  // successor radius
             const float rp = tile[kp1 * kRL + k1];  // predecessor radius
-            const int q2 = __shfl_sync(FULLM, pk, k2);
-            const int ks2 = __shfl_sync(FULLM, tq, q2 + 1 < R ? q2 + 1 : 0);
-            const int kpp2 = __shfl_sync(FULLM, tq, q2 > 0 ? q2 - 1 : R - 1);
-            const float dq2 = __shfl_sync(FULLM, dq, q2);
-            const float dqp2 = __shfl_sync(FULLM, dq, q2 > 0 ? q2 - 1 : 0);
+            // k2's neighbours on the tour and edge lengths, one shuffle level from k2
+            const int ks2 = __shfl_sync(FULLM, nsucc, k2);
+            const int kpp2 = __shfl_sync(FULLM, npred, k2);
+            const float dq2 = __shfl_sync(FULLM, dout, k2);
+            const float dqp2 = __shfl_sync(FULLM, din, k2);
             const bool sc = act && __fsub_rn(rs, d12) > kEps;
             const bool pc = act && __fsub_rn(rp, d12) > kEps;
             bool sok = false, pok = false;
@@ -80,11 +92,14 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
                 const float g = __fsub_rn(__fadd_rn(__fadd_rn(-rp, d12), tile[kp1 * kRL + kpp2]), dqp2);
                 pok = g < -kEps;
             }
+            // the scan stops at the first lane whose entry ends it: past the radius, or
+            // an improving move (kernel.cl:180-198, 202-230); found = that lane moves
             const unsigned sstop = __ballot_sync(FULLM, act && (!sc || sok));
             const unsigned pstop = __ballot_sync(FULLM, act && (!pc || pok));
+            const unsigned smove = __ballot_sync(FULLM, sok), pmove = __ballot_sync(FULLM, pok);
             const int sf = sstop ? __ffs(sstop) - 1 : 0, pf = pstop ? __ffs(pstop) - 1 : 0;
-            const bool sfound = sstop && __shfl_sync(FULLM, (int)sc, sf);
-            const bool pfound = pstop && __shfl_sync(FULLM, (int)pc, pf);
+            const bool sfound = (sstop & (0u - sstop) & smove) != 0u; // the lowest stop is a move
+            const bool pfound = (pstop & (0u - pstop) & pmove) != 0u;
             int h1, h2, h3, h4;
             if (sfound) {
                 h1 = k1;
@@ -121,6 +136,7 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
             const int tsrc = __shfl_sync(FULLM, tq, (lane >= a && lane <= jj) ? a + jj - lane : lane);
             if (lane >= a && lane <= jj) tq = tsrc;
             if (pk >= a && pk <= jj) pk = a + jj - pk;
+            by_node();
             open = __ballot_sync(FULLM, lane < R && !((dlb >> tq) & 1u)) & rmask; // the tour and bits changed
         }
     }
