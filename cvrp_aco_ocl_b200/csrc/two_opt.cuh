@@ -55,27 +55,40 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
     uint32_t dlb = first_route ? 0u : 1u; // bit k: don't-look bit of local node k
     int passes = 0;
     bool imp = true;
+    // the first half of an examination: node k1 at position q, its tour
+    // neighbours, its filtered list entry for this lane and the radii.  It
+    // depends only on q and the tour, so the next open position's is loaded
+    // while the current examination's ballots resolve (used when no move
+    // happens, which is the common case; recomputed after a move).
+    struct Head {
+        int k1, ks1, kp1, k2;
+        bool act;
+        float d12, rs, rp;
+    };
+    auto head = [&](int q) {
+        Head h;
+        h.k1 = __shfl_sync(FULLM, tq, q);
+        h.ks1 = __shfl_sync(FULLM, tq, q + 1 < R ? q + 1 : 0);
+        h.kp1 = __shfl_sync(FULLM, tq, q > 0 ? q - 1 : R - 1);
+        h.act = lane < (int)lcnt[h.k1];
+        h.k2 = h.act ? lnn[h.k1 * kRL + lane] : 0;
+        h.d12 = tile[h.k1 * kRL + h.k2];
+        h.rs = tile[h.k1 * kRL + h.ks1]; // successor radius
+        h.rp = tile[h.kp1 * kRL + h.k1]; // predecessor radius
+        return h;
+    };
     while (imp) {
         if (pass_limit > 0 && passes >= pass_limit) return ACO_ERR_LS_LIMIT;
         passes++;
         imp = false;
         uint32_t open = __ballot_sync(FULLM, lane < R && !((dlb >> tq) & 1u)) & rmask;
-        int q1 = -1;
+        if (!open) break;
+        int q1 = __ffs(open) - 1;
+        Head h = head(q1);
         for (;;) {
-            const uint32_t ahead = q1 < 0 ? open : (q1 >= 31 ? 0u : (open & ~((2u << q1) - 1u))); // positions > q1
-            if (!ahead) break;
-            q1 = __ffs(ahead) - 1;
-            // every shuffle below is independent of the others at its level
-            const int k1 = __shfl_sync(FULLM, tq, q1);
-            const int ks1 = __shfl_sync(FULLM, tq, q1 + 1 < R ? q1 + 1 : 0);
-            const int kp1 = __shfl_sync(FULLM, tq, q1 > 0 ? q1 - 1 : R - 1);
-            const int cnt = lcnt[k1];
-            const int j = lane;
-            const bool act = j < cnt;
-            const int k2 = act ? lnn[k1 * kRL + j] : 0;
-            const float d12 = tile[k1 * kRL + k2];
-            const float rs = tile[k1 * kRL + ks1];  // successor radius
-            const float rp = tile[kp1 * kRL + k1];  // predecessor radius
+            const int k1 = h.k1, ks1 = h.ks1, kp1 = h.kp1, k2 = h.k2;
+            const bool act = h.act;
+            const float d12 = h.d12, rs = h.rs, rp = h.rp;
             // k2's neighbours on the tour and edge lengths, one shuffle level from k2
             const int ks2 = __shfl_sync(FULLM, nsucc, k2);
             const int kpp2 = __shfl_sync(FULLM, npred, k2);
@@ -97,6 +110,10 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
             const unsigned sstop = __ballot_sync(FULLM, act && (!sc || sok));
             const unsigned pstop = __ballot_sync(FULLM, act && (!pc || pok));
             const unsigned smove = __ballot_sync(FULLM, sok), pmove = __ballot_sync(FULLM, pok);
+            // the next open position if this examination makes no move, and its head
+            const uint32_t rest = q1 >= 31 ? 0u : (open & ~((2u << q1) - 1u)); // positions > q1
+            const int qn = rest ? __ffs(rest) - 1 : 0;
+            const Head hn = head(qn);
             const int sf = sstop ? __ffs(sstop) - 1 : 0, pf = pstop ? __ffs(pstop) - 1 : 0;
             const bool sfound = (sstop & (0u - sstop) & smove) != 0u; // the lowest stop is a move
             const bool pfound = (pstop & (0u - pstop) & pmove) != 0u;
@@ -114,6 +131,9 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
             } else {
                 dlb |= 1u << k1; // kernel.cl:232
                 open &= ~(1u << q1);
+                if (!rest) break;
+                q1 = qn;
+                h = hn;
                 continue;
             }
             // exchange (kernel.cl:235-270)
@@ -138,6 +158,10 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
             if (pk >= a && pk <= jj) pk = a + jj - pk;
             by_node();
             open = __ballot_sync(FULLM, lane < R && !((dlb >> tq) & 1u)) & rmask; // the tour and bits changed
+            const uint32_t ahead = q1 >= 31 ? 0u : (open & ~((2u << q1) - 1u)); // the scan goes on after q1
+            if (!ahead) break;
+            q1 = __ffs(ahead) - 1;
+            h = head(q1);
         }
     }
     return ACO_OK;
