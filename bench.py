@@ -331,8 +331,8 @@ def run_batched(args, ws, rank, local, peak, peak_kind):
 
 
 def run_e2e(args, rank, local):
-    """aco_create from host arrays (coordinates, demands and seeds copied
-    host->device; distances and NN lists computed there), aco_init, then per
+    """aco_create from host arrays (coordinates and demands copied host->device;
+    distances, NN lists and seeds computed there), aco_init, then per
     step one iteration and a device->host read of its ant and best-so-far
     lengths (pipelined: iteration k is queued before iteration k-1's lengths
     are read), then the best tour read back: the reference's main.cpp loop
@@ -370,8 +370,9 @@ def run_e2e(args, rank, local):
     t1 = time.perf_counter()
     S.close()
     n = inst.n
-    # coordinates and demands, seeds (distances and lists are computed on the device from the coordinates)
-    h2d = n * 4 * 3 + ANTS * NLOC * 4
+    # coordinates and demands, per-ant index tables and work items, argument blocks (about 1 KB); distances,
+    # lists and the ants' seeds are computed on the device
+    h2d = n * 4 * 3 + ANTS * 4 * 3 + 1024
     d2h = (ANTS + 1) * 4 + 4  # lengths and the status word
     return {"value": ANTS * args.steps / (t1 - t0), "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h + (2 * n * 4 + 4) / args.steps,

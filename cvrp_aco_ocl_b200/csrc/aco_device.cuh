@@ -28,6 +28,17 @@ __device__ __forceinline__ uint32_t pm_mul(uint32_t a, uint32_t b)
     return r >= kPM ? r - kPM : r;
 }
 
+// 16807^e mod (2^31 - 1): the jump of a Park-Miller state over e draws.
+__device__ __forceinline__ uint32_t pm_pow16807(long long e)
+{
+    uint32_t r = 1u, b = 16807u;
+    for (; e > 0; e >>= 1) {
+        if (e & 1) r = pm_mul(r, b);
+        b = pm_mul(b, b);
+    }
+    return r;
+}
+
 // ran01's return value for a state x already advanced (kernel.cl:50).  AM = 2^-31.
 __device__ __forceinline__ float pm_uniform(uint32_t x)
 {

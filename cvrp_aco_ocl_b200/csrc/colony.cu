@@ -634,10 +634,8 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
                 for (int j = 0; j < ih.nn_ls; j++) nnls[(size_t)i * ih.nn_ls + j] = ih.nn[(size_t)i * ih.depth + j];
             up(ih.nnls_d, nnls.data(), nnls.size() * 4);
         }
-        std::vector<int> seeds((size_t)ih.A * ih.nloc);
-        int rs = p.rnd_seed + b; // instance b of a batch: rnd_seed + b
-        make_seeds(p.seed_time, &rs, ih.A, ih.nloc, seeds.data());
-        up(ih.seeds_d, seeds.data(), seeds.size() * 4);
+        // instance b of a batch: rnd_seed + b
+        ok = ok && launch_seeds(p.seed_time, p.rnd_seed + b, ih.A, ih.nloc, ih.seeds_d, sm_count, st) == cudaSuccess;
 
         ConstructArgs &c = cargs_h_[b];
         c = ConstructArgs{};

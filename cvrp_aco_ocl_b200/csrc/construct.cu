@@ -396,17 +396,6 @@ __device__ void fused_ls_warp(const ConstructArgs &a, unsigned char *smem, const
 // Barrier `id` shared by exactly two warps (an ant's warp and its helper).
 __device__ __forceinline__ void pair_barrier(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
 
-// 16807^e mod (2^31 - 1): the jump of a Park-Miller state over e draws.
-__device__ __forceinline__ uint32_t pm_pow16807(int e)
-{
-    uint32_t r = 1u, b = 16807u;
-    for (; e > 0; e >>= 1) {
-        if (e & 1) r = pm_mul(r, b);
-        b = pm_mul(b, b);
-    }
-    return r;
-}
-
 // Helper warp of one ant: the race rates of chunk c go to ring half c & 1; at
 // hand-over c both warps meet at the pair barrier, after which the ant's warp
 // has set flag[c & 1] (1 = the ant is done, 0 = continue).  The ant's warp

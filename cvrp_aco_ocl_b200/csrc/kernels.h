@@ -121,6 +121,9 @@ enum RowMode {
 // arrays of argument blocks in device memory, one per instance.
 // Staged host -> device uploads: the pieces of one blob copied to their
 // destinations by one kernel.
+// The ants' lane seeds on the device (same values as make_seeds on the host).
+cudaError_t launch_seeds(int seed_time, int rnd_seed, int n_ants, int nloc, int *seeds, int sm_count, cudaStream_t st);
+
 struct ScatterPiece {
     unsigned long long dst, src_off, bytes;
 };

@@ -21,6 +21,7 @@
 #include <cstdint>
 
 #include "../../include/cvrp_aco.h"
+#include "aco_device.cuh"
 #include "kernels.h"
 
 namespace aco {
@@ -162,6 +163,35 @@ cudaError_t launch_nn(int n, const float *dist, int ld, int depth, int *nn, int 
     cudaError_t e = cudaFuncSetAttribute(nn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     nn_kernel<<<(n + rows - 1) / rows, 32 * rows, smem, st>>>(n, dist, ld, depth, rows, nn, status);
+    return cudaGetLastError();
+}
+
+// The ants' lane seeds (g_aco.cpp:714-722): seed i = (int)(T0 + m (m + r_i) A)
+// with m = i mod A and r_i the (i+1)-th ran01 draw from rnd_seed, in fp32 as
+// written and converted as x86 cvttss2si does (NaN and out-of-range values give
+// INT_MIN).  Draw i+1 is x0 * 16807^(i+1) mod (2^31 - 1), so every seed is
+// computed independently.
+__global__ void seeds_kernel(int seed_time, uint32_t x0, int n_ants, long long total, int *seeds)
+{
+    const float t0 = (float)seed_time, a = (float)n_ants;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float m = (float)(int)(i % n_ants);
+        const float r = pm_uniform(pm_mul(x0, pm_pow16807(i + 1)));
+        const float v = __fadd_rn(t0, __fmul_rn(__fmul_rn(m, __fadd_rn(m, r)), a));
+        seeds[i] = (v >= -2147483648.0f && v < 2147483648.0f) ? __float2int_rz(v) : (int)0x80000000;
+    }
+}
+
+cudaError_t launch_seeds(int seed_time, int rnd_seed, int n_ants, int nloc, int *seeds, int sm_count, cudaStream_t st)
+{
+    long long r = (long long)rnd_seed % 2147483647ll;
+    if (r < 0) r += 2147483647ll;
+    const long long total = (long long)n_ants * nloc;
+    long long blocks = (total + 255) / 256;
+    if (blocks > sm_count * 8) blocks = sm_count * 8;
+    if (blocks < 1) blocks = 1;
+    seeds_kernel<<<(unsigned)blocks, 256, 0, st>>>(seed_time, (uint32_t)r, n_ants, total, seeds);
     return cudaGetLastError();
 }
 
