@@ -672,6 +672,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     up(cargs_d_, cargs_h_.data(), sizeof(ConstructArgs) * count);
     up(largs_d_, largs.data(), sizeof(LocalSearchArgs) * count);
     up(sargs_d_, sargs.data(), sizeof(StatsArgs) * count);
+    stats_one_ = sargs[0];
     up(uargs_d_, uargs.data(), sizeof(UpdateArgs) * count);
     up(ant_inst_d_, ant_inst.data(), ant_inst.size() * 4);
     up(ant_base_d_, ant_base.data(), ant_base.size() * 4);
@@ -923,7 +924,7 @@ int Colony::neighbourhood()
 
 int Colony::stats(bool elites)
 {
-    CK(launch_stats(sargs_d_, (int)inst.size(), elites ? 1 : 0, stats_smem, st));
+    CK(launch_stats(sargs_d_, (int)inst.size(), elites ? 1 : 0, stats_smem, st, inst.size() == 1 ? &stats_one_ : nullptr));
     return ACO_OK;
 }
 

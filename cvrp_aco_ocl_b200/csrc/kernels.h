@@ -156,7 +156,9 @@ cudaError_t launch_route_opt(const LocalSearchArgs *d_args, const int *d_ant_ins
 cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
                                 int total_ants, int ants_per_cta, int n_max, int warps, size_t smem, cudaStream_t st,
                                 const uint8_t *only = nullptr);
-cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st);
+// one: a single instance's arguments passed by value (d_args unused)
+cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st,
+                         const StatsArgs *one = nullptr);
 // Row passes (heuristic matrix, pheromone init, fused update, candidate gather):
 // one warp per row over all instances; d_row_base[b] = first global row of instance b.
 cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, int n_inst, int total_rows, int mode,

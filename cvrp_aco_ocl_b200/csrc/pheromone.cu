@@ -46,15 +46,26 @@ __device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v
     return v; // every thread holds the block minimum
 }
 
-__global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, int do_elites)
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(FULL, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+// args: one block per instance (batches); null: the single instance `one`,
+// passed by value so that its fields need no global load.
+__global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, StatsArgs one, int do_elites)
 {
     extern __shared__ float s_len[]; // lens[0..A) of this iteration
-    __shared__ unsigned long long red[32];
-    __shared__ int s_best, s_flag, s_elite[32], s_size[32];
-    __shared__ int s_rank[1024]; // keys below each entry (get_elites, one pass)
+    __shared__ unsigned long long red[32], s_wmin[32], s_thr;
+    __shared__ int s_best, s_flag, s_elite[32], s_size[32], s_ncand;
+    __shared__ unsigned long long s_cand[1024]; // get_elites candidates (keys at most the threshold)
     __shared__ float s_minval, s_bsf;
     __shared__ const int *s_tour[32];
-    const StatsArgs a = args[blockIdx.x];
+    const StatsArgs a = args ? args[blockIdx.x] : one;
     const int A = a.n_ants, T = a.T, tid = threadIdx.x, bs = blockDim.x, R = a.ras_ranks;
     const int lg = a.log2_nloc;
     // every global value the kernel needs is loaded up front, in parallel
@@ -95,29 +106,35 @@ __global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, int 
     // one pass of the block, each entry's rank is the number of keys below its
     // own, and the first R-1 finite ranks place themselves.
     if (do_elites && A <= bs) {
-        // P threads per entry, each counting the keys below it in one slice of the entries
-        const int P = A > 0 ? (bs / A < 8 ? bs / A : 8) : 1;
-        const int slice = (A + P - 1) / P;
-        for (int k = tid; k < A; k += bs) s_rank[k] = 0;
-        __syncthreads();
-        if (tid < A * P) {
-            const int k = tid / P, j0 = (tid - k * P) * slice;
-            const int j1 = j0 + slice < A ? j0 + slice : A;
-            const uint32_t bk = __float_as_uint(s_len[k]);
-            int c = 0;
-            for (int jb = j0; jb < j1; jb += 8) { // eight keys a round, loads first
-                uint32_t bj[8];
-#pragma unroll
-                for (int u = 0; u < 8; u++) bj[u] = jb + u < j1 ? __float_as_uint(s_len[jb + u]) : 0xffffffffu;
-#pragma unroll
-                for (int u = 0; u < 8; u++) c += (bj[u] < bk || (bj[u] == bk && jb + u < k)) ? 1 : 0;
-            }
-            if (c) atomicAdd(&s_rank[k], c);
+        // keys (length bits, index) are unique.  Threshold t: the (R-1)-th
+        // smallest of the warps' minima (at least R-1 keys are at most t, so the
+        // R-1 smallest all are); only keys up to t are ranked, among themselves.
+        const int warp = tid >> 5, lane = tid & 31, nw = (A + 31) >> 5;
+        const unsigned long long key =
+            tid < A ? ((unsigned long long)__float_as_uint(s_len[tid]) << 32) | (unsigned)tid : ~0ull;
+        const unsigned long long wm = warp_min_u64(key);
+        if (lane == 0 && warp < nw) s_wmin[warp] = wm;
+        if (tid == 0) {
+            s_ncand = 0;
+            s_thr = ~0ull;
         }
-        int fin = 0;
-        if (tid < A) fin = __float_as_uint(s_len[tid]) < 0x7f800000u;
-        const int nfin = __syncthreads_count(fin);
-        if (fin && s_rank[tid] < R - 1) s_elite[1 + s_rank[tid]] = tid;
+        __syncthreads();
+        if (warp == 0 && lane < nw && nw >= R - 1 && R > 1) { // lane i ranks warp minimum i
+            const unsigned long long mi = s_wmin[lane];
+            int below = 0;
+            for (int q = 0; q < nw; q++) below += s_wmin[q] < mi;
+            if (below == R - 2) s_thr = mi;
+        }
+        __syncthreads();
+        if (tid < A && key <= s_thr) s_cand[atomicAdd(&s_ncand, 1)] = key;
+        const int nfin = __syncthreads_count(tid < A && __float_as_uint(s_len[tid]) < 0x7f800000u);
+        const int nc = s_ncand;
+        if (tid < nc) {
+            const unsigned long long own = s_cand[tid];
+            int rk = 0;
+            for (int j = 0; j < nc; j++) rk += s_cand[j] < own;
+            if ((unsigned)(own >> 32) < 0x7f800000u && rk < R - 1) s_elite[1 + rk] = (int)(own & 0xffffffffu);
+        }
         if (tid >= 1 + nfin && tid < R) s_elite[tid] = 0;
     }
     __syncthreads();
@@ -166,7 +183,7 @@ __global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, int 
             const int e = s_elite[tid];
             a.elites[tid] = e;
             const int src = (tid == 0 && flag) ? s_best : e;
-            const float len = tid == 0 ? (flag ? s_minval : s_bsf) : a.lens[e];
+            const float len = tid == 0 ? (flag ? s_minval : s_bsf) : (A <= bs ? s_len[e] : a.lens[e]);
             a.d_tau[tid] = __fdiv_rn((float)(R - tid), len);
             const int *tour = a.solutions + (size_t)T * src;
             s_tour[tid] = tour;
@@ -435,7 +452,8 @@ __global__ void t0_kernel(unsigned long long *t0) { *t0 = globaltimer_ns(); }
 
 } // namespace
 
-cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st)
+cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st,
+                         const StatsArgs *one)
 {
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -446,7 +464,7 @@ cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, siz
     cudaError_t e = cudaFuncSetAttribute(stats_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    stats_kernel<<<n_inst, 1024, smem, st>>>(d_args, do_elites);
+    stats_kernel<<<n_inst, 1024, smem, st>>>(one ? nullptr : d_args, one ? *one : StatsArgs{}, do_elites);
     return cudaGetLastError();
 }
 
