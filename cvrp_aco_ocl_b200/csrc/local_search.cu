@@ -66,6 +66,7 @@ __host__ __device__ inline LsAnt ls_ant_layout(int n)
 constexpr size_t kLsWarp = kRL * kRL * 4 + kRL * kRL + kRL;
 constexpr int kLsRows = 8; // tile rows loaded per round
 constexpr int kMaxLsAnts = 8;
+constexpr int kLsOrder = 128; // routes of a CTA ordered longest first when at most this many
 constexpr unsigned FULL = 0xffffffffu;
 
 __host__ __device__ inline size_t ls_smem_bytes(int n_max, int apc, int warps)
@@ -235,6 +236,7 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_inst[kMaxLsAnts], s_ant[kMaxLsAnts], s_size[kMaxLsAnts], s_routes[kMaxLsAnts + 1];
     __shared__ int s_only[kMaxLsAnts]; // 1: the short routes of this ant are done already
+    __shared__ uint16_t s_order[kLsOrder], s_rlen[kLsOrder]; // routes, longest first
     __shared__ int s_next;
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -332,11 +334,35 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
         while (j + 1 < apc && s_routes[j + 1] <= f) j++;
         r = f - s_routes[j];
     };
+    // Longest routes first: the warps take routes in this order, so a warp that
+    // finishes early picks up a short one and the CTA ends with its longest
+    // route rather than with a second route behind it (results do not depend on
+    // the order: routes are independent).
+    const bool ordered = total_routes <= kLsOrder && total_routes <= (int)blockDim.x;
+    if (ordered) {
+        if (threadIdx.x < total_routes) {
+            int j, r;
+            locate(threadIdx.x, j, r);
+            const uint16_t *rstart = reinterpret_cast<const uint16_t *>(ant_ptr(j, AL.rstart));
+            s_rlen[threadIdx.x] = (uint16_t)(rstart[r + 1] - rstart[r]);
+        }
+        __syncthreads();
+        if (threadIdx.x < total_routes) {
+            const int f = threadIdx.x, lf = s_rlen[f];
+            int rank = 0;
+            for (int g = 0; g < total_routes; g++) {
+                const int lg = s_rlen[g];
+                rank += lg > lf || (lg == lf && g < f);
+            }
+            s_order[rank] = (uint16_t)f;
+        }
+        __syncthreads();
+    }
 
     int status = ACO_OK, status_inst = 0;
     for (int f = warp; f < total_routes;) {
         int j, r;
-        locate(f, j, r);
+        locate(ordered ? (int)s_order[f] : f, j, r);
         const LocalSearchArgs a = args[s_inst[j]];
         uint16_t *tour = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.tour));
         uint16_t *pos = reinterpret_cast<uint16_t *>(ant_ptr(j, AL.pos));
