@@ -59,7 +59,8 @@ def test_invalid_params_rejected_before_device():
     prob = Problem.from_instance(inst)
     from cvrp_aco_ocl_b200 import Solver
     for field, val in [("nloc", 48), ("nloc", 2048), ("ras_ranks", 0), ("ras_ranks", 33), ("nn_ls", 10),
-                       ("warps_per_ant", 3), ("rho", 0.0)]:
+                       ("warps_per_ant", 3), ("rho", 0.0), ("ls_ants", 9), ("ls_ants", -1), ("draw_warps", 2),
+                       ("draw_warps", -2), ("route_ls", 2), ("fuse_ls", 2), ("ls_flag", 2), ("ns_rounds", -1)]:
         p = default_params(inst.n)
         setattr(p, field, val)
         with pytest.raises(AcoError) as ei:
