@@ -400,16 +400,22 @@ __device__ __forceinline__ void pair_barrier(int id) { asm volatile("bar.sync %0
 // hand-over c both warps meet at the pair barrier, after which the ant's warp
 // has set flag[c & 1] (1 = the ant is done, 0 = continue).  The ant's warp
 // reads flag-free: it only waits at the same barriers.
-__device__ __forceinline__ void draw_warp(const int *seedp, float *ring, const int *flag, int bar_id, int lane)
+__device__ __forceinline__ uint32_t draw_chunk(uint32_t xs, float *buf, int lane)
 {
-    uint32_t xs = pm_norm(seedp[lane]);
-    for (int c = 0;; c++) {
-        float *buf = ring + (c & 1) * kDrawChunk * 32;
 #pragma unroll 4
-        for (int k = 0; k < kDrawChunk; k++) {
-            xs = pm_mul(xs, 16807u);
-            buf[k * 32 + lane] = race_rate(pm_uniform(xs));
-        }
+    for (int k = 0; k < kDrawChunk; k++) {
+        xs = pm_mul(xs, 16807u);
+        buf[k * 32 + lane] = race_rate(pm_uniform(xs));
+    }
+    return xs;
+}
+
+// xs: the lane's state after chunk 0, which the helper fills while the item's
+// tables are still being staged.
+__device__ __forceinline__ void draw_warp(uint32_t xs, float *ring, const int *flag, int bar_id, int lane)
+{
+    for (int c = 0;; c++) {
+        if (c > 0) xs = draw_chunk(xs, ring + (c & 1) * kDrawChunk * 32, lane);
         pair_barrier(bar_id);
         if (*reinterpret_cast<const volatile int *>(flag + (c & 1))) break;
     }
@@ -585,6 +591,14 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
         for (int i = threadIdx.x; i < 2 * apc; i += blockDim.x) pend_all[i] = 0;
         if (threadIdx.x < 4) reinterpret_cast<int *>(smem + L.cnt)[threadIdx.x] = 0;
     }
+    float *ring = reinterpret_cast<float *>(smem + L.ring) + (size_t)(DRAW ? warp % apc : 0) * 2 * kDrawChunk * 32;
+    int *hflag = reinterpret_cast<int *>(smem + L.flag) + (DRAW ? warp % apc : 0) * 2;
+    // helper warps: warp apc + j draws for ant j, its first chunk during the staging
+    const bool helper = DRAW && warp >= apc && warp < 2 * apc && ant0 + (warp - apc) < a.n_ants;
+    uint32_t hx = 0;
+    if (helper) hx = draw_chunk(pm_norm(a.seeds[(size_t)(ant0 + warp - apc) * a.nloc + lane]), ring, lane);
+    // an ant warp's Park-Miller states, loaded while the tables are staged
+    const int seed0 = warp < apc && ant0 + warp < a.n_ants ? a.seeds[(size_t)(ant0 + warp) * a.nloc + lane] : 0;
     const bool ok = mbar_wait(bar, phase);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) set_status(a.status, ACO_ERR_TIMEOUT);
@@ -593,11 +607,8 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
     }
 
     const int ant = ant0 + warp;
-    float *ring = reinterpret_cast<float *>(smem + L.ring) + (size_t)(DRAW ? warp % apc : 0) * 2 * kDrawChunk * 32;
-    int *hflag = reinterpret_cast<int *>(smem + L.flag) + (DRAW ? warp % apc : 0) * 2;
-    if (DRAW && warp >= apc) { // helper warps: warp apc + j draws for ant j
-        if (warp < 2 * apc && ant0 + (warp - apc) < a.n_ants)
-            draw_warp(a.seeds + (size_t)(ant0 + warp - apc) * a.nloc, ring, hflag, 1 + warp - apc, lane);
+    if (DRAW && warp >= apc) {
+        if (helper) draw_warp(hx, ring, hflag, 1 + warp - apc, lane);
         return true;
     }
     if (LSF && warp >= apc) {
@@ -644,7 +655,7 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
         bool mind_stale = false;
         // lane l draws from the ant's Park-Miller state l (nloc >= 32), one number a step
         int *seedp = a.seeds + (size_t)ant * a.nloc;
-        uint32_t xs = pm_norm(seedp[lane]);
+        uint32_t xs = pm_norm(seed0);
         int hand = 0; // hand-overs passed (helper-warp draws)
         if (DRAW) {   // hand-over 0: the helper has filled chunk 0
             if (lane == 0) hflag[0] = 0;
