@@ -140,6 +140,7 @@ struct DeviceRes {
     int *pinned = nullptr;
     std::mutex mu;
     std::vector<int> free_slots;
+    std::vector<cudaStream_t> free_streams; // streams of destroyed colonies, idle, reused by new ones
 };
 
 constexpr int kMaxDevices = 64, kSlotInts = 16, kSlots = 256;
@@ -189,6 +190,21 @@ int *take_pinned_slot(DeviceRes &r)
     return r.pinned + (size_t)i * kSlotInts;
 }
 
+cudaStream_t take_stream(DeviceRes &r)
+{
+    std::lock_guard<std::mutex> lk(r.mu);
+    if (r.free_streams.empty()) return nullptr;
+    cudaStream_t s = r.free_streams.back();
+    r.free_streams.pop_back();
+    return s;
+}
+
+void give_stream(DeviceRes &r, cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lk(r.mu);
+    r.free_streams.push_back(s);
+}
+
 bool give_pinned_slot(DeviceRes &r, int *p)
 {
     if (!r.pinned || p < r.pinned || p >= r.pinned + kSlotInts * kSlots) return false;
@@ -219,7 +235,10 @@ Colony::~Colony()
     if (st) cudaStreamSynchronize(st);
     DeviceRes *r = device_res(dev);
     if (h_pin && !(r && give_pinned_slot(*r, h_pin))) cudaFreeHost(h_pin);
-    if (st) cudaStreamDestroy(st);
+    if (st) { // idle after the synchronisation above: kept for the next colony on this device
+        if (r && cudaStreamQuery(st) == cudaSuccess) give_stream(*r, st);
+        else cudaStreamDestroy(st);
+    }
 }
 
 int Colony::set_device() const
@@ -257,7 +276,8 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     sm_count = res->sm;
     int rc = set_device();
     if (rc != ACO_OK) return rc;
-    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    st = take_stream(*res);
+    if (!st) CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     h_pin = take_pinned_slot(*res);
     if (!h_pin) CK(cudaMallocHost(&h_pin, 64));
 
@@ -990,9 +1010,12 @@ int Colony::init()
     if (rc == ACO_OK) rc = stats(false);
     if (rc == ACO_OK) rc = pheromone_init(0.f, true);
     if (rc != ACO_OK) return rc;
+    // the iteration graph is captured and instantiated on the host while the
+    // device runs the initial iteration (capture records, it does not run)
+    if (p.use_graph) rc = ensure_graph();
     const int status = sync_status();
-    initialized = status == ACO_OK;
-    return status;
+    initialized = status == ACO_OK && rc == ACO_OK;
+    return status != ACO_OK ? status : rc;
 }
 
 int Colony::enqueue(int n_iter)

@@ -29,6 +29,10 @@
 // distance matrix.
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "aco_device.cuh"
 #include "kernels.h"
 #include "two_opt.cuh"
@@ -607,11 +611,25 @@ size_t local_search_smem(int n_max, int ants_per_cta, int warps) { return ls_sme
 
 int local_search_occupancy(int warps, size_t smem)
 {
+    // answers are kept per (device, warps, shared memory): a colony's shape
+    // search asks a few hundred of them
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, size_t>, int> memo;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(dev, warps, smem);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        const auto it = memo.find(key);
+        if (it != memo.end()) return it->second;
+    }
     if (cudaFuncSetAttribute(local_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return 0;
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, local_search_kernel, warps * 32, smem) != cudaSuccess)
         return 0;
+    std::lock_guard<std::mutex> lk(mu);
+    memo[key] = blocks;
     return blocks;
 }
 
