@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, Stat
     // entry is +inf and each further round takes index 0.  With all lengths in
     // one pass of the block, each entry's rank is the number of keys below its
     // own, and the first R-1 finite ranks place themselves.
-    if (do_elites && A <= bs) {
+    if (do_elites && A <= bs && R > 1) {
         // keys (length bits, index) are unique.  Threshold t: the (R-1)-th
         // smallest of the warps' minima (at least R-1 keys are at most t, so the
         // R-1 smallest all are); only keys up to t are ranked, among themselves.
