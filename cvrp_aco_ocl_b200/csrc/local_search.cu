@@ -15,8 +15,10 @@
 // budget the bit may still be clear; that error path reports ACO_ERR_LS_LIMIT
 // and its tours are valid but not matched bit for bit.)
 //
-// One CTA per ant; its warps pull routes from a shared counter.  A route of at
-// most 32 nodes (depot included) runs entirely in one warp's registers: lane q
+// local_search_kernel: CTAs of 1-8 ants whose warps pull the routes of all of
+// them from a shared counter, longest first; route_opt_kernel: a persistent
+// grid over the construct's list of every ant's routes (see below).  A route of
+// at most 32 nodes (depot included) runs entirely in one warp's registers: lane q
 // holds the local node at route position q, its edge length, and the position
 // of local node q; the don't-look bits are one warp-uniform mask; the route's
 // distance sub-matrix is a 32x32 shared tile; and every node's neighbour list
