@@ -464,7 +464,11 @@ cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, siz
     cudaError_t e = cudaFuncSetAttribute(stats_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    stats_kernel<<<n_inst, 1024, smem, st>>>(one ? nullptr : d_args, one ? *one : StatsArgs{}, do_elites);
+    // one thread per ant (smem holds one length per ant), at least 8 and at most 32 warps:
+    // fewer warps make every block barrier cheaper
+    int threads = (int)((smem / sizeof(float) + 31) / 32 * 32);
+    threads = threads < 256 ? 256 : (threads > 1024 ? 1024 : threads);
+    stats_kernel<<<n_inst, threads, smem, st>>>(one ? nullptr : d_args, one ? *one : StatsArgs{}, do_elites);
     return cudaGetLastError();
 }
 
