@@ -203,6 +203,7 @@ def run_ours(args, ws, rank, local):
     best_tour, best_len = S.best()
     sol, lens = S.solutions()
     draw = bool(S.config()[2] & 4)  # construct_nn_draw_kernel is the construct launched
+    launches = S.launches_per_iteration()
     S.close()
 
     # roofline of the dominant kernel: algorithmic bytes per launch / launch time
@@ -234,7 +235,7 @@ def run_ours(args, ws, rank, local):
                    "mode": "throughput", "ras_ranks": 6, "parallelism": f"replicas x{ws}",
                    "l2": "flushed before every timed iteration (256 MiB write)", "instance_seed": SEED_INSTANCE},
         "clocks": clk.summary(), "roofline": roofline,
-        "gpu_launches": args.steps * 4,  # construct, 2-opt, statistics, row pass per iteration
+        "gpu_launches": args.steps * launches,  # construct, 2-opt, statistics, row pass per iteration
         "best_length": float(best_len),
     }
     if not args.no_batched:
@@ -309,6 +310,7 @@ def run_batched(args, ws, rank, local, peak, peak_kind):
         dist.all_reduce(tot, op=dist.ReduceOp.SUM)
     ms_max = float(t.item())
     phase = B.time_phases(args.batch_steps)
+    launches = B.launches_per_iteration()  # the route-level 2-opt adds a kernel
     B.close()
     n_all = [pr.num_node for pr in probs]
     row_bytes = sum(16 * n * n for n in n_all)
@@ -320,7 +322,7 @@ def run_batched(args, ws, rank, local, peak, peak_kind):
         "value": float(tot.item()) * args.batch_steps / (ms_max / 1e3), "unit": UNIT,
         "ms_per_step": ms_max / args.batch_steps, "steps": args.batch_steps, "instances_this_rank": count,
         "ants_this_rank": total_ants, "setup_s": t_setup,
-        "gpu_launches": args.batch_steps * 4,
+        "gpu_launches": args.batch_steps * launches,
         "kernel_share": {k: float(v) for k, v in zip(KERNELS, phase / phase.sum())},
         "roofline": {"bound": "hbm", "kernel": "rows_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profile_traffic("rows_kernel@batch"),

@@ -34,7 +34,7 @@ EXPORTED = [
     "aco_pheromone_update_noalloc", "aco_batch_create", "aco_batch_init", "aco_batch_iterate",
     "aco_batch_enqueue_iterations", "aco_batch_status", "aco_batch_size", "aco_batch_get_best",
     "aco_batch_get_solutions", "aco_batch_get_pheromone", "aco_batch_time_phases", "aco_batch_get_stream",
-    "aco_batch_destroy", "aco_autotune", "aco_batch_autotune", "aco_mpnn_param_count", "aco_mpnn_workspace_bytes",
+    "aco_batch_destroy", "aco_batch_launches_per_iteration", "aco_autotune", "aco_batch_autotune", "aco_mpnn_param_count", "aco_mpnn_workspace_bytes",
     "aco_mpnn_forward", "aco_mpnn_grad", "aco_mpnn_adam", "aco_mpnn_status", "aco_set_prior", "aco_batch_set_prior",
     "aco_last_cuda_error", "aco_compute_distances_device", "aco_compute_nn_lists_device", "aco_validate",
     "aco_write_solution", "aco_batch_validate", "aco_batch_write_solutions", "aco_batch_get_bsf_records",
@@ -119,6 +119,7 @@ def lib() -> ctypes.CDLL:
         L.aco_get_stream.restype = vp
         L.aco_time_iterations.argtypes = [vp, ip, ctypes.POINTER(fp)]
         L.aco_enqueue_iterations.argtypes = [vp, ip]
+        L.aco_batch_launches_per_iteration.argtypes = [vp]
         L.aco_enqueue_lengths.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
         L.aco_read_lengths.argtypes = [vp, ctypes.c_longlong, vp, ctypes.c_size_t]
         L.aco_time_phases.argtypes = [vp, ip, vp]

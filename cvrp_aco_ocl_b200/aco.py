@@ -415,6 +415,9 @@ class Batch:
         check(lib().aco_batch_size(self.h, ctypes.byref(c), ctypes.byref(a)), "aco_batch_size")
         return c.value, a.value
 
+    def launches_per_iteration(self) -> int:
+        return lib().aco_batch_launches_per_iteration(self.h)
+
     def stream(self) -> int:
         return lib().aco_batch_get_stream(self.h)
 

@@ -967,6 +967,14 @@ int Colony::run_phases()
     return rc;
 }
 
+int Colony::launches_per_iteration() const
+{
+    int k = 3; // construct, statistics, pheromone pass
+    if (p.ls_flag) k += 1 + (use_routes_ && cn_lsw == 0 ? 1 : 0) + ((p.ls_flag & 2) ? 1 : 0); // 2-opt kernels, swap
+    if (p.ns_rounds > 0) k += 1;
+    return k;
+}
+
 int Colony::sync_status()
 {
     CK(cudaMemcpyAsync(h_pin, status_d, sizeof(int), cudaMemcpyDeviceToHost, st));

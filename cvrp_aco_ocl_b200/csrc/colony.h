@@ -64,6 +64,7 @@ public:
     int init();                  // g_ACO::init_aco for every instance
     int enqueue(int n_iter);     // n_iter iterations (graph replays), no sync
     int sync_status();           // wait for the stream, read the sticky status
+    int launches_per_iteration() const; // kernel launches of one iteration (graph nodes)
     int construct(bool fused = false); // fused: with the 2-opt warps when configured
     int local_search();
     int neighbourhood(); // the random-descent stage (ns_rounds > 0)

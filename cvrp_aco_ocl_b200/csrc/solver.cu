@@ -557,7 +557,13 @@ void *aco_get_stream(aco_solver *s) { return s ? (void *)s->c.st : nullptr; }
 int aco_launches_per_iteration(aco_solver *s)
 {
     if (!s) return ACO_ERR_INVALID;
-    return 3 + (s->c.p.ls_flag ? 1 : 0) + ((s->c.p.ls_flag & 2) ? 1 : 0) + (s->c.p.ns_rounds > 0 ? 1 : 0);
+    return s->c.launches_per_iteration();
+}
+
+int aco_batch_launches_per_iteration(aco_batch *b)
+{
+    if (!b) return ACO_ERR_INVALID;
+    return b->c.launches_per_iteration();
 }
 
 int aco_time_iterations(aco_solver *s, int n_iter, float *ms)

@@ -296,6 +296,8 @@ int aco_batch_get_solutions(aco_batch *b, int idx, int *solutions, size_t cap_in
 int aco_batch_get_pheromone(aco_batch *b, int idx, float *tau, float *total_info, size_t cap);
 int aco_batch_time_phases(aco_batch *b, int n_iter, float *ms4);
 void *aco_batch_get_stream(aco_batch *b);
+/* number of kernel launches one batch iteration makes (graph nodes).  No reference counterpart. */
+int aco_batch_launches_per_iteration(aco_batch *b);
 void aco_batch_destroy(aco_batch *b);
 
 /* ---- learned prior: edge-scoring network (no reference counterpart) -------
