@@ -70,3 +70,24 @@ def test_shipped_prior_weights_match_the_network():
     assert int(d["layers"]) == PR.LAYERS
     assert d["params"].size == lib().aco_mpnn_param_count(PR.LAYERS)
     assert np.all(np.isfinite(d["params"]))
+
+
+def test_table_without_newer_fields_loads_and_fills(tmp_path):
+    # a table written before ls_ants existed: the field defaults to 0 (automatic)
+    path = tmp_path / "old.json"
+    path.write_text('{"version": 1, "device": "x", "entries": [{"mode": 1, "n_lo": 3, "n_hi": 500, "ants": 128, '
+                    '"ants_per_block": 4, "warps_per_ant": 0, "ls_warps": 16, "stage_matrix": 0, '
+                    '"ms_per_iter": 1.0}]}')
+    t = TuneTable.load(str(path))
+    assert t.entries[0].ls_ants == 0 and t.entries[0].nn_ants == 0
+    p = default_params(200)
+    p.mode, p.n_ants = MODE_THROUGHPUT, 128
+    t.apply(p, 200)
+    assert p.ants_per_block == 4 and p.ls_warps == 16 and p.ls_ants == 0
+
+
+def test_committed_table_loads():
+    import os
+    from cvrp_aco_ocl_b200 import tune
+    t = TuneTable.load(os.path.join(os.path.dirname(tune.__file__), "tune_b200.json"))
+    assert t.entries and all(e.ls_ants == 0 for e in t.entries)
