@@ -1,27 +1,38 @@
 """Benchmark: ant-tours/s of the ACO iteration (construct + 2-opt + update).
 
-Workload (the single-instance GPU configuration): one synthetic CVRP instance
-with 200 customers (201 nodes; half uniform in [0,1000]^2, half from 8 Gaussian
-clusters, depot at the centre, demand U{1..100}, capacity for ~12 customers a
-route), 200 ants, 25-nearest-neighbour candidate lists (throughput mode:
-prefix-sum roulette), 2-opt over 25-NN lists, rank-based update with 6 ranks,
-fp32 pheromone / choice_info / distances.  A step is one ACO iteration (200
-ant-tours).  L2 is flushed (256 MiB write) before every timed iteration.
+Headline workload (the batched configuration, the largest that fits one GPU):
+512 independent synthetic CVRP instances per GPU, customer count uniform in
+[100, 1000], drawn alternately from the mixed generator (half uniform in
+[0,1000]^2, half from 8 Gaussian clusters, sigma 40, depot at the centre,
+demand U{1..100}, ~12 customers a route) and the large generator (uniform or
+clustered, depot random/centre/corner, uniform or 80/20 small/large demand,
+~15 customers a route); 128 ants each, 25-nearest-neighbour candidate lists,
+2-opt on 25-NN lists, rank-based update with 6 ranks, fp32 state.  All
+instances advance together: one iteration is one replay of a CUDA graph of five
+kernel launches for the whole batch.  A step is one iteration (65,536
+ant-tours).  The matrices (3.4 GB) exceed L2, so no flush is needed between
+timed iterations.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Under torchrun (N > 1) every rank runs an independent replica of the workload
-(the single-instance path does not shard); `value` is the total over ranks
-divided by the slowest rank's device time.  `--impl reference` times the CPU
-port of the reference's path (the oracle, all host threads) on the same
-workload; rank 0 alone runs it.
+Extra keys of the line: `single` (200 customers, 200 ants), `large` (1000
+customers, 256 ants, 30-NN lists), `parity` (the reference's own algorithm:
+50 customers, 50 ants, full-row I-Roulette, 2-opt on full lists, 800
+iterations, bit-compared with the CPU restatement of the reference's kernels)
+and `learned_vs_plain` (time for the learned-prior colony to come within 1% of
+the plain colony's FP64-checked best on held-out 1000-customer instances).
+
+Under torchrun (N > 1) the global batch is 512 x N instances, partitioned over
+the ranks by estimated cost (cvrp_aco_ocl_b200.shard; no collective on the data
+path): weak scaling, `value` = all ranks' ant-tours / the slowest rank's device
+time.  `--impl reference` times the CPU port of the reference's path (the
+oracle, all host threads) on a stratified sample of the same batch at the same
+iteration offsets; rank 0 alone runs it.
 """
 from __future__ import annotations
 
 import argparse
-import ctypes
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -34,39 +45,71 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_CUST, ANTS, NN_ANTS, NN_LS, NLOC = 200, 200, 25, 25, 256
-SEED_INSTANCE, SEED_TIME, RND_SEED = 2026, 1796300000, 4242
-BATCH_COUNT, BATCH_ANTS, BATCH_SEED = 512, 128, 512
-KERNELS = ["construct_nn_kernel", "local_search_kernel", "stats_kernel", "rows_kernel"]
 METRIC = "ant-tours/sec (construct+2-opt+update)"
 UNIT = "ant-tours/s"
-WORKLOAD = ("single CVRP instance, 200 customers (50% uniform, 50% 8 Gaussian clusters), 200 ants, "
-            "25-NN candidate lists, 2-opt on 25-NN lists, rank-based pheromone update")
+SEED_TIME, RND_SEED, NLOC = 1796300000, 4242, 256
+# headline: the batch
+BATCH_COUNT, BATCH_ANTS, BATCH_SEED, NN_ANTS, NN_LS, RANKS = 512, 128, 512, 25, 25, 6
+CPU_SAMPLE_STRIDE = 16  # the CPU legs run every 16th instance of the size-sorted batch (32 of 512)
+# extra sections
+SINGLE_CUST, SINGLE_ANTS, SINGLE_SEED = 200, 200, 2026
+LARGE_CUST, LARGE_ANTS, LARGE_K, LARGE_SEED = 1000, 256, 30, 3031
+# 800 iterations: on this configuration the reference's algorithm stops working at iteration 866.  With
+# rho = 0.1 and no lower bound on tau, tau * eta^beta of the unused edges underflows to 0 in fp32.  Every
+# choice value is then 0, and kernel.cl:461 sends the ant back to the depot forever.  The reference hangs
+# there; this build reports ACO_ERR_STEP_LIMIT.
+PARITY_CUST, PARITY_ANTS, PARITY_ITERS, PARITY_SEED = 50, 50, 800, 2024
+LEARNED_N, LEARNED_COUNT, LEARNED_PLAIN_ITERS, LEARNED_ANTS = 1001, 8, 500, 256
+PHASES = ["construct", "two_opt", "stats", "rows"]
+PHASE_KERNELS = {"construct": "construct_nn_kernel", "two_opt": "route_opt_kernel+local_search_kernel",
+                 "stats": "stats_kernel", "rows": "rows_kernel"}
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def make_instance(rank: int = 0):
+def batch_workload(ws: int, rank: int):
+    """This rank's shard of the global batch (512 x ws instances) and their
+    indices in it."""
     from cvrp_aco_ocl_b200 import instances as I
-    return I.gen_mixed(SEED_INSTANCE + rank, N_CUST)
+    from cvrp_aco_ocl_b200.shard import shard_of
+
+    every = I.gen_batch(BATCH_SEED, BATCH_COUNT * ws, 100, 1000)
+    idx = shard_of([x.n for x in every], BATCH_ANTS, ws, rank)
+    return [every[i] for i in idx], idx
+
+
+def batch_params(local: int):
+    from cvrp_aco_ocl_b200 import MODE_THROUGHPUT, default_params
+    p = default_params(1001)
+    p.mode, p.n_ants, p.nn_ants, p.nn_ls, p.nloc, p.ras_ranks = MODE_THROUGHPUT, BATCH_ANTS, NN_ANTS, NN_LS, NLOC, RANKS
+    p.seed_time, p.rnd_seed, p.device, p.ls_flag = SEED_TIME, RND_SEED, local, 1
+    return p
+
+
+def config(ws: int):
+    return {"workload": f"{BATCH_COUNT} independent CVRP instances per GPU, 100-1000 customers each (mixed and large "
+                        f"generators alternately), {BATCH_ANTS} ants each, {NN_ANTS}-NN candidate lists, 2-opt on "
+                        f"{NN_LS}-NN lists, rank-based pheromone update ({RANKS} ranks), one batched iteration per step",
+            "instances": BATCH_COUNT * ws, "ants": BATCH_ANTS, "nn_ants": NN_ANTS, "nn_ls": NN_LS,
+            "mode": "throughput", "ras_ranks": RANKS, "batch_seed": BATCH_SEED,
+            "parallelism": f"instances sharded by cost over {ws} GPU(s)",
+            "l2": "inputs exceed L2 (about 3.4 GB of matrices per GPU): no flush"}
 
 
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
 
 
-def profile_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summaries
-    (a line 'dram_bytes_per_launch <kernel> <bytes>'), or None."""
+def profile_figure(key: str, name: str):
+    """A machine-readable figure `<key> <name> <value>` from the committed ncu
+    summaries under profiles/, or None."""
     d = os.path.join(ROOT, "profiles")
     if not os.path.isdir(d):
         return None
@@ -74,9 +117,9 @@ def profile_traffic(kernel: str):
         try:
             for line in open(os.path.join(d, f)):
                 parts = line.split()
-                if len(parts) == 3 and parts[0] == "dram_bytes_per_launch" and parts[1] == kernel:
+                if len(parts) == 3 and parts[0] == key and parts[1] == name:
                     return float(parts[2])
-        except Exception:
+        except (OSError, ValueError):
             pass
     return None
 
@@ -98,7 +141,7 @@ class ClockSampler:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
-        except Exception:
+        except OSError:
             self.p = None
         time.sleep(0.3)
         return self
@@ -109,7 +152,7 @@ class ClockSampler:
             self.p.terminate()
             try:
                 self.p.wait(timeout=5)
-            except Exception:
+            except subprocess.TimeoutExpired:
                 self.p.kill()
 
     def summary(self):
@@ -136,326 +179,408 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def timed_launches(enqueue, stream, steps, dev):
+    """Device time of `steps` calls of enqueue(), each bracketed by CUDA events
+    recorded on the solver's own stream (milliseconds, summed)."""
+    import torch
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in evs:
+        e0.record(stream)
+        enqueue()
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    return sum(e0.elapsed_time(e1) for e0, e1 in evs)
+
+
 # --------------------------------------------------------------------------
+def kernel_rooflines(phase_ms, steps, row_bytes, clk, peak_hbm, peak_src, workload_tag):
+    """Per phase: launch time, share and the bound that limits it.  The pheromone
+    pass is HBM-bound (16 bytes per matrix element); the construct and the 2-opt
+    are issue-bound (many independent warp-serial chains, no bandwidth near a
+    limit): achieved = warp instructions per launch (ncu, committed under
+    profiles/) / the live launch time, against 148 SMs x 4 schedulers x the SM
+    clock sampled during the timed region."""
+    out = {}
+    total = float(sum(phase_ms))
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    issue_peak = 148 * 4 * mhz * 1e6 / 1e9  # G warp-instructions/s
+    for k, name in enumerate(PHASES):
+        launch_ms = float(phase_ms[k]) / steps
+        e = {"kernel": PHASE_KERNELS[name], "launch_ms": launch_ms, "share": float(phase_ms[k]) / total}
+        if name == "rows":
+            ach = row_bytes / (launch_ms / 1e3) / 1e9
+            e.update({"bound": "hbm", "achieved": ach, "peak": peak_hbm, "unit": "GB/s", "frac": ach / peak_hbm,
+                      "algorithmic_bytes_per_launch": row_bytes, "peak_source": peak_src,
+                      "traffic": profile_figure("dram_bytes_per_launch", f"rows_kernel@{workload_tag}")})
+        elif name in ("construct", "two_opt"):
+            ks = PHASE_KERNELS[name].split("+")
+            insts = [profile_figure("warp_inst_per_launch", f"{k2}@{workload_tag}") for k2 in ks]
+            inst = sum(insts) if all(v is not None for v in insts) else None
+            ach = inst / (launch_ms / 1e3) / 1e9 if inst is not None else None
+            e.update({"bound": "issue", "achieved": ach, "peak": issue_peak, "unit": "G warp-instructions/s",
+                      "frac": ach / issue_peak if ach is not None else None,
+                      "warp_instructions_per_launch": inst,
+                      "peak_source": f"148 SMs x 4 issue slots x {mhz:.0f} MHz (sampled)",
+                      "smem_frac_ncu": profile_figure("smem_pipe_frac", f"{ks[0]}@{workload_tag}"),
+                      "issue_active_ncu": profile_figure("issue_active_frac", f"{ks[0]}@{workload_tag}"),
+                      "traffic": sum(v for v in (profile_figure("dram_bytes_per_launch", f"{k2}@{workload_tag}")
+                                                 for k2 in ks) if v is not None) or None})
+        else:
+            e.update({"bound": "latency"})
+        out[name] = e
+    return out
+
+
 def run_ours(args, ws, rank, local):
     import torch
-    from cvrp_aco_ocl_b200 import MODE_THROUGHPUT, Problem, Solver, default_params
+    from cvrp_aco_ocl_b200 import Batch, Problem
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    dist = None
     if ws > 1:
         import datetime
-
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    inst = make_instance(rank)
-    prob = Problem.from_instance(inst)
+    insts, _ = batch_workload(ws, rank)
+    probs = [Problem.from_instance(x) for x in insts]
+    B = Batch(probs, batch_params(local))
+    B.init()
+    count, total_ants = B.size()
+    stream = torch.cuda.ExternalStream(B.stream(), device=dev)
+    for _ in range(args.warmup):
+        B.enqueue(1)
+    if B.status() != 0:
+        raise RuntimeError("batched warm-up failed")
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        ms = timed_launches(lambda: B.enqueue(1), stream, args.steps, dev)
+    rc = B.status()
+    if rc != 0:
+        raise RuntimeError(f"device status {rc}")
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    tot = torch.tensor([float(total_ants)], device=dev, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    ms_max = float(t.item())
+    value = float(tot.item()) * args.steps / (ms_max / 1e3)
+    launches = B.launches_per_iteration()
+    # per-phase device time, same batch and stream, phase by phase with events between
+    n_phase = max(3, args.steps // 2)
+    phase_ms = B.time_phases(n_phase)
+    B.close()
+    row_bytes = sum(16 * p.num_node * p.num_node for p in probs)
+    peak, peak_src = load_peaks()
+    clocks = clk.summary()
+    kern = kernel_rooflines(phase_ms, n_phase, row_bytes, clocks, peak, peak_src, "batch512")
+    dom = max(kern, key=lambda k: kern[k]["share"])
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded generators, no dataset)", "config": config(ws),
+        "clocks": clocks, "roofline": dict(kern[dom], phase=dom), "kernels": kern,
+        "roofline_hbm": dict(kern["rows"], phase="rows"),
+        "gpu_launches": args.steps * launches, "launches_per_iteration": launches,
+        "instances_this_rank": count, "ants_this_rank": total_ants,
+    }
+    # end to end through the public API, host buffers in, results out
+    e2e = run_e2e(args, ws, rank, local)
+    if dist is not None:
+        e = torch.tensor([e2e["seconds"]], device=dev, dtype=torch.float64)
+        dist.all_reduce(e, op=dist.ReduceOp.MAX)
+        e2e["value"] = float(tot.item()) * args.steps / float(e.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    result["e2e"] = e2e
+    if rank != 0:
+        return
+    if not args.no_extras:
+        result["single"] = run_single(args, local)
+        result["large"] = run_large(args, local)
+        result["parity"] = run_parity(args, local)
+        if not args.no_learned:
+            result["learned_vs_plain"] = run_learned(args)
+    if ws == 1 and not args.no_cpu_baseline:
+        v, done, dt, sample = oracle_batch_run(os.cpu_count() or 1, args.warmup, args.steps, args.cpu_seconds)
+        result["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                                  "sample": sample}
+    print(json.dumps(result, default=float))
 
-    def params():
-        p = default_params(inst.n)
-        p.n_ants, p.nn_ants, p.nn_ls, p.nloc, p.mode = ANTS, NN_ANTS, NN_LS, NLOC, MODE_THROUGHPUT
-        p.seed_time, p.rnd_seed, p.device, p.ls_flag = SEED_TIME, RND_SEED + rank, local, 1
-        return p
 
-    S = Solver(prob, params())
+def run_e2e(args, ws, rank, local):
+    """aco_batch_create from host arrays (coordinates and demands copied
+    host->device; distances, NN lists and seeds computed there), aco_batch_init,
+    then per step one iteration and a device->host read of every instance's ant
+    and best-so-far lengths (pipelined: iteration k is queued before iteration
+    k-1's lengths are read), then every best tour read back in one transfer:
+    the reference's main.cpp loop through the C ABI, for the whole batch, timed
+    by the host clock."""
+    import torch
+    from cvrp_aco_ocl_b200 import Batch, Problem
+
+    insts, _ = batch_workload(ws, rank)
+    probs = [Problem.from_instance(x) for x in insts]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    B = Batch(probs, batch_params(local))
+    B.init()
+    buf = np.zeros(B.lengths_total(), np.float32)
+    prev = -1
+    for _ in range(args.steps):
+        # queue iteration k and the copy of its lengths, then read iteration k-1's
+        B.enqueue(1)
+        tk = B.enqueue_lengths()
+        if prev >= 0:
+            B.read_lengths(prev, buf)
+        prev = tk
+    B.read_lengths(prev, buf)
+    tours, best = B.best_all()
+    t1 = time.perf_counter()
+    count, total_ants = B.size()
+    B.close()
+    h2d = sum(p.num_node * 4 * 3 for p in probs) + count * 1024  # coordinates, demands; tables and argument blocks
+    d2h_step = buf.size * 4 + 4  # lengths and the status word
+    d2h_end = sum(2 * p.num_node * 4 + 8 for p in probs)
+    return {"value": total_ants * args.steps / (t1 - t0), "unit": UNIT, "seconds": t1 - t0,
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h_step + d2h_end / args.steps,
+            "best_length_mean": float(np.mean(best)),
+            "note": "batch create + init + iterations with per-step length readback + best tours, host wall clock"}
+
+
+def single_params(n, ants, k, local, seed):
+    from cvrp_aco_ocl_b200 import MODE_THROUGHPUT, default_params
+    p = default_params(n)
+    p.n_ants, p.nn_ants, p.nn_ls, p.nloc, p.mode = ants, k, k, NLOC, MODE_THROUGHPUT
+    p.seed_time, p.rnd_seed, p.device, p.ls_flag = SEED_TIME, seed, local, 1
+    return p
+
+
+def run_one_instance(args, local, inst, ants, k, label):
+    """Device time of one instance's iterations (L2 flushed before each)."""
+    import torch
+    from cvrp_aco_ocl_b200 import Problem, Solver
+
+    dev = torch.device("cuda", local)
+    S = Solver(Problem.from_instance(inst), single_params(inst.n, ants, k, local, RND_SEED))
     S.init()
     stream = torch.cuda.ExternalStream(S.stream(), device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     for _ in range(args.warmup):
-        with torch.cuda.stream(stream):
-            flush.zero_()
         S.enqueue(1)
     S.status()
-    torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        for e0, e1 in evs:
-            with torch.cuda.stream(stream):
-                flush.zero_()  # L2 flush between timed iterations (not timed)
-                e0.record(stream)
-            S.enqueue(1)
-            with torch.cuda.stream(stream):
-                e1.record(stream)
-        torch.cuda.synchronize()
-    rc = S.status()
-    if rc != 0:
-        raise RuntimeError(f"device status {rc}")
+    torch.cuda.synchronize(dev)
+    for e0, e1 in evs:
+        with torch.cuda.stream(stream):
+            flush.zero_()  # L2 flush between timed iterations (not timed)
+        e0.record(stream)
+        S.enqueue(1)
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if S.status() != 0:
+        raise RuntimeError(f"{label}: device status")
     ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = ws * ANTS * args.steps / (ms_max / 1e3)
-
-    # per-kernel shares (device time, phase by phase, same workload and stream)
-    phase_ms = S.time_phases(max(5, args.steps // 2))
-    names = KERNELS
-    share = phase_ms / phase_ms.sum()
-    dom = int(np.argmax(phase_ms))
-    n_phase = max(5, args.steps // 2)
-    best_tour, best_len = S.best()
-    sol, lens = S.solutions()
-    draw = bool(S.config()[2] & 4)  # construct_nn_draw_kernel is the construct launched
-    launches = S.launches_per_iteration()
+    phase = S.time_phases(max(3, args.steps // 2))
+    _, best = S.best()
     S.close()
-
-    # roofline of the dominant kernel: algorithmic bytes per launch / launch time
-    n = inst.n
-    routes = int(np.count_nonzero(best_tour == 0)) - 1
-    steps_per_tour = (n - 1) + routes
-    algo = {
-        "construct_nn_kernel": ANTS * steps_per_tour * NN_ANTS * 12,   # neighbour id + choice_info + distance
-        "local_search_kernel": ANTS * 2 * (2 * n) * 4 * 4,              # tour read/write + edge lengths, 4 B each
-        "stats_kernel": (ANTS + 1) * 4 + 6 * (2 * n) * 4,
-        "rows_kernel": 16 * n * n,                                     # read tau, heur; write tau, total
-    }
-    peak, peak_kind = load_peaks()
-    dk = names[dom]
-    kname = "construct_nn_draw_kernel" if dk == "construct_nn_kernel" and draw else dk
-    dur_s = phase_ms[dom] / n_phase / 1e3
-    achieved = algo[dk] / dur_s / 1e9
-    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": profile_traffic(kname),
-                "algorithmic_bytes_per_launch": algo[dk], "launch_ms": phase_ms[dom] / n_phase,
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
-                "fallback 6.65 TB/s", "kernel_share": {k: float(s) for k, s in zip(names, share)}}
-
-    result = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": WORKLOAD, "n_nodes": n, "ants": ANTS, "nn_ants": NN_ANTS, "nn_ls": NN_LS,
-                   "mode": "throughput", "ras_ranks": 6, "parallelism": f"replicas x{ws}",
-                   "l2": "flushed before every timed iteration (256 MiB write)", "instance_seed": SEED_INSTANCE},
-        "clocks": clk.summary(), "roofline": roofline,
-        "gpu_launches": args.steps * launches,  # construct, 2-opt, statistics, row pass per iteration
-        "best_length": float(best_len),
-    }
-    if not args.no_batched:
-        result["batched"] = run_batched(args, ws, rank, local, peak, peak_kind)
-    # end to end through the public API with host buffers
-    if rank == 0 or ws > 1:
-        result["e2e"] = run_e2e(args, rank, local)
-    if ws > 1:
-        import torch.distributed as dist
-        e = torch.tensor([result["e2e"]["value"]], device=dev, dtype=torch.float64)
-        dist.all_reduce(e, op=dist.ReduceOp.MIN)
-        result["e2e"]["value"] = float(e.item()) * ws
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        if ws == 1 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline(seconds=args.cpu_seconds)
-        print(json.dumps(result, default=float))
+    return {"value": ants * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
+            "n_nodes": inst.n, "ants": ants, "nn_ants": k, "nn_ls": k, "best_length": float(best),
+            "phase_share": {nm: float(v) for nm, v in zip(PHASES, phase / phase.sum())},
+            "l2": "flushed before every timed iteration (256 MiB write)"}
 
 
-def run_batched(args, ws, rank, local, peak, peak_kind):
-    """Batched workload: BATCH_COUNT independent instances, customer count
-    uniform in [100, 1000] (mixed and large generators alternately), 128 ants
-    each, all served by the same four launches per iteration.  Instances are
-    sharded over ranks by estimated cost (cvrp_aco_ocl_b200.shard; no
-    collective on the data path).
-    Reports ant-tours/s over the whole batch and the roofline of the fused
-    pheromone pass, whose matrices (16 bytes per element over all instances)
-    far exceed L2."""
+def run_single(args, local):
+    from cvrp_aco_ocl_b200 import instances as I
+    r = run_one_instance(args, local, I.gen_mixed(SINGLE_SEED, SINGLE_CUST), SINGLE_ANTS, NN_ANTS, "single")
+    r["workload"] = (f"one instance, {SINGLE_CUST} customers (50% uniform, 50% 8 Gaussian clusters), "
+                     f"{SINGLE_ANTS} ants, {NN_ANTS}-NN lists, 2-opt on {NN_ANTS}-NN lists")
+    return r
+
+
+def run_large(args, local):
+    from cvrp_aco_ocl_b200 import instances as I
+    r = run_one_instance(args, local, I.gen_large(LARGE_SEED, LARGE_CUST), LARGE_ANTS, LARGE_K, "large")
+    r["workload"] = (f"one instance, {LARGE_CUST} customers (large generator), {LARGE_ANTS} ants, "
+                     f"{LARGE_K}-NN lists, 2-opt on {LARGE_K}-NN lists")
+    return r
+
+
+def run_parity(args, local):
+    """The reference's algorithm bit for bit: 50 customers (integer coordinates
+    in [0,100]^2, demand U{1..30}, capacity 160), 50 ants, alpha 1, beta 2,
+    rho 0.1, full-row I-Roulette with the reference's RNG stream (nloc 256),
+    2-opt on full neighbour lists, 800 iterations after init_aco (the
+    reference's algorithm itself breaks down at iteration 866 here, see
+    PARITY_ITERS).  Device time
+    of the iterations, end-to-end time through the C ABI (create, init,
+    iterations with per-iteration length readback, best tour), and the CPU
+    restatement of the reference's kernels (the oracle) timed on the host's
+    cores; the final state of both is compared bit for bit."""
     import torch
-    from cvrp_aco_ocl_b200 import MODE_THROUGHPUT, Batch, Problem, default_params
+
+    import oracle
+    from cvrp_aco_ocl_b200 import MODE_PARITY, Problem, Solver, default_params
     from cvrp_aco_ocl_b200 import instances as I
 
-    from cvrp_aco_ocl_b200.shard import shard_of
-
-    count_all = args.batch_count
-    every = I.gen_batch(BATCH_SEED, count_all, 100, 1000)
-    insts = [every[i] for i in shard_of([x.n for x in every], BATCH_ANTS, ws, rank)]
-    probs = [Problem.from_instance(x) for x in insts]
-    p = default_params(1001)
-    p.mode, p.n_ants, p.nn_ants, p.nn_ls, p.nloc = MODE_THROUGHPUT, BATCH_ANTS, NN_ANTS, NN_LS, NLOC
-    p.seed_time, p.rnd_seed, p.device, p.ls_flag = SEED_TIME, RND_SEED, local, 1
-    t0 = time.perf_counter()
-    B = Batch(probs, p)
-    B.init()
-    t_setup = time.perf_counter() - t0
-    count, total_ants = B.size()
-    for _ in range(max(3, args.batch_warmup)):
-        B.enqueue(1)
-    if B.status() != 0:
-        raise RuntimeError("batched warm-up failed")
-    dev = torch.device("cuda", local)
-    stream = torch.cuda.ExternalStream(B.stream(), device=dev)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.batch_steps)]
-    torch.cuda.synchronize()
-    for e0, e1 in evs:  # inputs (about 3 GB of matrices) exceed L2: no flush needed
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-        B.enqueue(1)
-        with torch.cuda.stream(stream):
-            e1.record(stream)
-    torch.cuda.synchronize()
-    if B.status() != 0:
-        raise RuntimeError("batched run failed")
-    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    tot = torch.tensor([float(total_ants)], device=dev, dtype=torch.float64)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    ms_max = float(t.item())
-    phase = B.time_phases(args.batch_steps)
-    launches = B.launches_per_iteration()  # the route-level 2-opt adds a kernel
-    B.close()
-    n_all = [pr.num_node for pr in probs]
-    row_bytes = sum(16 * n * n for n in n_all)
-    row_ms = float(phase[3]) / args.batch_steps
-    achieved = row_bytes / (row_ms / 1e3) / 1e9
-    return {
-        "workload": f"{count_all} independent instances, 100-1000 customers (seeded, mixed/large generators), "
-                    f"{BATCH_ANTS} ants each, {NN_ANTS}-NN lists, 2-opt on {NN_LS}-NN lists",
-        "value": float(tot.item()) * args.batch_steps / (ms_max / 1e3), "unit": UNIT,
-        "ms_per_step": ms_max / args.batch_steps, "steps": args.batch_steps, "instances_this_rank": count,
-        "ants_this_rank": total_ants, "setup_s": t_setup,
-        "gpu_launches": args.batch_steps * launches,
-        "kernel_share": {k: float(v) for k, v in zip(KERNELS, phase / phase.sum())},
-        "roofline": {"bound": "hbm", "kernel": "rows_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": profile_traffic("rows_kernel@batch"),
-                     "algorithmic_bytes_per_launch": row_bytes, "launch_ms": row_ms,
-                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
-                     "fallback 6.65 TB/s"},
-    }
-
-
-def run_e2e(args, rank, local):
-    """aco_create from host arrays (coordinates and demands copied host->device;
-    distances, NN lists and seeds computed there), aco_init, then per
-    step one iteration and a device->host read of its ant and best-so-far
-    lengths (pipelined: iteration k is queued before iteration k-1's lengths
-    are read), then the best tour read back: the reference's main.cpp loop
-    through the C ABI, timed by the host clock."""
-    import torch
-    from cvrp_aco_ocl_b200 import MODE_THROUGHPUT, Problem, Solver, default_params
-    from cvrp_aco_ocl_b200._lib import lib, ptr
-
-    inst = make_instance(rank)
+    inst = I.gen_uniform_small(PARITY_SEED, PARITY_CUST)
+    n, A = inst.n, PARITY_ANTS
     prob = Problem.from_instance(inst)
-    p = default_params(inst.n)
-    p.n_ants, p.nn_ants, p.nn_ls, p.nloc, p.mode = ANTS, NN_ANTS, NN_LS, NLOC, MODE_THROUGHPUT
-    p.seed_time, p.rnd_seed, p.device = SEED_TIME, RND_SEED + rank, local
-    lens = np.zeros(ANTS + 1, np.float32)
-    L = lib()
-    ticket = ctypes.c_longlong()
+
+    def params():
+        p = default_params(n)
+        p.n_ants, p.nloc, p.seed_time, p.rnd_seed, p.mode, p.device = A, NLOC, SEED_TIME, RND_SEED, MODE_PARITY, local
+        p.nn_ls, p.ls_flag = n - 2, 1
+        return p
+
+    S = Solver(prob, params())
+    S.init()
+    dev_ms = S.time_iterations(PARITY_ITERS)
+    sol, lens = S.solutions()
+    tau, tot = S.pheromone()
+    seeds = S.seeds()
+    _, best = S.best()
+    S.close()
+    # end to end
+    lens_buf = np.zeros(A + 1, np.float32)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    S = Solver(prob, p)
+    S = Solver(prob, params())
     S.init()
     prev = -1
-    for _ in range(args.steps):
-        # queue iteration k and the copy of its lengths, then read iteration k-1's:
-        # the GPU runs iteration k while the host reads
-        rc = L.aco_enqueue_iterations(S.h, 1) or L.aco_enqueue_lengths(S.h, ctypes.byref(ticket))
-        if rc == 0 and prev >= 0:
-            rc = L.aco_read_lengths(S.h, prev, ptr(lens), lens.size)
-        if rc != 0:
-            raise RuntimeError(rc)
-        prev = ticket.value
-    rc = L.aco_read_lengths(S.h, prev, ptr(lens), lens.size)
-    if rc != 0:
-        raise RuntimeError(rc)
-    tour, length = S.best()
-    t1 = time.perf_counter()
+    for _ in range(PARITY_ITERS):
+        S.enqueue(1)
+        tk = S.enqueue_lengths()
+        if prev >= 0:
+            S.read_lengths(prev, lens_buf)
+        prev = tk
+    S.read_lengths(prev, lens_buf)
+    S.best()
+    e2e_s = time.perf_counter() - t0
     S.close()
-    n = inst.n
-    # coordinates and demands, per-ant index tables and work items, argument blocks (about 1 KB); distances,
-    # lists and the ants' seeds are computed on the device
-    h2d = n * 4 * 3 + ANTS * 4 * 3 + 1024
-    d2h = (ANTS + 1) * 4 + 4  # lengths and the status word
-    return {"value": ANTS * args.steps / (t1 - t0), "unit": UNIT,
-            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h + (2 * n * 4 + 4) / args.steps,
-            "note": "create+init+iterations+readbacks, host wall clock"}
+    # the oracle: same seeds, same iterations
+    cores = os.cpu_count() or 1
+    dist = oracle.compute_distances(inst.x, inst.y)
+    nn = oracle.compute_nn_lists(dist, n - 2, n - 2)
+    sd, _ = oracle.make_seeds(SEED_TIME, RND_SEED, A, NLOC)
+    O = oracle.Oracle(dist, inst.demand, inst.capacity, A, NLOC, nn, sd, ls_flag=True, n_threads=cores)
+    O.init_aco()
+    c0 = time.perf_counter()
+    for _ in range(PARITY_ITERS):
+        O.run_iteration()
+    cpu_s = time.perf_counter() - c0
+    same = {"solutions": bool(np.array_equal(sol, O.solutions)), "lengths": bool(np.array_equal(lens, O.lens)),
+            "pheromone": bool(np.array_equal(tau, O.tau)), "total_info": bool(np.array_equal(tot, O.total)),
+            "seeds": bool(np.array_equal(seeds, O.seeds))}
+    if not all(same.values()):
+        print(f"bench: parity run differs from the oracle after {PARITY_ITERS} iterations: {same}", file=sys.stderr)
+    return {"workload": f"one instance, {PARITY_CUST} customers (integer coordinates in [0,100]^2, demand U{{1..30}}, "
+                        f"capacity 160), {A} ants, full-row I-Roulette with the reference's RNG stream (nloc {NLOC}), "
+                        f"2-opt on full lists, {PARITY_ITERS} iterations",
+            "value": A * PARITY_ITERS / (dev_ms / 1e3), "unit": UNIT, "ms_per_step": dev_ms / PARITY_ITERS,
+            "e2e": {"value": A * PARITY_ITERS / e2e_s, "unit": UNIT, "seconds": e2e_s},
+            "cpu_reference_port": {"value": A * PARITY_ITERS / cpu_s, "unit": UNIT, "cores": cores,
+                                   "seconds": cpu_s, "kind": "port (oracle/aco_oracle.c, kernel.cl restated)"},
+            "bit_exact_after_run": all(same.values()), "compared": same, "best_length": float(best)}
+
+
+def run_learned(args):
+    from cvrp_aco_ocl_b200 import learned_eval as LE
+    from cvrp_aco_ocl_b200 import prior as PR
+
+    scorer = PR.EdgeScorer.load(PR.DEFAULT_WEIGHTS)
+    t0 = time.perf_counter()
+    res = LE.time_to_equal_cost(scorer, LEARNED_N, args.learned_count, LEARNED_PLAIN_ITERS, LEARNED_ANTS, NN_ANTS)
+    res["seconds"] = time.perf_counter() - t0
+    res["workload"] = (f"{args.learned_count} held-out instances of {LEARNED_N - 1} customers (mixed and large "
+                       f"generators), {LEARNED_ANTS} ants, {NN_ANTS}-NN candidate lists in both arms, plain = "
+                       f"{LEARNED_PLAIN_ITERS} iterations; learned wall time includes graph build, network forward "
+                       f"and prior upload")
+    res["gate"] = "median ratio <= 0.5"
+    return res
 
 
 # --------------------------------------------------------------------------
-def oracle_run(n_threads: int, warmup: int, steps: int, max_seconds: float):
+def oracle_batch_run(n_threads: int, warmup: int, steps: int, max_seconds: float):
+    """The CPU port of the path (oracle/aco_oracle.c) on a stratified sample of
+    rank 0's batch: every 16th instance by size (32 of 512, 100-1000 customers),
+    with the same parameters and per-instance seeds as on the GPU; after
+    init_aco, `warmup` iterations, then `steps` timed iterations (the GPU arm's
+    offsets), each iteration over every sampled instance.  Threads split each
+    instance's ants."""
     import oracle
 
-    inst = make_instance(0)
-    dist = oracle.compute_distances(inst.x, inst.y)
-    nn = oracle.compute_nn_lists(dist, NN_LS, NN_ANTS)
-    seeds, _ = oracle.make_seeds(SEED_TIME, RND_SEED, ANTS, NLOC)
-    O = oracle.Oracle(dist, inst.demand, inst.capacity, ANTS, NLOC, nn, seeds, ls_flag=True, nn_ants_list=nn,
-                      n_threads=n_threads)
-    O.init_aco(throughput=True)
+    insts, _ = batch_workload(1, 0)
+    order = sorted(range(len(insts)), key=lambda i: (insts[i].n, i))
+    picked = order[::CPU_SAMPLE_STRIDE]
+    colonies = []
+    for b in picked:
+        inst = insts[b]
+        d = oracle.compute_distances(inst.x, inst.y)
+        k = min(NN_ANTS, inst.n - 2)
+        nn = oracle.compute_nn_lists(d, min(NN_LS, inst.n - 2), k)
+        seeds, _ = oracle.make_seeds(SEED_TIME, RND_SEED + b, BATCH_ANTS, NLOC)
+        O = oracle.Oracle(d, inst.demand, inst.capacity, BATCH_ANTS, NLOC, nn, seeds, ls_flag=True,
+                          nn_ants_list=nn, n_threads=n_threads)
+        O.init_aco(throughput=True)
+        colonies.append(O)
     for _ in range(warmup):
-        O.run_iteration(throughput=True)
+        for O in colonies:
+            O.run_iteration(throughput=True)
     done = 0
     t0 = time.perf_counter()
     while done < steps:
-        O.run_iteration(throughput=True)
+        for O in colonies:
+            O.run_iteration(throughput=True)
         done += 1
         if time.perf_counter() - t0 > max_seconds:
             break
     dt = time.perf_counter() - t0
-    return ANTS * done / dt, done, dt
-
-
-def cpu_baseline(seconds: float = 15.0):
-    cores = os.cpu_count() or 1
-    value, done, dt = oracle_run(cores, 1, 10**9, seconds)
-    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{done} iterations of the same workload ({done * ANTS} ant-tours) in {dt:.1f} s, "
-                      f"CPU port of the path (oracle/aco_oracle.c), {cores} threads over ants"}
+    ants = BATCH_ANTS * len(colonies)
+    sample = (f"{len(colonies)} of the batch's {len(insts)} instances (every {CPU_SAMPLE_STRIDE}th by size, "
+              f"{insts[picked[0]].n}-{insts[picked[-1]].n} nodes), iterations {warmup + 1}-{warmup + done} after "
+              f"init ({done * ants} ant-tours) in {dt:.1f} s, {n_threads} threads over each instance's ants")
+    return ants * done / dt, done, dt, sample
 
 
 def run_reference(args, ws, rank):
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    value, done, dt = oracle_run(cores, args.warmup, args.steps, max_seconds=240.0)
+    value, done, dt, sample = oracle_batch_run(cores, args.warmup, args.steps, max_seconds=240.0)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": ws, "steps": done,
             "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(done, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
-            "config": {"workload": WORKLOAD, "n_nodes": N_CUST + 1, "ants": ANTS, "nn_ants": NN_ANTS,
-                       "nn_ls": NN_LS, "mode": "throughput", "ras_ranks": 6},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{done} iterations ({done * ANTS} ant-tours) in {dt:.1f} s"},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, no dataset)",
+            "config": config(ws),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
 def main():
+    global BATCH_COUNT
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload section")
-    ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=120.0, help="bound on the timed CPU iterations")
+    ap.add_argument("--no-extras", action="store_true", help="only the headline batch (profiling captures)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain section")
+    ap.add_argument("--learned-count", type=int, default=LEARNED_COUNT)
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT,
-                    help="instances of the batched section (smaller counts for profiling captures)")
-    ap.add_argument("--only-batched", action="store_true",
-                    help="run the batched section alone and print it as the line")
-    ap.add_argument("--batch-warmup", type=int, default=3)
+                    help="instances per GPU of the headline batch (smaller counts for profiling captures)")
     args = ap.parse_args()
-    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    BATCH_COUNT = args.batch_count
+    if args.impl == "ours":
+        args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, ws, rank)
-        return
-    if args.only_batched:
-        import torch
-        torch.cuda.set_device(local)
-        peak, peak_kind = load_peaks()
-        line = run_batched(args, 1, 0, local, peak, peak_kind)
-        print(json.dumps(line, default=float))
         return
     run_ours(args, ws, rank, local)
 

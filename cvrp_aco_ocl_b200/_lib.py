@@ -39,6 +39,8 @@ EXPORTED = [
     "aco_last_cuda_error", "aco_compute_distances_device", "aco_compute_nn_lists_device", "aco_validate",
     "aco_write_solution", "aco_batch_validate", "aco_batch_write_solutions", "aco_batch_get_bsf_records",
     "aco_save_checkpoint", "aco_load_checkpoint", "aco_batch_save_checkpoint", "aco_batch_load_checkpoint",
+    "aco_batch_enqueue_lengths", "aco_batch_read_lengths", "aco_batch_get_best_all", "aco_clear_status",
+    "aco_set_wait_limit",
 ]
 
 
@@ -68,7 +70,7 @@ class AcoParams(ctypes.Structure):
         ("ns_rounds", ctypes.c_int),
         ("ls_ants", ctypes.c_int),
         ("draw_warps", ctypes.c_int),
-        ("route_ls", ctypes.c_int),
+        ("route_ls", ctypes.c_int), ("wait_limit", ctypes.c_int),
     ]
 
 
@@ -164,6 +166,11 @@ def lib() -> ctypes.CDLL:
                      "aco_batch_load_checkpoint"):
             getattr(L, name).argtypes = [vp, ctypes.c_char_p]
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
+        L.aco_batch_enqueue_lengths.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.aco_batch_read_lengths.argtypes = [vp, ctypes.c_longlong, vp, ctypes.c_size_t]
+        L.aco_batch_get_best_all.argtypes = [vp, vp, ctypes.c_size_t, vp, vp]
+        L.aco_clear_status.argtypes = [vp]
+        L.aco_set_wait_limit.argtypes = [vp, ip]
         _lib = L
     return _lib
 

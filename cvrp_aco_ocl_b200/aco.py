@@ -327,6 +327,14 @@ class Solver:
     def status(self) -> int:
         return lib().aco_status(self.h)
 
+    def clear_status(self) -> int:
+        """The sticky device status, then reset to ACO_OK."""
+        return lib().aco_clear_status(self.h)
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls before a device wait gives up (0 = the default)."""
+        check(lib().aco_set_wait_limit(self.h, polls), "aco_set_wait_limit")
+
     def stream(self) -> int:
         return lib().aco_get_stream(self.h)
 
@@ -428,6 +436,41 @@ class Batch:
         check(lib().aco_batch_get_best(self.h, b, ptr(buf), T, ctypes.byref(size), ctypes.byref(length)),
               "aco_batch_get_best")
         return buf[: size.value].copy(), length.value
+
+    def ants_of(self, b: int) -> int:
+        return self.A if self.A > 0 else self.problems[b].num_node  # n_ants = 0: one ant per node
+
+    def lengths_total(self) -> int:
+        """Floats one lengths readback holds: every instance's ants and best-so-far."""
+        return sum(self.ants_of(b) + 1 for b in range(len(self.problems)))
+
+    def enqueue_lengths(self) -> int:
+        """Queue a copy of every instance's lengths as the stream stands; returns its ticket."""
+        t = ctypes.c_longlong()
+        check(lib().aco_batch_enqueue_lengths(self.h, ctypes.byref(t)), "aco_batch_enqueue_lengths")
+        return t.value
+
+    def read_lengths(self, ticket: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Wait for a queued copy: instance b's A_b + 1 lengths (ants, best-so-far)
+        follow those of instances 0..b-1."""
+        if out is None:
+            out = np.zeros(self.lengths_total(), np.float32)
+        check(lib().aco_batch_read_lengths(self.h, ticket, ptr(out), out.size), "aco_batch_read_lengths")
+        return out
+
+    def best_all(self) -> Tuple[List[np.ndarray], np.ndarray]:
+        """Every instance's best-so-far tour and length in one transfer."""
+        Ts = [2 * p.num_node for p in self.problems]
+        tours = np.zeros(sum(Ts), np.int32)
+        sizes = np.zeros(len(Ts), np.int32)
+        lens = np.zeros(len(Ts), np.float32)
+        check(lib().aco_batch_get_best_all(self.h, ptr(tours), tours.size, ptr(sizes), ptr(lens)),
+              "aco_batch_get_best_all")
+        out, off = [], 0
+        for T, s in zip(Ts, sizes):
+            out.append(tours[off:off + s].copy())
+            off += T
+        return out, lens
 
     def solutions(self, b: int) -> Tuple[np.ndarray, np.ndarray]:
         T = 2 * self.problems[b].num_node

@@ -140,19 +140,37 @@ __device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, uint32_
                  : "memory");
 }
 
-// Bounded wait on phase `parity` of `bar`.  Returns false after ~`limit`
-// polls (the caller reports ACO_ERR_TIMEOUT); never spins forever.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit = 1u << 24)
+constexpr uint32_t kWaitPolls = 1u << 24; // default poll limit of a bounded wait (about a second)
+
+// The poll limit a kernel was given (a device word; <= 0 or null: the default).
+__device__ __forceinline__ uint32_t wait_polls(const int *limit)
+{
+    const int v = limit ? *limit : 0;
+    return v > 0 ? (uint32_t)v : kWaitPolls;
+}
+
+// Bounded wait on phase `parity` of `bar`.  Returns false after `limit` polls
+// (the caller reports ACO_ERR_TIMEOUT); never spins forever.  The first poll
+// does not block (test_wait), the later ones may suspend briefly (try_wait).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit = kWaitPolls)
 {
     const uint32_t addr = smem_u32(bar);
     for (uint32_t it = 0; it < limit; it++) {
         uint32_t done;
-        asm volatile("{\n\t.reg .pred p;\n\t"
-                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                     "selp.u32 %0, 1, 0, p;\n\t}"
-                     : "=r"(done)
-                     : "r"(addr), "r"(parity)
-                     : "memory");
+        if (it == 0)
+            asm volatile("{\n\t.reg .pred p;\n\t"
+                         "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                         "selp.u32 %0, 1, 0, p;\n\t}"
+                         : "=r"(done)
+                         : "r"(addr), "r"(parity)
+                         : "memory");
+        else
+            asm volatile("{\n\t.reg .pred p;\n\t"
+                         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                         "selp.u32 %0, 1, 0, p;\n\t}"
+                         : "=r"(done)
+                         : "r"(addr), "r"(parity)
+                         : "memory");
         if (done) return true;
         if (it > 64) __nanosleep(64);
     }

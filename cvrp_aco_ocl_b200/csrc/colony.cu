@@ -289,7 +289,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         return o;
     };
     struct Offs {
-        size_t dist, heur, tau, total, chc, dem, key, jump, adv, cand32, nn16, nnls, seeds, sol, lens, elites, succ,
+        size_t dist, heur, tau, total, chc, dem, key, jump, adv, cand32, nn16, nnls, seeds, sol, elites, succ,
             dep, dtau, rec, nbsf, iter, xy, nnfull;
     };
     std::vector<Offs> offs(count);
@@ -308,7 +308,6 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         o.nnls = take((size_t)ih.n * std::max(1, ih.nn_ls) * 4);
         o.seeds = take((size_t)ih.A * ih.nloc * 4);
         o.sol = take(((size_t)ih.T * (ih.A + 1) + 1) * 4);
-        o.lens = take(((size_t)ih.A + 1) * 4);
         o.elites = take((size_t)ih.R * 4);
         o.succ = take((size_t)ih.R * ih.n * 4);
         o.dep = take((size_t)ih.n * 4);
@@ -320,14 +319,23 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         o.nnfull = ih.device_prep ? take((size_t)ih.n * std::max(1, ih.depth) * 4) : 0;
     }
     const size_t o_status = take(4), o_t0 = take(8), o_queue = take(8); // construct queue: next item, CTAs done
+    const size_t o_wait = take(4); // poll limit of the device waits
     total_ants = 0;
     total_rows = 0;
     ld_max = 32;
-    for (const InstHost &ih : inst) {
+    slot_base_h_.assign(count + 1, 0); // the lengths of all instances: one contiguous block
+    tour_base_h_.assign(count + 1, 0); // the packed best-so-far tours of get_best_all
+    for (int b = 0; b < count; b++) {
+        const InstHost &ih = inst[b];
         total_ants += ih.A;
         total_rows += ih.n;
         ld_max = std::max(ld_max, ih.ld);
+        slot_base_h_[b + 1] = slot_base_h_[b] + ih.A + 1;
+        tour_base_h_[b + 1] = tour_base_h_[b] + ih.T;
     }
+    const size_t o_lens_all = take((size_t)slot_base_h_[count] * 4);
+    const size_t o_tour_base = take((size_t)(count + 1) * 4), o_best_tours = take((size_t)tour_base_h_[count] * 4);
+    const size_t o_best_sizes = take((size_t)count * 4), o_best_lens = take((size_t)count * 4);
     const size_t o_ant_inst = take((size_t)total_ants * 4), o_ant_base = take((size_t)(count + 1) * 4);
     const size_t o_row_base = take((size_t)(count + 1) * 4), o_zero_base = take(16);
     const size_t o_slot_base = take((size_t)(count + 1) * 4), o_valid = take((size_t)(total_ants + count) * 4);
@@ -387,7 +395,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         ih.adv_d = (uint32_t *)(base + o.adv); ih.cand32_d = (uint32_t *)(base + o.cand32);
         ih.nn16_d = (uint16_t *)(base + o.nn16); ih.nnls_d = (int *)(base + o.nnls);
         ih.seeds_d = (int *)(base + o.seeds); ih.sol_d = (int *)(base + o.sol);
-        ih.lens_d = (float *)(base + o.lens); ih.elites_d = (int *)(base + o.elites);
+        ih.lens_d = (float *)(base + o_lens_all) + slot_base_h_[b]; ih.elites_d = (int *)(base + o.elites);
         ih.succ_d = (int *)(base + o.succ); ih.dep_d = (uint32_t *)(base + o.dep);
         ih.dtau_d = (float *)(base + o.dtau); ih.rec_d = (aco_record *)(base + o.rec);
         ih.nbsf_d = (int *)(base + o.nbsf); ih.iter_d = (int *)(base + o.iter);
@@ -397,6 +405,12 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         }
     }
     status_d = (int *)(base + o_status);
+    wait_d = (int *)(base + o_wait);
+    lens_all_d_ = (float *)(base + o_lens_all);
+    tour_base_d_ = (int *)(base + o_tour_base);
+    best_tours_d_ = (int *)(base + o_best_tours);
+    best_sizes_d_ = (int *)(base + o_best_sizes);
+    best_lens_d_ = (float *)(base + o_best_lens);
     t0_d_ = (unsigned long long *)(base + o_t0);
     queue_d_ = (int *)(base + o_queue);
     ant_inst_d_ = (int *)(base + o_ant_inst);
@@ -671,6 +685,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         c.route_rem = route_rem_d_;
         c.route_cap = route_cap_;
         c.seeds = ih.seeds_d; c.solutions = ih.sol_d; c.lens = ih.lens_d; c.status = status_d;
+        c.wait_limit = wait_d;
         LocalSearchArgs &l = largs[b];
         l = LocalSearchArgs{};
         l.n = n; l.ld = ih.ld; l.n_ants = ih.A; l.T = ih.T; l.nn_ls = ih.nn_ls; l.rmax = 32;
@@ -697,9 +712,10 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     up(ant_inst_d_, ant_inst.data(), ant_inst.size() * 4);
     up(ant_base_d_, ant_base.data(), ant_base.size() * 4);
     up(row_base_d_, row_base.data(), row_base.size() * 4);
-    slot_base_h_.assign(count + 1, 0);
-    for (int b = 0; b < count; b++) slot_base_h_[b + 1] = slot_base_h_[b] + inst[b].A + 1;
     up(slot_base_d_, slot_base_h_.data(), slot_base_h_.size() * 4);
+    up(tour_base_d_, tour_base_h_.data(), tour_base_h_.size() * 4);
+    const int wl = std::max(0, p.wait_limit);
+    up(wait_d, &wl, 4);
     up(items_d_, items.data(), items.size() * sizeof(int2));
     up(sw_items_d_, swi.data(), swi.size() * sizeof(int2));
     up(ns_items_d_, nsi.data(), nsi.size() * sizeof(int2));
@@ -778,6 +794,19 @@ int Colony::validate(int *flags, int *invalid_per_inst, int *n_invalid)
         if (invalid_per_inst) invalid_per_inst[b] = inv[b];
     }
     if (n_invalid) *n_invalid = (int)total;
+    return sync_status();
+}
+
+int Colony::get_best_all(int *tours, size_t cap_ints, int *sizes, float *lengths)
+{
+    const int count = (int)inst.size();
+    if (tours && cap_ints < (size_t)tour_base_h_[count]) return ACO_ERR_CAPACITY;
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    CK(launch_gather_best(cargs_d_, count, tour_base_d_, best_tours_d_, best_sizes_d_, best_lens_d_, st));
+    if (tours) CK(cudaMemcpyAsync(tours, best_tours_d_, sizeof(int) * tour_base_h_[count], cudaMemcpyDeviceToHost, st));
+    if (sizes) CK(cudaMemcpyAsync(sizes, best_sizes_d_, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+    if (lengths) CK(cudaMemcpyAsync(lengths, best_lens_d_, sizeof(float) * count, cudaMemcpyDeviceToHost, st));
     return sync_status();
 }
 
@@ -973,6 +1002,28 @@ int Colony::launches_per_iteration() const
     if (p.ls_flag) k += 1 + (use_routes_ && cn_lsw == 0 ? 1 : 0) + ((p.ls_flag & 2) ? 1 : 0); // 2-opt kernels, swap
     if (p.ns_rounds > 0) k += 1;
     return k;
+}
+
+int Colony::set_wait_limit(int polls)
+{
+    if (polls < 0) return ACO_ERR_INVALID;
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    h_pin[3] = polls; // pinned: the copy is ordered on the stream, the word read by the next launch
+    CK(cudaMemcpyAsync(wait_d, h_pin + 3, sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    p.wait_limit = polls;
+    return ACO_OK;
+}
+
+int Colony::clear_status()
+{
+    int rc = set_device();
+    if (rc != ACO_OK) return rc;
+    const int prev = sync_status();
+    CK(cudaMemsetAsync(status_d, 0, sizeof(int), st));
+    CK(cudaStreamSynchronize(st));
+    return prev;
 }
 
 int Colony::sync_status()

@@ -64,6 +64,8 @@ public:
     int init();                  // g_ACO::init_aco for every instance
     int enqueue(int n_iter);     // n_iter iterations (graph replays), no sync
     int sync_status();           // wait for the stream, read the sticky status
+    int clear_status();          // sync_status, then reset the sticky status to ACO_OK
+    int set_wait_limit(int polls); // poll limit of the device waits (0 = default), from the next launch
     int launches_per_iteration() const; // kernel launches of one iteration (graph nodes)
     int construct(bool fused = false); // fused: with the 2-opt warps when configured
     int local_search();
@@ -85,6 +87,14 @@ public:
     int load_checkpoint(const char *path);
     int time_phases(int n_iter, float *ms4);
     int set_device() const;
+    // Every instance's best-so-far tour (2n ints at the prefix sum of 2n),
+    // size and length, gathered on the device and copied in one transfer.
+    int get_best_all(int *tours, size_t cap_ints, int *sizes, float *lengths);
+    // All instances' lengths are one contiguous block: instance b's A+1 floats
+    // (ants, then best-so-far) start at lens_base()[b].
+    const float *lens_all() const { return lens_all_d_; }
+    int lens_total() const { return slot_base_h_.empty() ? 0 : slot_base_h_.back(); }
+    int tours_total() const { return tour_base_h_.empty() ? 0 : tour_base_h_.back(); }
 
     aco_params p{};
     int dev = 0, sm_count = 148;
@@ -94,6 +104,7 @@ public:
     std::chrono::steady_clock::time_point t_init;
     int *h_pin = nullptr;
     int *status_d = nullptr;
+    int *wait_d = nullptr;       // poll limit the construct kernels read at every launch
 
     // launch configuration
     int cp_wpa = 1, cp_apc = 1;
@@ -132,7 +143,10 @@ private:
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
     int *row_base_d_ = nullptr, *zero_base_d_ = nullptr;
     int *slot_base_d_ = nullptr, *valid_d_ = nullptr, *invalid_d_ = nullptr;
-    std::vector<int> slot_base_h_;
+    std::vector<int> slot_base_h_, tour_base_h_;
+    float *lens_all_d_ = nullptr;
+    int *tour_base_d_ = nullptr, *best_tours_d_ = nullptr, *best_sizes_d_ = nullptr;
+    float *best_lens_d_ = nullptr;
     ConstructArgs *cargs_d_ = nullptr;
     LocalSearchArgs *largs_d_ = nullptr;
     StatsArgs *sargs_d_ = nullptr;

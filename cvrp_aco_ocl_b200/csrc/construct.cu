@@ -105,8 +105,8 @@ __global__ void __launch_bounds__(512) construct_parity_kernel(ConstructArgs a)
         for (int r = threadIdx.x; r < n; r += blockDim.x)
             tma_bulk_g2s(s_mat + (size_t)r * n4, a.total + (size_t)r * ld, n4 * 4, bar);
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_d0[i] = a.dist[(size_t)i * ld]; // column 0
-    const bool ok = mbar_wait(bar, 0);
-    if (__syncthreads_or(!ok)) {
+    const bool ok = mbar_wait(bar, 0, wait_polls(a.wait_limit));
+    if (__syncthreads_or(!ok)) { // give up, but let the copies in flight land first (default bound)
         if (threadIdx.x == 0) set_status(a.status, ACO_ERR_TIMEOUT);
         if (!ok) mbar_wait(bar, 0);
         return;
@@ -599,8 +599,8 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
     if (helper) hx = draw_chunk(pm_norm(a.seeds[(size_t)(ant0 + warp - apc) * a.nloc + lane]), ring, lane);
     // an ant warp's Park-Miller states, loaded while the tables are staged
     const int seed0 = warp < apc && ant0 + warp < a.n_ants ? a.seeds[(size_t)(ant0 + warp) * a.nloc + lane] : 0;
-    const bool ok = mbar_wait(bar, phase);
-    if (__syncthreads_or(!ok)) {
+    const bool ok = mbar_wait(bar, phase, wait_polls(a.wait_limit));
+    if (__syncthreads_or(!ok)) { // give up, but let the copies in flight land first (default bound)
         if (threadIdx.x == 0) set_status(a.status, ACO_ERR_TIMEOUT);
         if (!ok) mbar_wait(bar, phase);
         return false;

@@ -59,6 +59,7 @@ struct ConstructArgs {
     int *solutions;
     float *lens;
     int *status;
+    const int *wait_limit; // polls before a staging wait gives up (device word; <= 0: the default)
 };
 
 struct LocalSearchArgs {
@@ -182,6 +183,10 @@ int local_search_occupancy(int warps, size_t smem);
 // exact; invalid[b] counts the others (zeroed by the caller).
 cudaError_t launch_validate(const ConstructArgs *d_args, int n_inst, int max_slots, int max_n, int *flags,
                             const int *slot_base, int *invalid, cudaStream_t st);
+// The best-so-far tour, size and length of every instance, packed (validate.cu):
+// instance b's 2n ints at tours + tour_base[b], sizes[b], lens[b].
+cudaError_t launch_gather_best(const ConstructArgs *d_args, int n_inst, const int *d_tour_base, int *tours,
+                               int *sizes, float *lens, cudaStream_t st);
 
 // Inter-route swap stage (swap.cu): one CTA per item {instance, first ant}
 // with `apc` ants (one warp each).

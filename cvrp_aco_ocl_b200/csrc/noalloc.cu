@@ -15,6 +15,12 @@
 // array (it keeps the last call's contents; each call re-initialises what it
 // reads), so calls that overlap on the GPU -- on different streams, or from
 // different threads -- race and must be serialised by the caller.
+//
+// The elite tours come from the caller's buffers, so they are checked before
+// any scratch write: an elite whose tour size lies outside [2, 2n-1] or that
+// holds a node id outside [0, n) deposits nothing, and its elites_out entry
+// reads ACO_ERR_INVALID instead of the ant id.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -38,9 +44,13 @@ struct NoAllocScratch {
 // The scratch: 148 KB of device memory in the library image, no allocation.
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-// Device address of g_noalloc_scratch per device, looked up once per device.
+// Device address of g_noalloc_scratch per device, looked up once per device and
+// context: a context that is destroyed and created again (cudaDeviceReset) may
+// load the module at another address, so the cached address is keyed on the
+// context it was looked up in.
 std::mutex g_scratch_mu;
 NoAllocScratch *g_scratch_ptr[64] = {};
+CUcontext g_scratch_ctx[64] = {};
 
 __device__ __forceinline__ unsigned long long block_min_key(unsigned long long v, unsigned long long *red)
 {
@@ -89,12 +99,32 @@ __global__ void __launch_bounds__(1024) noalloc_deposit_list_kernel(NoAllocScrat
     }
     for (int e = tid; e < ras_ranks * n; e += bs) sc->succ[e] = -1; // clear what the last call left
     for (int e = tid; e < n; e += bs) sc->depmask[e] = 0u;
+    // Check every elite tour before it is read as indices: size in [2, T-1],
+    // every node id in [0, n).  A failing elite deposits nothing (d_tau = 0 and
+    // no list entries) and is reported as ACO_ERR_INVALID.
+    __shared__ int s_bad[kMaxRanks];
+    if (tid < ras_ranks) s_bad[tid] = 0;
+    __syncthreads();
+    for (int r = 0; r < ras_ranks; r++) {
+        const int *tour = solutions + (size_t)T * sc->elites[r];
+        const int size = tour[T - 1];
+        if (size < 2 || size > T - 1) {
+            if (tid == 0) s_bad[r] = 1;
+            continue;
+        }
+        for (int k = tid; k < size; k += bs) {
+            const int u = tour[k];
+            if (u < 0 || u >= n) s_bad[r] = 1;
+        }
+    }
     __syncthreads();
     if (tid < ras_ranks) {
-        sc->d_tau[tid] = __fdiv_rn((float)(ras_ranks - tid), lens[sc->elites[tid]]);
-        if (elites_out) elites_out[tid] = sc->elites[tid];
+        const bool bad = s_bad[tid] != 0;
+        sc->d_tau[tid] = bad ? 0.0f : __fdiv_rn((float)(ras_ranks - tid), lens[sc->elites[tid]]);
+        if (elites_out) elites_out[tid] = bad ? ACO_ERR_INVALID : sc->elites[tid];
     }
     for (int r = 0; r < ras_ranks; r++) {
+        if (s_bad[r]) continue;
         const int *tour = solutions + (size_t)T * sc->elites[r];
         const int size = tour[T - 1];
         for (int k = tid; k < size - 1; k += bs) {
@@ -137,17 +167,40 @@ int exp_int(float e)
     return -1;
 }
 
-// Set-up, once per device with that device current: the device address of the
-// scratch array (its host-side name is only a stand-in, not a device address).
+// Set-up, once per device and context, with that device current: the device
+// address of the scratch array (its host-side name is only a stand-in, not a
+// device address).  The current context comes from the driver's
+// cuCtxGetCurrent, reached through cudaGetDriverEntryPoint so the library
+// needs no link against libcuda.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+
+CtxGetCurrentFn ctx_get_current()
+{
+    static CtxGetCurrentFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    return fn;
+}
+
 int scratch_address(NoAllocScratch **out)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ACO_ERR_CUDA;
+    const CtxGetCurrentFn get = ctx_get_current();
+    CUcontext ctx = nullptr; // null until the runtime has made the device's primary context current
+    if (!get || get(&ctx) != CUDA_SUCCESS) return ACO_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
+    if (ctx == nullptr || !g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
+        void *p = nullptr; // the lookup also initialises the primary context when needed
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return ACO_ERR_CUDA;
+        if (ctx == nullptr && (get(&ctx) != CUDA_SUCCESS || ctx == nullptr)) return ACO_ERR_CUDA;
         g_scratch_ptr[dev] = static_cast<NoAllocScratch *>(p);
+        g_scratch_ctx[dev] = ctx;
     }
     *out = g_scratch_ptr[dev];
     return ACO_OK;

@@ -36,26 +36,35 @@ using namespace aco;
 // iteration before waiting for the lengths of the previous one.
 constexpr int kLenSlots = 4;
 
+// The ring of one colony: slot k holds `words` lengths and the status word.
+struct LenRing {
+    float *ring = nullptr;
+    int words = 0;
+    cudaEvent_t ev[kLenSlots] = {};
+    long long ticket[kLenSlots] = {-1, -1, -1, -1};
+    long long next = 0;
+    void release(Colony &c)
+    {
+        if (!ring) return;
+        c.set_device();
+        cudaStreamSynchronize(c.st);
+        for (int k = 0; k < kLenSlots; k++)
+            if (ev[k]) cudaEventDestroy(ev[k]);
+        cudaFreeHost(ring);
+        ring = nullptr;
+    }
+};
+
 struct aco_solver {
     Colony c;
-    float *len_ring = nullptr; // kLenSlots x (A + 2) pinned words: A + 1 lengths, the status word
-    cudaEvent_t len_ev[kLenSlots] = {};
-    long long len_ticket[kLenSlots] = {-1, -1, -1, -1};
-    long long next_ticket = 0;
-    ~aco_solver()
-    {
-        if (len_ring) {
-            c.set_device();
-            cudaStreamSynchronize(c.st);
-            for (int k = 0; k < kLenSlots; k++)
-                if (len_ev[k]) cudaEventDestroy(len_ev[k]);
-            cudaFreeHost(len_ring);
-        }
-    }
+    LenRing lr; // A + 1 lengths per slot
+    ~aco_solver() { lr.release(c); }
 };
 
 struct aco_batch {
     Colony c;
+    LenRing lr; // every instance's A + 1 lengths per slot (the colony's contiguous block)
+    ~aco_batch() { lr.release(c); }
 };
 
 namespace {
@@ -91,6 +100,7 @@ int check_params(const aco_params &p, int n)
     if (p.ls_ants < 0 || p.ls_ants > 8) return ACO_ERR_INVALID;
     if (p.draw_warps < -1 || p.draw_warps > 1) return ACO_ERR_INVALID;
     if (p.route_ls < -1 || p.route_ls > 1) return ACO_ERR_INVALID;
+    if (p.wait_limit < 0) return ACO_ERR_INVALID;
     if (!(p.rho > 0.0f && p.rho <= 1.0f)) return ACO_ERR_INVALID;
     if (p.n_ants > 56 * 1024) return ACO_ERR_INVALID; // the statistics kernel holds n_ants lengths in shared memory
     return ACO_OK;
@@ -348,54 +358,87 @@ int aco_iterate(aco_solver *s, int n_iter)
     return run_sync(s->c, s->c.enqueue(n_iter));
 }
 
+int aco_clear_status(aco_solver *s) { return s ? s->c.clear_status() : ACO_ERR_INVALID; }
+
+int aco_set_wait_limit(aco_solver *s, int polls) { return s ? s->c.set_wait_limit(polls) : ACO_ERR_INVALID; }
+
 int aco_enqueue_iterations(aco_solver *s, int n_iter)
 {
     if (!s || n_iter < 0) return ACO_ERR_INVALID;
     return s->c.enqueue(n_iter);
 }
 
+namespace {
+// Queue a copy of `words` floats from `src` (and the status word) into the
+// next ring slot; the ticket names the slot's copy.
+int ring_enqueue(Colony &c, LenRing &lr, const float *src, int words, long long *ticket)
+{
+    if (!c.initialized) return ACO_ERR_STATE;
+    if (c.set_device() != ACO_OK) return ACO_ERR_CUDA;
+    if (!lr.ring) { // first use: the ring and its events
+        if (cudaMallocHost(&lr.ring, sizeof(float) * (size_t)(words + 1) * kLenSlots) != cudaSuccess) {
+            lr.ring = nullptr;
+            return ACO_ERR_NOMEM;
+        }
+        lr.words = words;
+        for (int k = 0; k < kLenSlots; k++) CK(cudaEventCreateWithFlags(&lr.ev[k], cudaEventDisableTiming));
+    }
+    const long long t = lr.next;
+    const int slot = (int)(t % kLenSlots);
+    float *dst = lr.ring + (size_t)slot * (words + 1);
+    CK(cudaMemcpyAsync(dst, src, sizeof(float) * words, cudaMemcpyDeviceToHost, c.st));
+    CK(cudaMemcpyAsync(dst + words, c.status_d, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+    CK(cudaEventRecord(lr.ev[slot], c.st));
+    lr.ticket[slot] = t;
+    lr.next = t + 1;
+    *ticket = t;
+    return ACO_OK;
+}
+
+int ring_read(Colony &c, LenRing &lr, long long ticket, float *lens, size_t cap)
+{
+    const int slot = (int)(ticket % kLenSlots);
+    if (!lr.ring || lr.ticket[slot] != ticket) return ACO_ERR_STATE; // never queued, or overwritten
+    if (cap < (size_t)lr.words) return ACO_ERR_CAPACITY;
+    if (c.set_device() != ACO_OK) return ACO_ERR_CUDA;
+    CK(cudaEventSynchronize(lr.ev[slot]));
+    const float *src = lr.ring + (size_t)slot * (lr.words + 1);
+    std::memcpy(lens, src, sizeof(float) * lr.words);
+    int status;
+    std::memcpy(&status, src + lr.words, sizeof(int));
+    return status; // the device status word when the copy was queued
+}
+} // namespace
+
 int aco_enqueue_lengths(aco_solver *s, long long *ticket)
 {
     if (!s || !ticket) return ACO_ERR_INVALID;
-    Colony &c = s->c;
-    if (!c.initialized) return ACO_ERR_STATE;
-    if (c.set_device() != ACO_OK) return ACO_ERR_CUDA;
-    const int A = c.inst[0].A;
-    if (!s->len_ring) { // first use: the ring and its events
-        if (cudaMallocHost(&s->len_ring, sizeof(float) * (size_t)(A + 2) * kLenSlots) != cudaSuccess) {
-            s->len_ring = nullptr;
-            return ACO_ERR_NOMEM;
-        }
-        for (int k = 0; k < kLenSlots; k++)
-            CK(cudaEventCreateWithFlags(&s->len_ev[k], cudaEventDisableTiming));
-    }
-    const long long t = s->next_ticket;
-    const int slot = (int)(t % kLenSlots);
-    float *dst = s->len_ring + (size_t)slot * (A + 2);
-    CK(cudaMemcpyAsync(dst, c.inst[0].lens_d, sizeof(float) * (A + 1), cudaMemcpyDeviceToHost, c.st));
-    CK(cudaMemcpyAsync(dst + A + 1, c.status_d, sizeof(int), cudaMemcpyDeviceToHost, c.st));
-    CK(cudaEventRecord(s->len_ev[slot], c.st));
-    s->len_ticket[slot] = t;
-    s->next_ticket = t + 1;
-    *ticket = t;
-    return ACO_OK;
+    return ring_enqueue(s->c, s->lr, s->c.inst[0].lens_d, s->c.inst[0].A + 1, ticket);
 }
 
 int aco_read_lengths(aco_solver *s, long long ticket, float *lens, size_t cap)
 {
     if (!s || !lens || ticket < 0) return ACO_ERR_INVALID;
-    Colony &c = s->c;
-    const int slot = (int)(ticket % kLenSlots);
-    if (!s->len_ring || s->len_ticket[slot] != ticket) return ACO_ERR_STATE; // never queued, or overwritten
-    const int A = c.inst[0].A;
-    if (cap < (size_t)(A + 1)) return ACO_ERR_CAPACITY;
-    if (c.set_device() != ACO_OK) return ACO_ERR_CUDA;
-    CK(cudaEventSynchronize(s->len_ev[slot]));
-    const float *src = s->len_ring + (size_t)slot * (A + 2);
-    std::memcpy(lens, src, sizeof(float) * (A + 1));
-    int status;
-    std::memcpy(&status, src + A + 1, sizeof(int));
-    return status; // the device status word when the copy was queued
+    return ring_read(s->c, s->lr, ticket, lens, cap);
+}
+
+int aco_batch_enqueue_lengths(aco_batch *b, long long *ticket)
+{
+    if (!b || !ticket) return ACO_ERR_INVALID;
+    return ring_enqueue(b->c, b->lr, b->c.lens_all(), b->c.lens_total(), ticket);
+}
+
+int aco_batch_read_lengths(aco_batch *b, long long ticket, float *lens, size_t cap)
+{
+    if (!b || !lens || ticket < 0) return ACO_ERR_INVALID;
+    return ring_read(b->c, b->lr, ticket, lens, cap);
+}
+
+int aco_batch_get_best_all(aco_batch *b, int *tours, size_t cap_ints, int *tour_sizes, float *lengths)
+{
+    if (!b) return ACO_ERR_INVALID;
+    if (!b->c.initialized) return ACO_ERR_STATE;
+    return b->c.get_best_all(tours, cap_ints, tour_sizes, lengths);
 }
 
 int aco_run(aco_solver *s, float optimum, int *iterations_done)

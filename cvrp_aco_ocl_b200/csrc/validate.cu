@@ -90,7 +90,32 @@ __global__ void __launch_bounds__(kWarps * 32) validate_kernel(const ConstructAr
     }
 }
 
+// The best-so-far slot of every instance packed into one buffer: instance b's
+// tour (2n ints, the reference layout of slot A) at tour_base[b], its size and
+// length at [b].  One CTA per instance.
+__global__ void __launch_bounds__(256) gather_best_kernel(const ConstructArgs *args, const int *tour_base,
+                                                          int *tours, int *sizes, float *lens)
+{
+    const int b = blockIdx.x;
+    const ConstructArgs &a = args[b];
+    const int T = a.T, A = a.n_ants;
+    const int *src = a.solutions + (size_t)A * T;
+    int *dst = tours + tour_base[b];
+    for (int p = threadIdx.x; p < T; p += blockDim.x) dst[p] = src[p];
+    if (threadIdx.x == 0) {
+        sizes[b] = src[T - 1];
+        lens[b] = a.lens[A];
+    }
+}
+
 } // namespace
+
+cudaError_t launch_gather_best(const ConstructArgs *d_args, int n_inst, const int *d_tour_base, int *tours,
+                               int *sizes, float *lens, cudaStream_t st)
+{
+    gather_best_kernel<<<n_inst, 256, 0, st>>>(d_args, d_tour_base, tours, sizes, lens);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_validate(const ConstructArgs *d_args, int n_inst, int max_slots, int max_n, int *flags,
                             const int *slot_base, int *invalid, cudaStream_t st)

@@ -75,6 +75,46 @@ def time_to(trace, target: float):
     return None
 
 
+def held_out_instance(n: int, r: int):
+    """Held-out instance r of n nodes (n - 1 customers): mixed generator for
+    even r, large for odd r, seeds disjoint from the training set."""
+    seed = EVAL_SEED + 1000 * n + r
+    inst = I.gen_mixed(seed, n - 1) if r % 2 == 0 else I.gen_large(seed, n - 1)
+    return seed, inst
+
+
+def time_to_equal_cost(scorer: PR.EdgeScorer, n: int, count: int, plain_iters: int, ants: int, nn_ants: int,
+                       gamma: float = PR.DEFAULT_GAMMA, step: int = 10, first: int = 0) -> Dict:
+    """The metric's second half on `count` held-out instances of n nodes: the
+    plain colony's best after `plain_iters` iterations, rechecked in FP64, is
+    the target; the learned colony's wall time to come within 1% of it (graph
+    build, network forward and prior upload inside that time), over the plain
+    colony's wall time.  Both arms run `ants` ants on `nn_ants`-long candidate
+    lists (2-opt on 25-NN lists).  Instances the learned colony does not reach
+    within the plain colony's time count as ratio 1 in the median."""
+    recs = []
+    for r in range(first, first + count):
+        seed, inst = held_out_instance(n, r)
+        prob = Problem.from_instance(inst)
+        from .aco import compute_distances
+        prob.distance = compute_distances(prob.x, prob.y, prob.dis_type)
+        plain = run_arm(prob, colony_params(n, ants, nn_ants, seed), max_iters=plain_iters, step=step)
+        target = plain["best_fp64"] * 1.01
+        learned = run_arm(prob, colony_params(n, ants, nn_ants, seed),
+                          prior_fn=lambda: scorer.prior(prob, gamma=gamma),
+                          max_iters=10 * plain_iters, step=step, target=target, time_cap=plain["seconds"])
+        hit = time_to(learned["trace"], target)
+        recs.append({"n": n, "seed": seed, "plain_best_fp64": plain["best_fp64"], "plain_seconds": plain["seconds"],
+                     "plain_iters": plain["iters"], "target_fp64": target, "learned_seconds_to_target": hit,
+                     "learned_best_fp64": learned["best_fp64"], "learned_iters": learned["iters"],
+                     "feasible": plain["feasible"] and learned["feasible"],
+                     "ratio": (hit / plain["seconds"]) if hit is not None else None})
+    ratios = [x["ratio"] if x["ratio"] is not None else 1.0 for x in recs]
+    return {"instances": recs, "median_ratio": float(np.median(ratios)) if ratios else None,
+            "within_half_time": sum(1 for x in recs if x["ratio"] is not None and x["ratio"] <= 0.5),
+            "count": len(recs), "all_feasible": all(x["feasible"] for x in recs)}
+
+
 def evaluate(scorer: PR.EdgeScorer, sizes: List[int], per_size: int, plain_iters: int, ants: int, gamma: float,
              step: int = 10, log=print) -> Dict:
     out = {"config": {"sizes": sizes, "per_size": per_size, "plain_iters": plain_iters, "ants": ants,

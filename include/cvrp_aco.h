@@ -107,6 +107,9 @@ typedef struct aco_params {
                              of at most 32 nodes and one persistent kernel improves them all, spread over the SMs;
                              -1 = one CTA per group of ants; 0 = automatic (the list above 4 ants per SM); same
                              results either way */
+    int wait_limit;       /* polls of an mbarrier before a device wait gives up with ACO_ERR_TIMEOUT (0 = the
+                             default, 2^24 polls, about a second); no reference counterpart (kernel.cl has no
+                             bounded waits) */
 } aco_params;
 
 /* One best-so-far record {iteration, length, seconds since init} (problem.h:62-66). */
@@ -196,6 +199,14 @@ int aco_set_state(aco_solver *s, const float *tau, const float *total_info, cons
                   const float *lens, const int *seeds);
 /* sticky device status of the last launches (ACO_OK or an ACO_ERR_* code). */
 int aco_status(aco_solver *s);
+/* Waits for the stream, returns the sticky device status and resets it to
+ * ACO_OK, so the solver can go on after a reported error (no reference
+ * counterpart: the reference exit(1)s, g_aco.cpp:607-614). */
+int aco_clear_status(aco_solver *s);
+/* Polls of an mbarrier before a device wait gives up (aco_params.wait_limit;
+ * 0 = the default); takes effect from the next launch, graph replays included.
+ * No reference counterpart. */
+int aco_set_wait_limit(aco_solver *s, int polls);
 const char *aco_strerror(int code);
 /* CUDA's description of the last CUDA error that a call on this thread turned
  * into ACO_ERR_CUDA (diagnostics; no reference counterpart). */
@@ -298,6 +309,19 @@ int aco_batch_time_phases(aco_batch *b, int n_iter, float *ms4);
 void *aco_batch_get_stream(aco_batch *b);
 /* number of kernel launches one batch iteration makes (graph nodes).  No reference counterpart. */
 int aco_batch_launches_per_iteration(aco_batch *b);
+/* Pipelined readback of every instance's lengths, as aco_enqueue_lengths /
+ * aco_read_lengths for one solver (the reference reads them back after every
+ * iteration, g_aco.cpp:407-417): `lens` receives sum over instances of
+ * (n_ants + 1) floats, instance b's ants then its best-so-far at offset
+ * sum_{c<b} (n_ants + 1).  At most 4 tickets are outstanding.  No reference
+ * counterpart. */
+int aco_batch_enqueue_lengths(aco_batch *b, long long *ticket);
+int aco_batch_read_lengths(aco_batch *b, long long ticket, float *lens, size_t cap);
+/* Every instance's best-so-far tour in one transfer (update_best_so_far_from_device,
+ * g_aco.cpp:527-552, for the whole batch): tours receives sum of 2n ints,
+ * instance b's slot (reference layout, size in its last int) at offset
+ * sum_{c<b} 2n_c; tour_sizes and lengths (count entries each) may be NULL. */
+int aco_batch_get_best_all(aco_batch *b, int *tours, size_t cap_ints, int *tour_sizes, float *lengths);
 void aco_batch_destroy(aco_batch *b);
 
 /* ---- learned prior: edge-scoring network (no reference counterpart) -------
@@ -356,11 +380,15 @@ int aco_batch_get_bsf_records(aco_batch *b, int idx, aco_record *out, int cap, i
  *   solutions, lens : the reference layout (2n*(n_ants+1)+1 ints, n_ants+1
  *                     floats) after the statistics step (best-so-far in slot n_ants);
  *   elites_out      : ras_ranks ints, or NULL.
+ * The elite tours are checked before they are used as indices: an elite whose
+ * size is outside [2, 2n-1] or that holds a node id outside [0, n) deposits
+ * nothing, and its elites_out entry reads ACO_ERR_INVALID instead of its ant id.
  * Scratch is a fixed 148 KB array inside the library (kept by every GPU that
  * loads it until exit): n <= 4096 and ras_ranks <= 8, else ACO_ERR_CAPACITY.
- * The first call on a device looks up that array's device address; make it
- * before any stream capture.  Calls share the array, so calls that overlap on
- * the GPU race.  Allocates nothing, frees nothing. */
+ * The first call on a device (and again after its context is recreated) looks
+ * up that array's device address; make it before any stream capture.  Calls
+ * share the array, so calls that overlap on the GPU race.  Allocates nothing,
+ * frees nothing. */
 int aco_pheromone_update_noalloc(int n, int ld, int n_ants, int ras_ranks, float rho, float alpha, float beta,
                                  float *tau, float *total_info, const float *dist, const int *solutions,
                                  const float *lens, int *elites_out, void *stream);

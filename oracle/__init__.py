@@ -52,6 +52,11 @@ class OrcState(ctypes.Structure):
     ]
 
 
+# Root of the reference's source tree (its cvrp_ocl/ and dataset/ folders), read
+# only by the recipes that compile or read the reference for the checker.
+REFERENCE_ROOT = os.environ.get("CVRP_REFERENCE_DIR", "/root/reference")
+
+
 def build(quiet: bool = True) -> None:
     """Compile liboracle.so (and _ref/libcvrp_ref.so where the reference sources
     are present) with the committed Makefile."""
@@ -59,8 +64,8 @@ def build(quiet: bool = True) -> None:
     if quiet:
         kw.update(stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     subprocess.run(["make", "liboracle.so"], **kw)
-    if os.path.isdir("/root/reference/cvrp_ocl"):
-        subprocess.run(["make", "ref"], **kw)
+    if os.path.isdir(os.path.join(REFERENCE_ROOT, "cvrp_ocl")):
+        subprocess.run(["make", "ref", f"REF={REFERENCE_ROOT}"], **kw)
 
 
 _lib = None

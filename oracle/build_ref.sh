@@ -4,11 +4,11 @@
 # gpu/g_aco.cpp) and its OpenCL kernels (gpu/kernel.cl, compiled as C++) linked
 # against the fake OpenCL runtime in oracle/refshim.  Test infrastructure only.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_DIR]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_DIR]   (default $CVRP_REFERENCE_DIR, else /root/reference)
 # Intermediate files go to a temporary directory; only the .so lands in oracle/_ref/.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF_ROOT="${1:-/root/reference}"
+REF_ROOT="${1:-${CVRP_REFERENCE_DIR:-/root/reference}}"
 SRC="$REF_ROOT/cvrp_ocl"
 OUT="$HERE/_ref"
 if [ ! -f "$SRC/gpu/kernel.cl" ]; then

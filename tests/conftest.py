@@ -9,7 +9,7 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE_DIR = "/root/reference/cvrp_ocl"
+REFERENCE_DIR = os.path.join(os.environ.get("CVRP_REFERENCE_DIR", "/root/reference"), "cvrp_ocl")
 
 
 def pytest_configure(config):

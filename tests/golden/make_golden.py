@@ -4,8 +4,9 @@ Runs the reference (cvrp_ocl/gpu/kernel.cl + g_aco.cpp + host .cpp files,
 compiled for the CPU against oracle/refshim's fake OpenCL runtime by
 oracle/build_ref.sh) on small seeded synthetic instances and stores every
 device buffer after init_aco and after each iteration in an .npz per case.
-It reads the reference sources under /root/reference; the fixtures it writes
-are committed, so the tests read them wherever the reference is absent.
+It reads the reference sources under $CVRP_REFERENCE_DIR (default
+/root/reference); the fixtures it writes are committed, so the tests read them
+wherever the reference is absent.
 
     python tests/golden/make_golden.py
 """

@@ -17,7 +17,7 @@ from cvrp_aco_ocl_b200 import (AcoError, Problem, check_solution, compute_distan
 from cvrp_aco_ocl_b200 import _lib
 from cvrp_aco_ocl_b200 import instances as I
 
-REF_DATASET = "/root/reference/dataset"
+REF_DATASET = os.path.join(os.environ.get("CVRP_REFERENCE_DIR", "/root/reference"), "dataset")
 
 
 def header_symbols():
