@@ -45,12 +45,15 @@ __device__ __forceinline__ float pm_uniform(uint32_t x)
     return __fmul_rn(__int2float_rn((int)x), 4.656612873077392578125e-10f);
 }
 
-// Natural logarithm for the throughput sampler's exponential race, written out
-// so that the host restatement computes the same bits: u = m * 2^e with m in
-// [sqrt(1/2), sqrt(2)), ln(u) = e*ln2 + 2*atanh(s), s = (m-1)/(m+1), the odd
-// series of atanh to s^9 (|s| <= 0.1716: truncation below 2e-9 relative).
-// Defined for u >= 0 (u = 0 gives -127*ln2).
-__device__ __forceinline__ float race_ln(float u)
+// The throughput sampler's exponential clock: E = -ln(u) ~ Exp(1) for u
+// uniform in (0, 1], without a division, written out so that the host
+// restatement computes the same bits.  u = m * 2^e with m in [sqrt(1/2),
+// sqrt(2)), t = m - 1, ln(m) = t + t^2 * Q(t) with Q the degree-6 polynomial
+// fitted by least squares on Chebyshev nodes of that interval to
+// (ln(1+t) - t) / t^2, weighted for relative error (|relative error of ln(m)|
+// below 3e-7 in fp32), evaluated by Horner with fused multiply-adds.
+// u = 1 gives E = +0.
+__device__ __forceinline__ float race_exp1(float u)
 {
     const uint32_t b = __float_as_uint(u);
     int e = (int)(b >> 23) - 127;
@@ -60,30 +63,27 @@ __device__ __forceinline__ float race_ln(float u)
         e += 1;
     }
     const float t = __fsub_rn(m, 1.0f);
-    const float s = __fdiv_rn(t, __fadd_rn(t, 2.0f));
-    const float s2 = __fmul_rn(s, s);
-    float p = __fmaf_rn(s2, 1.0f / 9.0f, 1.0f / 7.0f);
-    p = __fmaf_rn(s2, p, 1.0f / 5.0f);
-    p = __fmaf_rn(s2, p, 1.0f / 3.0f);
-    p = __fmul_rn(s2, p);
-    const float ls = __fmul_rn(2.0f, __fmaf_rn(s, p, s));
-    return __fmaf_rn((float)e, 0.693147182f, ls);
+    float q = __fmaf_rn(-0.098038554f, t, 0.16080461f);
+    q = __fmaf_rn(q, t, -0.172902f);
+    q = __fmaf_rn(q, t, 0.19920385f);
+    q = __fmaf_rn(q, t, -0.24968483f);
+    q = __fmaf_rn(q, t, 0.333343f);
+    q = __fmaf_rn(q, t, -0.5000038f);
+    const float lm = __fmaf_rn(t, __fmul_rn(t, q), t);
+    return __fsub_rn(0.0f, __fmaf_rn((float)e, 0.693147182f, lm)); // 0 - x: +0 at u = 1, not -0
 }
 
-// Rate of a lane's exponential clock: 1 / E with E = -ln(u) ~ Exp(1).  The
-// candidate with the largest weight * rate (smallest E / weight) wins, which
-// selects candidate j with probability weight_j / sum(weight).  u = 1 gives
-// E = +0 and rate +inf.
-__device__ __forceinline__ float race_rate(float u) { return __fdiv_rn(1.0f, __fsub_rn(0.0f, race_ln(u))); }
+// Race key of a lane: the bits of E / weight = E * (1 / weight) (non-negative,
+// so ordered as unsigned) with the low 5 bits replaced by the lane, so that one
+// unsigned min reduction yields the winner -- the smallest E_j / w_j, which
+// selects candidate j with probability w_j / sum(w) -- and equal keys go to the
+// lowest lane.  The candidate tables hold 1 / weight; a candidate of weight 0
+// (reciprocal +inf) cannot win: kNoKey.
+constexpr uint32_t kNoKey = 0xffffffffu;
 
-// Race key of a lane: the bits of weight * rate (non-negative, so ordered as
-// unsigned) with the low 5 bits replaced by 31 - lane, so that one unsigned max
-// reduction yields the winner and equal keys go to the lowest lane; 0 = no
-// candidate.
-__device__ __forceinline__ uint32_t race_key(float w, float rate, int lane)
+__device__ __forceinline__ uint32_t race_key(float e, float winv, int lane)
 {
-    const uint32_t b = __float_as_uint(__fmul_rn(w, rate)) & ~31u;
-    return (b < 32u ? 32u : b) | (uint32_t)(31 - lane);
+    return (__float_as_uint(__fmul_rn(e, winv)) & ~31u) | (uint32_t)lane;
 }
 
 // Sticky error: the first failing kernel's code wins.

@@ -372,6 +372,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         route_cap_ = use_routes_ ? (int)cap : 0;
     }
     const size_t o_rdesc = take((size_t)route_cap_ * sizeof(int2)), o_rctr = take(16);
+    const size_t o_lslist = take((size_t)total_ants * 4), o_lsctr = take(16); // flagged ants for the per-ant 2-opt
     const size_t o_rrem = take((size_t)total_ants * 4);
 
     void *arena = nullptr;
@@ -431,6 +432,8 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     route_desc_d_ = (int2 *)(base + o_rdesc);
     route_ctr_d_ = (int *)(base + o_rctr);
     route_rem_d_ = (int *)(base + o_rrem);
+    ls_list_d_ = (int *)(base + o_lslist);
+    ls_list_ctr_d_ = (int *)(base + o_lsctr);
 
     // ---- configuration (shared-memory budgets over the largest instance)
     const bool throughput = p.mode == ACO_MODE_THROUGHPUT;
@@ -683,6 +686,8 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         c.route_desc = use_routes_ ? route_desc_d_ : nullptr;
         c.route_ctr = route_ctr_d_;
         c.route_rem = route_rem_d_;
+        c.ls_list = ls_list_d_;
+        c.ls_list_ctr = ls_list_ctr_d_;
         c.route_cap = route_cap_;
         c.seeds = ih.seeds_d; c.solutions = ih.sol_d; c.lens = ih.lens_d; c.status = status_d;
         c.wait_limit = wait_d;
@@ -942,7 +947,10 @@ int Colony::construct(bool fused)
     last_fused_ = lsw > 0;
     // the route list is rewound by the 2-opt kernel that consumes it; a second
     // construct without one in between starts it afresh
-    if (use_routes_ && lsw == 0 && routes_pending_) CK(cudaMemsetAsync(route_ctr_d_, 0, 16, st));
+    if (use_routes_ && lsw == 0 && routes_pending_) {
+        CK(cudaMemsetAsync(route_ctr_d_, 0, 16, st));
+        CK(cudaMemsetAsync(ls_list_ctr_d_, 0, 16, st));
+    }
     routes_pending_ = use_routes_ && lsw == 0;
     CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st, lsw,
                            cn_draw));
@@ -958,8 +966,11 @@ int Colony::local_search()
         CK(launch_route_opt(largs_d_, ant_inst_d_, ant_base_d_, route_desc_d_, route_ctr_d_, route_cap_, route_rem_d_,
                             ls_needed_d_, ls_nmax, kRouteWarps, sm_count, st));
     routes_pending_ = false;
+    // after the route-level kernel only the ants the construct listed remain: a
+    // persistent grid over that list; after a fused construct, every ant's flag
     CK(launch_local_search(largs_d_, ant_inst_d_, ant_base_d_, total_ants, ls_apc, ls_nmax, ls_warps, ls_smem, st,
-                           last_fused_ || routes ? ls_needed_d_ : nullptr));
+                           last_fused_ || routes ? ls_needed_d_ : nullptr, routes ? ls_list_d_ : nullptr,
+                           routes ? ls_list_ctr_d_ : nullptr, sm_count));
     last_fused_ = false;
     if (p.ls_flag & 2) CK(launch_swap(cargs_d_, sw_items_d_, sw_items, sw_apc, sw_smem, kSwapLimitPerNode, st));
     return ACO_OK;

@@ -139,6 +139,7 @@ private:
     int route_cap_ = 0;
     int2 *route_desc_d_ = nullptr;
     int *route_ctr_d_ = nullptr, *route_rem_d_ = nullptr;
+    int *ls_list_d_ = nullptr, *ls_list_ctr_d_ = nullptr; // ants left to the per-ant 2-opt
     bool last_fused_ = false;
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
     int *row_base_d_ = nullptr, *zero_base_d_ = nullptr;

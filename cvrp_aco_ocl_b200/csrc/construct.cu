@@ -19,9 +19,10 @@
 // warp-per-ant sampling over a nearest-neighbour candidate list staged in
 // shared memory by TMA bulk copies.  The roulette is run as an exponential
 // race: lane j draws u_j from its own Park-Miller stream and candidate j wins
-// with the largest weight_j / -ln(u_j), which picks j with probability
-// weight_j / sum(weight) like the roulette, in one warp max-reduction instead
-// of a prefix scan (the draws are off the step's dependent chain).
+// with the smallest -ln(u_j) / weight_j, which picks j with probability
+// weight_j / sum(weight) like the roulette, in one warp min-reduction instead
+// of a prefix scan (the draws are off the step's dependent chain).  The
+// candidate tables hold 1 / weight, so a step needs no division.
 //
 // Rows of total_info and the lookup tables are staged into shared memory with
 // 1-D cp.async.bulk copies (no cluster multicast) completing on an mbarrier.
@@ -229,7 +230,7 @@ __global__ void __launch_bounds__(512) construct_parity_kernel(ConstructArgs a)
 // total_info matrix into shared memory with TMA bulk copies, then runs one
 // warp per ant.  Per ant:
 //   * lane l draws from the ant's Park-Miller state l, one number a step, and
-//     turns it into the rate of its exponential clock (race_rate);
+//     turns it into its exponential clock E = -ln(u) (race_exp1);
 //   * with helper warps (draw), a second warp per ant makes those draws and
 //     rates 16 steps ahead into a double-buffered shared ring, handing over at
 //     a two-warp named barrier every 16 steps, so the ant's warp keeps only the
@@ -396,7 +397,7 @@ __device__ void fused_ls_warp(const ConstructArgs &a, unsigned char *smem, const
 // Barrier `id` shared by exactly two warps (an ant's warp and its helper).
 __device__ __forceinline__ void pair_barrier(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
 
-// Helper warp of one ant: the race rates of chunk c go to ring half c & 1; at
+// Helper warp of one ant: the race clocks of chunk c go to ring half c & 1; at
 // hand-over c both warps meet at the pair barrier, after which the ant's warp
 // has set flag[c & 1] (1 = the ant is done, 0 = continue).  The ant's warp
 // reads flag-free: it only waits at the same barriers.
@@ -405,7 +406,7 @@ __device__ __forceinline__ uint32_t draw_chunk(uint32_t xs, float *buf, int lane
 #pragma unroll 4
     for (int k = 0; k < kDrawChunk; k++) {
         xs = pm_mul(xs, 16807u);
-        buf[k * 32 + lane] = race_rate(pm_uniform(xs));
+        buf[k * 32 + lane] = race_exp1(pm_uniform(xs));
     }
     return xs;
 }
@@ -466,8 +467,23 @@ __device__ __forceinline__ void emit_routes(const ConstructArgs &a, const uint16
         for (int k = lane; k < nshort && rbase + k < a.route_cap; k += 32) a.route_desc[rbase + k] = make_int2(-1, 0);
     if (lane == 0) {
         a.route_rem[g] = fits ? nshort : 0;
-        a.ls_needed[g] = (uint8_t)(!fits ? 2 : (longr ? 1 : 0));
+        const uint8_t need = (uint8_t)(!fits ? 2 : (longr ? 1 : 0));
+        a.ls_needed[g] = need;
+        if (need) { // one entry per ant and construct: the list holds every ant of the colony
+            const int k = atomicAdd(a.ls_list_ctr, 1);
+            a.ls_list[k] = g;
+        }
     }
+}
+
+// Register visited set (n <= 1024): bit k of a lane's word is node lane + 32k.
+// The lane's unvisited customers: its in-range bits not yet set (node 0, the
+// depot, is bit 0 of lane 0 and always set).
+__device__ __forceinline__ uint32_t open_bits(uint32_t vis, int n, int lane)
+{
+    const int cnt = lane < n ? (n - lane + 31) >> 5 : 0; // nodes lane, lane + 32, ... below n
+    const uint32_t valid = cnt >= 32 ? 0xffffffffu : (1u << cnt) - 1u;
+    return ~vis & valid;
 }
 
 // Smallest demand among the unvisited customers of an ant (warp-wide result).
@@ -476,10 +492,13 @@ __device__ __forceinline__ int min_open_demand(const int *s_dem, uint32_t vis, c
                                                int lane)
 {
     int m = 0x7fffffff;
-    for (int k = 0; k < words; k++) {
-        const int i = lane + 32 * k;
-        const uint32_t vk = REGVIS ? vis : vism[k];
-        if (i > 0 && i < n && !((vk >> (REGVIS ? k : lane)) & 1u)) m = min(m, s_dem[i]);
+    if (REGVIS) { // only this lane's unvisited nodes
+        for (uint32_t o = open_bits(vis, n, lane); o; o &= o - 1u) m = min(m, s_dem[lane + 32 * (__ffs(o) - 1)]);
+    } else {
+        for (int k = 0; k < words; k++) {
+            const int i = lane + 32 * k;
+            if (i > 0 && i < n && !((vism[k] >> lane) & 1u)) m = min(m, s_dem[i]);
+        }
     }
     return (int)__reduce_min_sync(0xffffffffu, (unsigned)m);
 }
@@ -493,6 +512,40 @@ __device__ __forceinline__ int best_of_row(const float *row, const int *s_dem, c
 {
     const unsigned FULL = 0xffffffffu;
     uint32_t bk = 0u, bi = 0xffffffffu;
+    if (REGVIS) {
+        // Only the lane's unvisited nodes, lowest first (so a strict > keeps the
+        // lowest index of a lane's equal values), four a round with their loads
+        // issued first; rounds until the lane with the most unvisited nodes is done.
+        uint32_t open = open_bits(vis, n, lane);
+        const int rounds = ((int)__reduce_max_sync(FULL, (unsigned)__popc(open)) + 3) >> 2;
+        const int capleft = cap - load;
+        for (int r = 0; r < rounds; r++) {
+            int idx[4], dm[4];
+            float rv[4], dv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = open ? lane + 32 * (__ffs(open) - 1) : -1;
+                open &= open - 1u;
+                const int ic = i >= 0 ? i : 0;
+                idx[u] = i;
+                rv[u] = row[ic];
+                dm[u] = i >= 0 ? s_dem[ic] : 0x7fffffff; // no node: fails the capacity test
+                if (FIN) dv[u] = __ldg(drow + ic);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                bool ff = dm[u] <= capleft;
+                if (FIN) ff = ff && __fadd_rn(__fadd_rn(rdist, __fadd_rn(dv[u], serv)), s_d0[idx[u] >= 0 ? idx[u] : 0]) <= maxd;
+                const uint32_t kk = ff ? __float_as_uint(rv[u]) + 1u : 0u;
+                const bool better = kk > bk;
+                bk = better ? kk : bk;
+                bi = better ? (uint32_t)idx[u] : bi;
+            }
+        }
+        const uint32_t hk = __reduce_max_sync(FULL, bk);
+        if (hk == 0u) return -1;
+        return (int)__reduce_min_sync(FULL, bk == hk ? bi : 0xffffffffu);
+    }
     constexpr int G = FIN ? 4 : 8;
     for (int k0 = 0; k0 < words; k0 += G) { // branch-free: every lane tests its own nodes
         // G nodes a lane at a time, all loads first (indices clamped into range)
@@ -673,7 +726,7 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 err = ACO_ERR_STEP_LIMIT;
                 break;
             }
-            float rate;
+            float ex; // this lane's exponential clock for the step
             if (DRAW) {
                 const int sc = step & (kDrawChunk - 1);
                 if (sc == 0 && step > 0) { // next chunk: hand-over `hand`, continue
@@ -682,10 +735,10 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                     pair_barrier(1 + warp);
                     hand++;
                 }
-                rate = ring[((hand - 1) & 1) * kDrawChunk * 32 + sc * 32 + lane];
+                ex = ring[((hand - 1) & 1) * kDrawChunk * 32 + sc * 32 + lane];
             } else {
                 xs = pm_mul(xs, 16807u);
-                rate = race_rate(pm_uniform(xs)); // off the dependent chain of the step
+                ex = race_exp1(pm_uniform(xs)); // off the dependent chain of the step
             }
             int c, dc;
             if (PACKED) {
@@ -696,17 +749,17 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 c = s_nn[cur * Kp + jl];
                 dc = s_dem[c];
             }
-            const float wv = s_chc[cur * Kp + jl];
+            const float winv = s_chc[cur * Kp + jl]; // 1 / total_info of the candidate
             const uint32_t vw = REGVIS ? __shfl_sync(FULL, vis, c & 31) : vism[c >> 5];
             bool f = lane < K && !((vw >> (REGVIS ? (c >> 5) : (c & 31))) & 1u) && (load + dc <= cap);
             if (FIN && f)
                 f = __fadd_rn(__fadd_rn(rdist, __fadd_rn(__ldg(a.dist + (size_t)cur * ld + c), a.serv_time)),
                               s_d0[c]) <= a.max_dist;
-            // exponential race: the largest wv * rate wins (probability wv / sum of wv)
-            const uint32_t hk = __reduce_max_sync(FULL, f && wv > 0.f ? race_key(wv, rate, lane) : 0u);
+            // exponential race: the smallest E / w wins (probability w / sum of w); weight 0 never wins
+            const uint32_t hk = __reduce_min_sync(FULL, f && winv < INFINITY ? race_key(ex, winv, lane) : kNoKey);
             int nxt = -1, nd = 0;
-            if (hk != 0u) {
-                const uint32_t pick = __shfl_sync(FULL, (uint32_t)c | ((uint32_t)dc << 16), 31 - (int)(hk & 31u));
+            if (hk != kNoKey) {
+                const uint32_t pick = __shfl_sync(FULL, (uint32_t)c | ((uint32_t)dc << 16), (int)(hk & 31u));
                 nxt = (int)(pick & 0xFFFFu);
                 nd = (int)(pick >> 16);
             } else if (DRAW) {
@@ -896,8 +949,10 @@ __device__ __forceinline__ void construct_nn_body(const ConstructArgs *args, con
     }
 }
 
+// Register budget: one CTA of the widest launch (16 warps) per SM, the
+// residency the staged tables allow on the batched workloads.
 template <bool FIN, int KIND>
-__global__ void __launch_bounds__(512) construct_nn_kernel(const ConstructArgs *args, const int2 *items, int n_items,
+__global__ void __launch_bounds__(512, 1) construct_nn_kernel(const ConstructArgs *args, const int2 *items, int n_items,
                                                            int *queue, int apc, int lsw)
 {
     construct_nn_body<FIN, KIND>(args, items, n_items, queue, apc, lsw);

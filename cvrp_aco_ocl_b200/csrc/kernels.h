@@ -9,8 +9,8 @@
 //   seeds                  : A*nloc int32 (one Park-Miller state per work-item lane)
 //   nn_ls_list             : n x nn_ls int32 (2-opt); nn16 / cand32 : n x Kp candidate
 //                            lists (uint16 node ids / node | demand << 16)
-//   chc                    : n x Kp fp32, total_info of every candidate (throughput mode),
-//                            written by the pheromone pass
+//   chc                    : n x Kp fp32, 1 / total_info of every candidate (throughput
+//                            mode: the race's reciprocal weights), written by the pheromone pass
 //
 // Every kernel except the parity construct reads its instance from an array of
 // argument blocks in device memory, so one launch serves one instance or a
@@ -37,7 +37,7 @@ struct ConstructArgs {
     const uint32_t *adv;   // nloc: 16807^(draws of lane l per step) mod m
     const uint16_t *nn16;  // n x Kp candidate lists (throughput), uint16 node ids
     const uint32_t *cand32;// n x Kp candidate lists, packed node | demand << 16
-    const float *chc;      // n x Kp total_info of the candidates
+    const float *chc;      // n x Kp: 1 / total_info of the candidates (+inf for weight 0)
     int K, Kp;             // candidate-list length and padded row length (multiple of 8)
     int smat;              // throughput construct: stage the whole total_info matrix
     int packed;            // throughput construct: use cand32 (else nn16 + demand lookups)
@@ -55,6 +55,9 @@ struct ConstructArgs {
     int2 *route_desc;
     int *route_ctr, *route_rem;
     int route_cap;
+    // the ants whose ls_needed is set, listed for the per-ant 2-opt kernel
+    // (route-list mode): ls_list_ctr[0] entries, capacity = the colony's ants
+    int *ls_list, *ls_list_ctr;
     int *seeds;
     int *solutions;
     float *lens;
@@ -102,7 +105,7 @@ struct UpdateArgs {
     const uint32_t *depmask;
     const float *d_tau;
     const float *bsf_len;    // lens[A] (trail_0 = 1/(rho * bsf))
-    float *chc;              // n x Kp, or null (no candidate table)
+    float *chc;              // n x Kp reciprocal candidate weights, or null (no candidate table)
     const uint16_t *nn16;    // n x Kp
     int K, Kp;
 };
@@ -152,11 +155,15 @@ cudaError_t launch_route_opt(const LocalSearchArgs *d_args, const int *d_ant_ins
                              const int2 *d_desc, int *d_ctr, int cap, int *d_rem, const uint8_t *d_flagged, int n_max,
                              int warps, int sm_count, cudaStream_t st);
 // 2-opt: CTAs of `ants_per_cta` ants (1..8) and `warps` warps pulling routes;
-// n_max sizes the per-ant shared buffers.  only (after a fused construct):
-// skip ants whose flag is 0 and, in the others, routes of at most 32 nodes.
+// n_max sizes the per-ant shared buffers.  only (after a fused construct or the
+// route-level kernel): skip ants whose flag is 0 and, in the others, routes of
+// at most 32 nodes when the flag is 1.  list / list_ctr (with only): the flagged
+// ants as the construct listed them (list_ctr[0] entries), taken by a
+// persistent grid of at most sm_count x occupancy CTAs, which rewinds the list.
 cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
                                 int total_ants, int ants_per_cta, int n_max, int warps, size_t smem, cudaStream_t st,
-                                const uint8_t *only = nullptr);
+                                const uint8_t *only = nullptr, const int *list = nullptr, int *list_ctr = nullptr,
+                                int sm_count = 148);
 // one: a single instance's arguments passed by value (d_args unused)
 cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st,
                          const StatsArgs *one = nullptr);

@@ -31,6 +31,7 @@
 // distance matrix.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -235,9 +236,14 @@ __device__ int two_opt_route_generic(Route &c, int pass_limit)
     return ACO_OK;
 }
 
+// Grid mode (list == null): CTA b improves the global ants [b * apc, b * apc +
+// apc).  List mode: a persistent grid takes groups of apc ants from the list
+// the construct kernel wrote (the ants flagged in `only`, list_ctr[0] of them),
+// so the CTAs see only those ants; the last CTA rewinds the list.
 __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArgs *args, const int *ant_inst,
                                                              const int *ant_base, const uint8_t *only, int apc,
-                                                             int n_max, int total_ants)
+                                                             int n_max, int total_ants, const int *list,
+                                                             int *list_ctr)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_inst[kMaxLsAnts], s_ant[kMaxLsAnts], s_size[kMaxLsAnts], s_routes[kMaxLsAnts + 1];
@@ -252,10 +258,21 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
     uint8_t *lnn = wbase + kRL * kRL * 4;
     uint8_t *lcnt = lnn + kRL * kRL;
     auto ant_ptr = [&](int j, size_t off) { return smem + (size_t)j * AL.bytes + off; };
+    __shared__ int s_group;
+    const int listed = list ? min(list_ctr[0], total_ants) : 0;
+    for (int grp = blockIdx.x;;) {
+    if (list) {
+        __syncthreads(); // the previous group is done with shared memory
+        if (threadIdx.x == 0) s_group = atomicAdd(list_ctr + 1, 1);
+        __syncthreads();
+        grp = s_group;
+        if (grp * apc >= listed) break;
+    }
 
-    // the CTA's ants: global ants [blockIdx.x * apc, ... + apc)
+    // the CTA's ants: global ants [grp * apc, ... + apc), or entries of the list
     if (threadIdx.x < apc) {
-        const int j = threadIdx.x, g = blockIdx.x * apc + j;
+        const int j = threadIdx.x;
+        const int g = list ? (grp * apc + j < listed ? __ldg(list + grp * apc + j) : total_ants) : grp * apc + j;
         int inst = -1, ant = 0, size = 0;
         if (g < total_ants && (!only || only[g])) { // `only`: the ants a fused construct left to this kernel
             inst = __ldg(ant_inst + g);
@@ -480,6 +497,19 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
         }
         if (lane == 0) args[s_inst[j]].lens[s_ant[j]] = len;
     }
+    if (!list) break;
+    }
+    if (list) { // the last CTA to finish rewinds the list for the next construct
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(list_ctr + 2, 1) == (int)gridDim.x - 1) {
+                list_ctr[0] = 0;
+                list_ctr[1] = 0;
+                list_ctr[2] = 0;
+            }
+        }
+    }
 }
 
 } // namespace
@@ -655,14 +685,22 @@ cudaError_t launch_route_opt(const LocalSearchArgs *d_args, const int *d_ant_ins
 
 cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_inst, const int *d_ant_base,
                                 int total_ants, int ants_per_cta, int n_max, int warps, size_t smem, cudaStream_t st,
-                                const uint8_t *only)
+                                const uint8_t *only, const int *list, int *list_ctr, int sm_count)
 {
     if (ants_per_cta < 1 || ants_per_cta > kMaxLsAnts || warps < ants_per_cta) return cudaErrorInvalidValue;
+    if ((list == nullptr) != (list_ctr == nullptr) || (list && !only)) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(local_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int blocks = (total_ants + ants_per_cta - 1) / ants_per_cta;
+    int blocks = (total_ants + ants_per_cta - 1) / ants_per_cta;
+    if (list) { // persistent over the listed ants: as many CTAs as fit at once, at most one per group
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, local_search_kernel, warps * 32, smem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        blocks = std::min(blocks, sm_count * per_sm);
+    }
     local_search_kernel<<<blocks, warps * 32, smem, st>>>(d_args, d_ant_inst, d_ant_base, only, ants_per_cta, n_max,
-                                                          total_ants);
+                                                          total_ants, list, list_ctr);
     return cudaGetLastError();
 }
 

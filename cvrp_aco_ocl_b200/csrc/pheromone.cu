@@ -416,12 +416,12 @@ __device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, f
             }
         }
     }
-    if (a.chc) { // compact candidate table: chc[i][j] = total[i][nn[i][j]]
+    if (a.chc) { // compact candidate table: chc[i][j] = 1 / total[i][nn[i][j]] (the race's reciprocal weight)
         // the row was written by this warp; __syncwarp orders those stores before
         // the re-reads below (they hit L2, the lines were just written)
         __syncwarp();
         for (int j = lane; j < a.K; j += 32)
-            a.chc[(size_t)i * a.Kp + j] = a.total[off + a.nn16[(size_t)i * a.Kp + j]];
+            a.chc[(size_t)i * a.Kp + j] = __fdiv_rn(1.0f, a.total[off + a.nn16[(size_t)i * a.Kp + j]]);
     }
 }
 

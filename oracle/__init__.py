@@ -107,8 +107,8 @@ def lib():
         L.orc_pow_rule.argtypes = [ctypes.c_float, ctypes.c_float]
         L.orc_pow_rule.restype = ctypes.c_float
         L.orc_f2i_x86.argtypes = [ctypes.c_float]
-        L.orc_race_ln.argtypes = [ctypes.c_float]
-        L.orc_race_ln.restype = ctypes.c_float
+        L.orc_race_exp1.argtypes = [ctypes.c_float]
+        L.orc_race_exp1.restype = ctypes.c_float
         sp = ctypes.POINTER(OrcState)
         for name in ("orc_construct", "orc_local_search", "orc_init_aco", "orc_run_aco_iteration"):
             getattr(L, name).argtypes = [sp, ctypes.c_int]
@@ -130,9 +130,9 @@ def ran01(seed: int):
     return r, s.value
 
 
-def race_ln(u: float) -> float:
-    """ln(u) as the throughput sampler computes it (fp32, own series)."""
-    return float(lib().orc_race_ln(ctypes.c_float(u)))
+def race_exp1(u: float) -> float:
+    """-ln(u) as the throughput sampler computes it (fp32, own polynomial)."""
+    return float(lib().orc_race_exp1(ctypes.c_float(u)))
 
 
 def make_seeds(seed_time: int, rnd_seed: int, n_ants: int, nloc: int):

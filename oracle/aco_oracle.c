@@ -848,39 +848,40 @@ int orc_run_aco_iteration(orc_state *s, int n_threads)
 /* Throughput mode: this project's candidate-list sampler (no reference    */
 /* counterpart).  Lane j (0..31) of an ant owns its Park-Miller state j and */
 /* draws u_j every step; the first nn_ants entries of the NN list are the  */
-/* candidates, and the feasible one with the largest choice_info / -ln(u_j) */
-/* wins (exponential race: the roulette's probabilities), keyed as the     */
-/* device does it; full-row argmax fallback over all feasible customers    */
-/* when no candidate has weight; depot return otherwise.                   */
+/* candidates, and the feasible one with the smallest -ln(u_j) /          */
+/* choice_info wins (exponential race: the roulette's probabilities),      */
+/* keyed as the device does it; full-row argmax fallback over all feasible */
+/* customers when no candidate has weight; depot return otherwise.         */
 /* ---------------------------------------------------------------------- */
 static float f_of_bits(uint32_t b) { float f; memcpy(&f, &b, 4); return f; }
 static uint32_t bits_of_f(float f) { uint32_t b; memcpy(&b, &f, 4); return b; }
 
-/* ln(u) = e*ln2 + 2*atanh((m-1)/(m+1)), m in [sqrt(1/2), sqrt(2)), odd series
- * of atanh to s^9 -- the device's race_ln operation for operation. */
-float orc_race_ln(float u)
+/* E = -ln(u): u = m*2^e, m in [sqrt(1/2), sqrt(2)), t = m - 1,
+ * ln(m) = t + t^2*Q(t), Q the degree-6 least-squares fit on Chebyshev nodes --
+ * the device's race_exp1 operation for operation (Horner with fmaf). */
+float orc_race_exp1(float u)
 {
     const uint32_t b = bits_of_f(u);
     int e = (int)(b >> 23) - 127;
     float m = f_of_bits((b & 0x007fffffu) | 0x3f800000u);
     if (m > 1.41421354f) { m = m * 0.5f; e += 1; }
     const float t = m - 1.0f;
-    const float s = t / (t + 2.0f);
-    const float s2 = s * s;
-    float p = fmaf(s2, 1.0f / 9.0f, 1.0f / 7.0f);
-    p = fmaf(s2, p, 1.0f / 5.0f);
-    p = fmaf(s2, p, 1.0f / 3.0f);
-    p = s2 * p;
-    const float ls = 2.0f * fmaf(s, p, s);
-    return fmaf((float)e, 0.693147182f, ls);
+    float q = fmaf(-0.098038554f, t, 0.16080461f);
+    q = fmaf(q, t, -0.172902f);
+    q = fmaf(q, t, 0.19920385f);
+    q = fmaf(q, t, -0.24968483f);
+    q = fmaf(q, t, 0.333343f);
+    q = fmaf(q, t, -0.5000038f);
+    const float tq = t * q;
+    const float lm = fmaf(t, tq, t);
+    return 0.0f - fmaf((float)e, 0.693147182f, lm);
 }
 
-/* The device's race_key: bits of w / -ln(u), low 5 bits = 31 - lane. */
-static uint32_t race_key(float w, float u, int lane)
+/* The device's race_key: bits of E * (1/w), low 5 bits = lane; the smallest wins. */
+#define RACE_NO_KEY 0xffffffffu
+static uint32_t race_key(float e, float winv, int lane)
 {
-    const float rate = 1.0f / (0.0f - orc_race_ln(u));
-    const uint32_t b = bits_of_f(w * rate) & ~31u;
-    return (b < 32u ? 32u : b) | (uint32_t)(31 - lane);
+    return (bits_of_f(e * winv) & ~31u) | (uint32_t)lane;
 }
 
 static int construct_nn_one(const orc_state *s, int ant, const int *nnl, int K,
@@ -899,19 +900,19 @@ static int construct_nn_one(const orc_state *s, int ant, const int *nnl, int K,
         if (step >= T - 3) { tour[T - 1] = 0; s->lens[ant] = INFINITY; return ORC_ERR_STEP_LIMIT; }
         float u[32];
         for (int j = 0; j < 32; j++) u[j] = orc_ran01(&seed[j]);
-        uint32_t hk = 0;
+        uint32_t hk = RACE_NO_KEY;
         int nxt = -1;
         for (int j = 0; j < K; j++) {
             const int c = nnl[(size_t)cur * K + j];
             const float dc = dist[(size_t)cur * n + c];
-            const float w = total[(size_t)cur * n + c];
+            const float winv = 1.0f / total[(size_t)cur * n + c]; /* the candidate table's reciprocal weight */
             if (!visited[c] && route_load + s->demand[c] <= s->capacity &&
-                route_dist + (dc + s->serv_time) + dist0[c] <= s->max_dist && w > 0.0f) {
-                const uint32_t key = race_key(w, u[j], j);
-                if (key > hk) { hk = key; nxt = c; }
+                route_dist + (dc + s->serv_time) + dist0[c] <= s->max_dist && winv < INFINITY) {
+                const uint32_t key = race_key(orc_race_exp1(u[j]), winv, j);
+                if (key < hk) { hk = key; nxt = c; }
             }
         }
-        if (hk == 0) {
+        if (hk == RACE_NO_KEY) {
             float bv = -1.0f;
             for (int i = 1; i < n; i++) {
                 const float di = dist[(size_t)cur * n + i];

@@ -55,8 +55,8 @@ typedef struct orc_state {
 /* ---- RNG, seeds -------------------------------------------------------- */
 float orc_ran01(int *idum);
 int orc_f2i_x86(float v);
-/* ln(u) of the throughput sampler's exponential race (the device's race_ln) */
-float orc_race_ln(float u);
+/* -ln(u), the throughput sampler's exponential clock (the device's race_exp1) */
+float orc_race_exp1(float u);
 void orc_make_seeds(int seed_time, int *rnd_seed, int n_ants, int nloc, int *seeds);
 
 /* ---- inputs ------------------------------------------------------------ */

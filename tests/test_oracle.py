@@ -90,17 +90,18 @@ def test_ran01_known_answers():
         assert got == (16807 * (x % m)) % m, x
 
 
-def test_race_ln_accuracy():
-    # the throughput sampler's logarithm: within 4 ulp-ish (2e-7 absolute + relative) of
-    # the true ln over the draws ran01 can return, exact 0 at u = 1
+def test_race_exp1_accuracy():
+    # the throughput sampler's exponential clock -ln(u): within a few ulp (3e-7 absolute +
+    # relative) of the true value over every draw ran01 can return, exact 0 at u = 1
     rng = np.random.default_rng(3)
     xs = np.concatenate([rng.integers(1, 2**31 - 1, 20000), [1, 2, 3, 2**31 - 2, 2**30, 2**31 - 64]])
     for x in xs:
         u = np.float32(np.float32(int(x)) * np.float32(4.656612873077392578125e-10))
-        got = oracle.race_ln(float(u))
-        want = float(np.log(np.float64(u)))
-        assert abs(got - want) <= 2e-7 + 2e-7 * abs(want), (x, got, want)
-    assert oracle.race_ln(1.0) == 0.0
+        got = oracle.race_exp1(float(u))
+        want = -float(np.log(np.float64(u)))
+        assert got >= 0.0 and math.copysign(1.0, got) > 0  # +0, never -0 (the key orders bits)
+        assert abs(got - want) <= 3e-7 + 3e-7 * abs(want), (x, got, want)
+    assert oracle.race_exp1(1.0) == 0.0 and math.copysign(1.0, oracle.race_exp1(1.0)) > 0
 
 
 def test_seed_formula_overflow_to_int_min():
