@@ -81,10 +81,34 @@ struct Staging {
     }
 };
 
+// FNV-1a over bytes, continued from h.
+uint64_t fnv1a(uint64_t h, const void *data, size_t bytes)
+{
+    const unsigned char *b = static_cast<const unsigned char *>(data);
+    for (size_t k = 0; k < bytes; k++) {
+        h ^= b[k];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+constexpr uint64_t kFnvBasis = 14695981039346656037ull;
+
 // Per-instance host preparation: distances, feasibility, NN lists.
 int prep_instance(const InstanceSpec &sp, const aco_params &p, InstHost &ih)
 {
     const int n = sp.n;
+    {   // the instance's identity for checkpoints: its data as given
+        uint64_t hh = fnv1a(kFnvBasis, &n, sizeof n);
+        if (sp.x) hh = fnv1a(hh, sp.x, sizeof(float) * (size_t)n);
+        if (sp.y) hh = fnv1a(hh, sp.y, sizeof(float) * (size_t)n);
+        hh = fnv1a(hh, sp.demand, sizeof(int) * (size_t)n);
+        if (sp.dist) hh = fnv1a(hh, sp.dist, sizeof(float) * (size_t)n * n);
+        const float f[2] = {sp.max_dist, sp.serv_time};
+        const int k[2] = {sp.capacity, sp.dist_type};
+        hh = fnv1a(hh, f, sizeof f);
+        ih.data_hash = fnv1a(hh, k, sizeof k);
+    }
     ih.n = n;
     ih.ld = (n + 31) & ~31;
     ih.n4 = (n + 3) & ~3;
@@ -338,6 +362,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     const size_t o_best_sizes = take((size_t)count * 4), o_best_lens = take((size_t)count * 4);
     const size_t o_ant_inst = take((size_t)total_ants * 4), o_ant_base = take((size_t)(count + 1) * 4);
     const size_t o_row_base = take((size_t)(count + 1) * 4), o_zero_base = take(16);
+    const size_t o_row_inst = take((size_t)total_rows * 4); // instance of every global matrix row
     const size_t o_slot_base = take((size_t)(count + 1) * 4), o_valid = take((size_t)(total_ants + count) * 4);
     const size_t o_invalid = take((size_t)count * 4);
     const size_t o_cargs = take(sizeof(ConstructArgs) * count), o_largs = take(sizeof(LocalSearchArgs) * count);
@@ -417,6 +442,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     ant_inst_d_ = (int *)(base + o_ant_inst);
     ant_base_d_ = (int *)(base + o_ant_base);
     row_base_d_ = (int *)(base + o_row_base);
+    row_inst_d_ = (int *)(base + o_row_inst);
     zero_base_d_ = (int *)(base + o_zero_base); // {0}: row base of a one-instance launch
     slot_base_d_ = (int *)(base + o_slot_base);
     valid_d_ = (int *)(base + o_valid);
@@ -578,7 +604,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     if (stats_smem > kSmemBudget) return ACO_ERR_INVALID; // n_ants lengths must fit in shared memory
 
     // ---- host tables and uploads
-    std::vector<int> ant_inst(total_ants), ant_base(count + 1), row_base(count + 1);
+    std::vector<int> ant_inst(total_ants), ant_base(count + 1), row_base(count + 1), row_inst(total_rows);
     std::vector<int2> items, swi, nsi;
     {
         int a0 = 0, r0 = 0;
@@ -586,6 +612,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
             ant_base[b] = a0;
             row_base[b] = r0;
             for (int k = 0; k < inst[b].A; k++) ant_inst[a0 + k] = b;
+            for (int k = 0; k < inst[b].n; k++) row_inst[r0 + k] = b;
             a0 += inst[b].A;
             r0 += inst[b].n;
         }
@@ -717,6 +744,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     up(ant_inst_d_, ant_inst.data(), ant_inst.size() * 4);
     up(ant_base_d_, ant_base.data(), ant_base.size() * 4);
     up(row_base_d_, row_base.data(), row_base.size() * 4);
+    up(row_inst_d_, row_inst.data(), row_inst.size() * 4);
     up(slot_base_d_, slot_base_h_.data(), slot_base_h_.size() * 4);
     up(tour_base_d_, tour_base_h_.data(), tour_base_h_.size() * 4);
     const int wl = std::max(0, p.wait_limit);
@@ -739,13 +767,14 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
 
 int Colony::run_rows(int mode, float trail)
 {
-    CK(launch_rows(uargs_d_, row_base_d_, (int)inst.size(), total_rows, mode, trail, sm_count, st));
+    CK(launch_rows(uargs_d_, row_base_d_, inst.size() > 1 ? row_inst_d_ : nullptr, total_rows, mode, trail, sm_count,
+                   st));
     return ACO_OK;
 }
 
 int Colony::run_rows_one(int b, int mode)
 {
-    CK(launch_rows(uargs_d_ + b, zero_base_d_, 1, inst[b].n, mode, 0.f, sm_count, st));
+    CK(launch_rows(uargs_d_ + b, zero_base_d_, nullptr, inst[b].n, mode, 0.f, sm_count, st));
     return ACO_OK;
 }
 
@@ -764,7 +793,11 @@ int Colony::set_prior(int b, const float *prior, int ld)
     }
     int rc = set_device();
     if (rc != ACO_OK) return rc;
+    ih.prior_hash = 0;
     if (prior) {
+        uint64_t hh = kFnvBasis;
+        for (int i = 0; i < n; i++) hh = fnv1a(hh, prior + (size_t)i * ld, sizeof(float) * (size_t)n);
+        ih.prior_hash = hh | 1u; // nonzero: a prior is set
         CK(cudaMemcpy2DAsync(ih.heur_d, (size_t)ih.ld * 4, prior, (size_t)ld * 4, (size_t)n * 4, n,
                              cudaMemcpyHostToDevice, st));
         rc = run_rows_one(b, ROW_PRIOR);
@@ -816,13 +849,15 @@ int Colony::get_best_all(int *tours, size_t cap_ints, int *sizes, float *lengths
 }
 
 // ---- checkpoint ---------------------------------------------------------
-// File: the magic, a header describing the colony (count, then per instance
-// n, A, nloc, mode, K, nn_ls, ras_ranks, record_cap and the fp32 bits of
-// alpha, beta, rho), then per instance its iteration counter, number of
+// File: the magic, a header describing the colony (count and the
+// run-shaping parameters -- seed_time, rnd_seed, ls_flag, ns_rounds,
+// record_cap, mode -- then per instance n, A, nloc, K, nn_ls, ras_ranks, the
+// fp32 bits of alpha, beta, rho, and the 64-bit hashes of the instance's data
+// and of its prior), then per instance its iteration counter, number of
 // best-so-far records, tau (n x n), tours and lengths (the reference layout),
 // lane seeds and records.  Integers and floats are stored in host byte order.
 namespace {
-constexpr char kMagic[8] = {'A', 'C', 'O', 'C', 'K', 'P', 'T', '1'};
+constexpr char kMagic[8] = {'A', 'C', 'O', 'C', 'K', 'P', 'T', '2'};
 
 struct FileCloser {
     FILE *f;
@@ -836,13 +871,17 @@ struct FileCloser {
 static std::vector<int> checkpoint_header(const Colony &c)
 {
     std::vector<int> h;
-    h.push_back((int)c.inst.size());
+    const int run[] = {(int)c.inst.size(), c.p.seed_time, c.p.rnd_seed, c.p.ls_flag, c.p.ns_rounds, c.p.record_cap,
+                       c.p.mode};
+    h.insert(h.end(), run, run + sizeof(run) / sizeof(run[0]));
     for (const InstHost &ih : c.inst) {
         int a, b, r;
         std::memcpy(&a, &c.p.alpha, 4);
         std::memcpy(&b, &c.p.beta, 4);
         std::memcpy(&r, &c.p.rho, 4);
-        const int v[] = {ih.n, ih.A, ih.nloc, c.p.mode, ih.K, ih.nn_ls, ih.R, c.p.record_cap, a, b, r};
+        const int v[] = {ih.n, ih.A, ih.nloc, ih.K, ih.nn_ls, ih.R, a, b, r,
+                         (int)(uint32_t)ih.data_hash, (int)(uint32_t)(ih.data_hash >> 32),
+                         (int)(uint32_t)ih.prior_hash, (int)(uint32_t)(ih.prior_hash >> 32)};
         h.insert(h.end(), v, v + sizeof(v) / sizeof(v[0]));
     }
     return h;
@@ -937,8 +976,9 @@ int Colony::load_checkpoint(const char *path)
     return rc;
 }
 
-int Colony::construct(bool fused)
+int Colony::construct(bool in_iteration)
 {
+    const bool fused = in_iteration;
     if (p.mode != ACO_MODE_THROUGHPUT) {
         CK(launch_construct_parity(cargs_h_[0], cp_wpa, cp_apc, cp_stage, st));
         return ACO_OK;
@@ -952,8 +992,10 @@ int Colony::construct(bool fused)
         CK(cudaMemsetAsync(ls_list_ctr_d_, 0, 16, st));
     }
     routes_pending_ = use_routes_ && lsw == 0;
+    // inside an iteration the 2-opt follows and, with the route list, writes every tour length
+    const bool lens_later = in_iteration && routes_pending_ && (p.ls_flag & 1);
     CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st, lsw,
-                           cn_draw));
+                           cn_draw, lens_later));
     return ACO_OK;
 }
 

@@ -34,6 +34,8 @@ struct InstHost {
     int n = 0, ld = 0, n4 = 0, A = 0, T = 0, K = 0, Kp = 8, nn_ls = 0, R = 0, nloc = 0, lg = 0, kmax = 0;
     int capacity = 0;
     float max_dist = 0, serv_time = 0;
+    uint64_t data_hash = 0;  // FNV-1a of the instance's data (checkpoint identity)
+    uint64_t prior_hash = 0; // of the prior set by set_prior (0: none)
     bool smat = false, packed = false, gtab = false;
     bool device_prep = false;              // distances and lists computed on the device
     const float *x = nullptr, *y = nullptr; // caller's coordinates (valid during create)
@@ -67,7 +69,9 @@ public:
     int clear_status();          // sync_status, then reset the sticky status to ACO_OK
     int set_wait_limit(int polls); // poll limit of the device waits (0 = default), from the next launch
     int launches_per_iteration() const; // kernel launches of one iteration (graph nodes)
-    int construct(bool fused = false); // fused: with the 2-opt warps when configured
+    // in_iteration: the 2-opt follows (fused 2-opt warps when configured; with the
+    // route list the 2-opt writes the tour lengths); false: the phase alone
+    int construct(bool in_iteration = false);
     int local_search();
     int neighbourhood(); // the random-descent stage (ns_rounds > 0)
     int stats(bool elites);
@@ -142,7 +146,7 @@ private:
     int *ls_list_d_ = nullptr, *ls_list_ctr_d_ = nullptr; // ants left to the per-ant 2-opt
     bool last_fused_ = false;
     int *queue_d_ = nullptr, *ant_inst_d_ = nullptr, *ant_base_d_ = nullptr;
-    int *row_base_d_ = nullptr, *zero_base_d_ = nullptr;
+    int *row_base_d_ = nullptr, *zero_base_d_ = nullptr, *row_inst_d_ = nullptr;
     int *slot_base_d_ = nullptr, *valid_d_ = nullptr, *invalid_d_ = nullptr;
     std::vector<int> slot_base_h_, tour_base_h_;
     float *lens_all_d_ = nullptr;

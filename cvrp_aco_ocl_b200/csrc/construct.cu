@@ -598,9 +598,11 @@ __device__ __noinline__ FallbackPick fallback_pick(const float *row, const int *
             mind};
 }
 
+// lens_later: the route-level 2-opt follows and writes every listed ant's
+// length, so the construct leaves it out (error paths still write +inf).
 template <bool FIN, bool SMAT, bool PACKED, bool REGVIS, bool GTAB = false, bool LSF = false, bool DRAW = false>
 __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int apc, int ant0, unsigned char *smem, uint32_t phase,
-                                  int lsw = 0)
+                                  int lsw = 0, bool lens_later = false)
 {
     const int n = a.n, ld = a.ld, K = a.K, Kp = a.Kp, T = a.T;
     const int n4 = (n + 3) & ~3;
@@ -855,23 +857,34 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             __syncwarp();
             for (int p = lane; p < size; p += 32) tour[p] = tbuf[p];
             // tour length: the fp32 sum of the edges in step order (kernel.cl:475,483); after the
-            // fused 2-opt, of its edge lengths in position order (kernel.cl:534-538)
+            // fused 2-opt, of its edge lengths in position order (kernel.cl:534-538).  Four
+            // chunks of 32 edges have their loads in flight before their sums.
             const float *f_dt = reinterpret_cast<const float *>(smem + L.dt) + (size_t)warp * 2 * n;
             float tdist = 0.f;
-            for (int base = 0; base < size - 1; base += 32) {
-                const int p = base + lane;
-                const float e = p < size - 1 ? (use_dt ? f_dt[p] : __ldg(a.dist + (size_t)tbuf[p] * ld + tbuf[p + 1]))
-                                             : 0.f;
-                const int m = size - 1 - base < 32 ? size - 1 - base : 32;
+            if (!lens_later) {
+                for (int base = 0; base < size - 1; base += 128) {
+                    float e[4];
 #pragma unroll
-                for (int k = 0; k < 32; k++) {
-                    const float y = __shfl_sync(FULL, e, k);
-                    if (k < m) tdist = __fadd_rn(tdist, y);
+                    for (int c = 0; c < 4; c++) {
+                        const int p = base + 32 * c + lane;
+                        e[c] = p < size - 1
+                                   ? (use_dt ? f_dt[p] : __ldg(a.dist + (size_t)tbuf[p] * ld + tbuf[p + 1]))
+                                   : 0.f;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const int m = size - 1 - (base + 32 * c);
+#pragma unroll
+                        for (int k = 0; k < 32; k++) {
+                            const float y = __shfl_sync(FULL, e[c], k);
+                            if (k < m) tdist = __fadd_rn(tdist, y);
+                        }
+                    }
                 }
             }
             if (lane == 0) {
                 tour[T - 1] = size;
-                a.lens[ant] = tdist;
+                if (!lens_later) a.lens[ant] = tdist;
             }
             if (!LSF && a.route_desc) emit_routes(a, tbuf, size, a.ant_base + ant, lane);
         }
@@ -885,26 +898,26 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
 // register or shared visited set, with or without helper-warp draws.
 template <bool FIN, bool DRAW>
 __device__ __forceinline__ bool construct_nn_plain(const ConstructArgs &a, int apc, int ant0, unsigned char *smem,
-                                                   uint32_t phase)
+                                                   uint32_t phase, bool ll)
 {
     if (a.gtab)
-        return a.packed ? construct_nn_item<FIN, false, true, false, true, false, DRAW>(a, apc, ant0, smem, phase)
-                        : construct_nn_item<FIN, false, false, false, true, false, DRAW>(a, apc, ant0, smem, phase);
+        return a.packed ? construct_nn_item<FIN, false, true, false, true, false, DRAW>(a, apc, ant0, smem, phase, 0, ll)
+                        : construct_nn_item<FIN, false, false, false, true, false, DRAW>(a, apc, ant0, smem, phase, 0, ll);
     if (a.n <= 1024) {
         if (a.smat)
-            return a.packed ? construct_nn_item<FIN, true, true, true, false, false, DRAW>(a, apc, ant0, smem, phase)
-                            : construct_nn_item<FIN, true, false, true, false, false, DRAW>(a, apc, ant0, smem, phase);
-        return a.packed ? construct_nn_item<FIN, false, true, true, false, false, DRAW>(a, apc, ant0, smem, phase)
-                        : construct_nn_item<FIN, false, false, true, false, false, DRAW>(a, apc, ant0, smem, phase);
+            return a.packed ? construct_nn_item<FIN, true, true, true, false, false, DRAW>(a, apc, ant0, smem, phase, 0, ll)
+                            : construct_nn_item<FIN, true, false, true, false, false, DRAW>(a, apc, ant0, smem, phase, 0, ll);
+        return a.packed ? construct_nn_item<FIN, false, true, true, false, false, DRAW>(a, apc, ant0, smem, phase, 0, ll)
+                        : construct_nn_item<FIN, false, false, true, false, false, DRAW>(a, apc, ant0, smem, phase, 0, ll);
     }
-    return a.packed ? construct_nn_item<FIN, false, true, false, false, false, DRAW>(a, apc, ant0, smem, phase)
-                    : construct_nn_item<FIN, false, false, false, false, false, DRAW>(a, apc, ant0, smem, phase);
+    return a.packed ? construct_nn_item<FIN, false, true, false, false, false, DRAW>(a, apc, ant0, smem, phase, 0, ll)
+                    : construct_nn_item<FIN, false, false, false, false, false, DRAW>(a, apc, ant0, smem, phase, 0, ll);
 }
 
 // KIND: 0 = plain, 1 = helper-warp draws, 2 = fused 2-opt (lsw improving warps)
 template <bool FIN, int KIND>
 __device__ __forceinline__ void construct_nn_body(const ConstructArgs *args, const int2 *items, int n_items, int *queue,
-                                                  int apc, int lsw)
+                                                  int apc, int lsw, bool lens_later)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_item;
@@ -933,7 +946,7 @@ __device__ __forceinline__ void construct_nn_body(const ConstructArgs *args, con
             else ok = a.packed ? construct_nn_item<FIN, false, true, true, false, true>(a, apc, ant0, smem, phase, lsw)
                                : construct_nn_item<FIN, false, false, true, false, true>(a, apc, ant0, smem, phase, lsw);
         } else {
-            ok = construct_nn_plain<FIN, KIND == 1>(a, apc, ant0, smem, phase);
+            ok = construct_nn_plain<FIN, KIND == 1>(a, apc, ant0, smem, phase, lens_later && a.route_desc != nullptr);
         }
         if (!ok) break; // uniform: decided by __syncthreads_or
         phase ^= 1u;
@@ -953,18 +966,19 @@ __device__ __forceinline__ void construct_nn_body(const ConstructArgs *args, con
 // residency the staged tables allow on the batched workloads.
 template <bool FIN, int KIND>
 __global__ void __launch_bounds__(512, 1) construct_nn_kernel(const ConstructArgs *args, const int2 *items, int n_items,
-                                                           int *queue, int apc, int lsw)
+                                                           int *queue, int apc, int lsw, int lens_later)
 {
-    construct_nn_body<FIN, KIND>(args, items, n_items, queue, apc, lsw);
+    construct_nn_body<FIN, KIND>(args, items, n_items, queue, apc, lsw, lens_later != 0);
 }
 
 // The helper-warp variant runs one CTA per SM (few ants, latency bound): its
 // registers are not squeezed for a second CTA.
 template <bool FIN>
 __global__ void __launch_bounds__(512, 1) construct_nn_draw_kernel(const ConstructArgs *args, const int2 *items,
-                                                                   int n_items, int *queue, int apc, int lsw)
+                                                                   int n_items, int *queue, int apc, int lsw,
+                                                                   int lens_later)
 {
-    construct_nn_body<FIN, 1>(args, items, n_items, queue, apc, lsw);
+    construct_nn_body<FIN, 1>(args, items, n_items, queue, apc, lsw, lens_later != 0);
 }
 
 template <int WPA, bool FIN, bool SMAT>
@@ -1001,7 +1015,8 @@ size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool p
 }
 
 cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue, int apc,
-                                size_t smem, int sm_count, bool finite_maxd, cudaStream_t st, int ls_warps, bool draw)
+                                size_t smem, int sm_count, bool finite_maxd, cudaStream_t st, int ls_warps, bool draw,
+                                bool lens_later)
 {
     if (ls_warps > 0) draw = false;
     auto kern = ls_warps > 0 ? (finite_maxd ? construct_nn_kernel<true, 2> : construct_nn_kernel<false, 2>)
@@ -1018,7 +1033,7 @@ cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items
     if (draw && warps < 2 * apc) warps = 2 * apc;
     if (ls_warps > 0) warps = apc + ls_warps;
     if (warps > 16) return cudaErrorInvalidValue;
-    kern<<<blocks, warps * 32, smem, st>>>(d_args, d_items, n_items, d_queue, apc, ls_warps);
+    kern<<<blocks, warps * 32, smem, st>>>(d_args, d_items, n_items, d_queue, apc, ls_warps, lens_later ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -143,9 +143,12 @@ cudaError_t launch_construct_parity(const ConstructArgs &a, int warps_per_ant, i
 // routes of its ants as soon as they are complete (all instances n <= 1024,
 // candidate tables staged); ants with a route of more than 32 nodes are marked
 // in ls_needed for the 2-opt kernel.
+// lens_later: the route-level 2-opt follows in the same iteration and writes
+// the lengths of every ant it gets from the route list; the construct leaves
+// them out for instances that have the list.
 cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue,
                                 int ants_per_cta, size_t smem, int sm_count, bool finite_maxd, cudaStream_t st,
-                                int ls_warps = 0, bool draw = false);
+                                int ls_warps = 0, bool draw = false, bool lens_later = false);
 // 2-opt: one CTA of `warps` warps per ant; d_ant_inst[g] = instance of global ant g,
 // d_ant_base[b] = first global ant of instance b.
 // Route-level 2-opt over the construct's route list (d_ctr: {entries, next,
@@ -168,9 +171,10 @@ cudaError_t launch_local_search(const LocalSearchArgs *d_args, const int *d_ant_
 cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st,
                          const StatsArgs *one = nullptr);
 // Row passes (heuristic matrix, pheromone init, fused update, candidate gather):
-// one warp per row over all instances; d_row_base[b] = first global row of instance b.
-cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, int n_inst, int total_rows, int mode,
-                        float trail, int sm_count, cudaStream_t st);
+// one warp per row over all instances; d_row_base[b] = first global row of instance b,
+// d_row_inst[g] = the instance of global row g (null: one instance).
+cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, const int *d_row_inst, int total_rows,
+                        int mode, float trail, int sm_count, cudaStream_t st);
 cudaError_t launch_t0(unsigned long long *t0, cudaStream_t st);
 
 // Shared-memory bytes of the launches (the host picks configurations that fit

@@ -614,14 +614,26 @@ __global__ void __launch_bounds__(512, 2) route_opt_kernel(const LocalSearchArgs
             __threadfence();
             const int size = __ldcg(gt + a.T - 1);
             float len = 0.f;
-            for (int base = 0; base < size - 1; base += 32) {
-                const int p = base + lane;
-                const float e = p < size - 1 ? __ldg(a.dist + (size_t)__ldcg(gt + p) * a.ld + __ldcg(gt + p + 1)) : 0.f;
-                const int m = size - 1 - base < 32 ? size - 1 - base : 32;
+            // four chunks of 32 edges: their tour and distance loads in flight before the sums
+            for (int base = 0; base < size - 1; base += 128) {
+                int u[4], w[4];
+                float e[4];
 #pragma unroll
-                for (int k = 0; k < 32; k++) {
-                    const float x = __shfl_sync(FULL, e, k);
-                    if (k < m) len = __fadd_rn(len, x);
+                for (int c = 0; c < 4; c++) {
+                    const int p = base + 32 * c + lane;
+                    u[c] = p < size - 1 ? __ldcg(gt + p) : 0;
+                    w[c] = p < size - 1 ? __ldcg(gt + p + 1) : 0;
+                }
+#pragma unroll
+                for (int c = 0; c < 4; c++) e[c] = __ldg(a.dist + (size_t)u[c] * a.ld + w[c]);
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int m = size - 1 - (base + 32 * c);
+#pragma unroll
+                    for (int k = 0; k < 32; k++) {
+                        const float x = __shfl_sync(FULL, e[c], k);
+                        if (k < m) len = __fadd_rn(len, x);
+                    }
                 }
             }
             if (lane == 0) a.lens[ant] = len;

@@ -282,9 +282,12 @@ __global__ void __launch_bounds__(TPB) node_gemm_kernel(int N, const float *h, c
     tmem_teardown(tm, 256);
 }
 
-// Edge layer forward on tiles of npt = 128/k nodes.
+// Edge layer forward on tiles of npt = 128/k nodes.  M: the tile's 128 rows of
+// 64 fp32 values at row stride MS (the accumulator, then the gated messages),
+// padded so that the TMEM-lane-per-row writes fall in distinct banks.
+constexpr int MS = H + 1;
 struct EdgeFwdSmem {
-    static constexpr size_t A = 0, B = A + 128 * H * 2, M = B + H * H * 2, BYTES = M + 128 * H * 4;
+    static constexpr size_t A = 0, B = A + 128 * H * 2, M = B + H * H * 2, BYTES = M + 128 * MS * 4;
 };
 
 __global__ void __launch_bounds__(TPB) edge_fwd_kernel(int N, int k, const float *Wt, const float *a_bias,
@@ -309,31 +312,46 @@ __global__ void __launch_bounds__(TPB) edge_fwd_kernel(int N, int k, const float
         operands_ready();
         gemm_issue(tm, As, Bs, H, H, false);
         if (!gemm_wait(&bar, phase, status)) break;
-        const int r = threadIdx.x;
-        float d[64];
-        tmem_row64(tm, 0, d);
-        if (r < rows) {
-            const size_t ei = e0 + r;
-            const int src = n0 + r / k;
-            int j = nbr[ei];
-            if ((unsigned)j >= (unsigned)N) { // a neighbour id outside the batch: report, read node 0
-                set_status(status, ACO_ERR_INVALID);
-                j = 0;
-            }
-            const float *Pi = P + (size_t)src * 4 * H, *Pj = P + (size_t)j * 4 * H;
-            for (int c = 0; c < H; c++) {
-                const float qv = d[c] + a_bias[c] + Pi[2 * H + c] + Pj[3 * H + c];
-                const float en = e_in[ei * H + c] + fmaxf(qv, 0.f);
-                q_out[ei * H + c] = qv;
-                e_out[ei * H + c] = en;
-                ms[r * H + c] = sigmoidf_(en) * Pj[H + c];
+        {   // the accumulator rows into shared memory (thread r holds TMEM lane r = row r)
+            const int r = threadIdx.x;
+            float d[64];
+            tmem_row64(tm, 0, d);
+#pragma unroll
+            for (int c = 0; c < H; c++) ms[r * MS + c] = d[c];
+        }
+        __syncthreads();
+        // epilogue by rows: a warp takes row r, lane l its channels 2l, 2l+1, so every
+        // global access of e, q and the P rows is one coalesced 256-byte row
+        {
+            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, c = 2 * lane;
+            const float2 ab = *reinterpret_cast<const float2 *>(a_bias + c);
+            for (int r = warp; r < rows; r += TPB / 32) {
+                const size_t ei = e0 + r;
+                const int src = n0 + r / k;
+                int j = nbr[ei];
+                if ((unsigned)j >= (unsigned)N) { // a neighbour id outside the batch: report, read node 0
+                    if (lane == 0) set_status(status, ACO_ERR_INVALID);
+                    j = 0;
+                }
+                const float *Pi = P + (size_t)src * 4 * H, *Pj = P + (size_t)j * 4 * H;
+                const float2 pi = *reinterpret_cast<const float2 *>(Pi + 2 * H + c);
+                const float2 pj = *reinterpret_cast<const float2 *>(Pj + 3 * H + c);
+                const float2 vj = *reinterpret_cast<const float2 *>(Pj + H + c);
+                const float2 ein = *reinterpret_cast<const float2 *>(e_in + ei * H + c);
+                float *mr = ms + r * MS + c;
+                const float q0 = mr[0] + ab.x + pi.x + pj.x, q1 = mr[1] + ab.y + pi.y + pj.y;
+                const float en0 = ein.x + fmaxf(q0, 0.f), en1 = ein.y + fmaxf(q1, 0.f);
+                *reinterpret_cast<float2 *>(q_out + ei * H + c) = make_float2(q0, q1);
+                *reinterpret_cast<float2 *>(e_out + ei * H + c) = make_float2(en0, en1);
+                mr[0] = sigmoidf_(en0) * vj.x; // the gated message replaces the accumulator
+                mr[1] = sigmoidf_(en1) * vj.y;
             }
         }
         __syncthreads();
         for (int idx = threadIdx.x; idx < nodes * H; idx += blockDim.x) {
             const int qn = idx / H, c = idx - qn * H, i = n0 + qn;
             float acc = 0.f;
-            for (int j = 0; j < k; j++) acc += ms[(qn * k + j) * H + c];
+            for (int j = 0; j < k; j++) acc += ms[(qn * k + j) * MS + c];
             const float uv = P[(size_t)i * 4 * H + c] + acc / (float)k;
             u_out[(size_t)i * H + c] = uv;
             h_out[(size_t)i * H + c] = h_in[(size_t)i * H + c] + fmaxf(uv, 0.f);

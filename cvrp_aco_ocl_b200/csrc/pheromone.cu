@@ -13,9 +13,11 @@
 // compute_total_info (:782-789) as one pass: one warp per matrix row, float4
 // loads and stores; it reads tau and heur (= eta^beta, precomputed once) and
 // writes tau and total_info -- 16 bytes of HBM traffic per element -- and, in
-// throughput mode, the total_info of the row's candidates (re-read from L2
-// after the row is written) into the compact candidate table the construct
-// kernel loads by TMA.
+// throughput mode, the reciprocal total_info of the row's candidates (re-read
+// from L2 after the row is written) into the compact candidate table the
+// construct kernel loads by TMA.  The deposit is added inside the stream: the
+// lane holding a deposit column's float4 adds the elites' amounts in elite
+// order before total_info is formed, so no column is read twice.
 #include <cuda_runtime.h>
 
 #include "aco_device.cuh"
@@ -220,45 +222,22 @@ __global__ void __launch_bounds__(1024) stats_kernel(const StatsArgs *args, Stat
     if (tid == 0) *a.iteration = iter + 1; // main.cpp:86 (Problem::iteration++)
 }
 
-// Deposit of elite ranks into one float4 of row i (columns c4..c4+3), in
-// elite order 0, 1, ..., R-1 -- the order the oracle applies the deposit in.
-__device__ __forceinline__ void deposit4(const UpdateArgs &a, int i, int c4, const int (&sr)[8], const float (&dr)[8],
-                                         float &v0, float &v1, float &v2, float &v3)
+// Deposit into one float4 of the depot row (columns c4..c4+3): depot ->
+// customer edges from the per-column elite masks, in elite order 0, 1, ...,
+// R-1 -- the order the oracle applies the deposit in.
+__device__ __forceinline__ void deposit4_depot(const UpdateArgs &a, int c4, float &v0, float &v1, float &v2, float &v3)
 {
     const int R = a.ras_ranks, n = a.n;
-    if (i != 0) {
-#pragma unroll
-        for (int r = 0; r < 8; r++) {
-            const unsigned d = (unsigned)(sr[r] - c4);
-            if (r < R && d < 4u) {
-                if (d == 0) v0 = __fadd_rn(v0, dr[r]);
-                else if (d == 1) v1 = __fadd_rn(v1, dr[r]);
-                else if (d == 2) v2 = __fadd_rn(v2, dr[r]);
-                else v3 = __fadd_rn(v3, dr[r]);
-            }
-        }
-        for (int r = 8; r < R; r++) { // more than 8 ranks: read the rest directly
-            const unsigned d = (unsigned)(__ldg(a.succ + (size_t)r * n + i) - c4);
-            if (d < 4u) {
-                const float dt = __ldg(a.d_tau + r);
-                if (d == 0) v0 = __fadd_rn(v0, dt);
-                else if (d == 1) v1 = __fadd_rn(v1, dt);
-                else if (d == 2) v2 = __fadd_rn(v2, dt);
-                else v3 = __fadd_rn(v3, dt);
-            }
-        }
-    } else { // depot row: depot -> customer edges from the per-column masks
-        const uint32_t m0 = c4 + 0 < n ? __ldg(a.depmask + c4 + 0) : 0u;
-        const uint32_t m1 = c4 + 1 < n ? __ldg(a.depmask + c4 + 1) : 0u;
-        const uint32_t m2 = c4 + 2 < n ? __ldg(a.depmask + c4 + 2) : 0u;
-        const uint32_t m3 = c4 + 3 < n ? __ldg(a.depmask + c4 + 3) : 0u;
-        for (int r = 0; r < R; r++) {
-            const float dt = __ldg(a.d_tau + r);
-            if ((m0 >> r) & 1u) v0 = __fadd_rn(v0, dt);
-            if ((m1 >> r) & 1u) v1 = __fadd_rn(v1, dt);
-            if ((m2 >> r) & 1u) v2 = __fadd_rn(v2, dt);
-            if ((m3 >> r) & 1u) v3 = __fadd_rn(v3, dt);
-        }
+    const uint32_t m0 = c4 + 0 < n ? __ldg(a.depmask + c4 + 0) : 0u;
+    const uint32_t m1 = c4 + 1 < n ? __ldg(a.depmask + c4 + 1) : 0u;
+    const uint32_t m2 = c4 + 2 < n ? __ldg(a.depmask + c4 + 2) : 0u;
+    const uint32_t m3 = c4 + 3 < n ? __ldg(a.depmask + c4 + 3) : 0u;
+    for (int r = 0; r < R; r++) {
+        const float dt = __ldg(a.d_tau + r);
+        if ((m0 >> r) & 1u) v0 = __fadd_rn(v0, dt);
+        if ((m1 >> r) & 1u) v1 = __fadd_rn(v1, dt);
+        if ((m2 >> r) & 1u) v2 = __fadd_rn(v2, dt);
+        if ((m3 >> r) & 1u) v3 = __fadd_rn(v3, dt);
     }
 }
 
@@ -266,18 +245,38 @@ __device__ __forceinline__ void deposit4(const UpdateArgs &a, int i, int c4, con
 // issued before its arithmetic, so a lane keeps four float4 of each input
 // matrix in flight.
 constexpr int kU = 4;
+constexpr int kRowWarps = 8; // warps (rows in flight) per CTA of the row kernel
 
-// Evaporation + total_info over one customer row, U float4 per lane per chunk
-// (A1: alpha == 1, so tau^alpha is tau itself).  The deposit columns are fixed
-// up afterwards (row_pass).
+// Evaporation + deposit + total_info over customer row i, U float4 per lane
+// per chunk.  Lanes r < R first read elite r's successor column of node i and
+// its amount into the warp's slots s_col / s_amt; every lane then marks which
+// of its float4 (index k: columns 4 * (lane + 32k) .. + 3) hold a deposit
+// column -- bit k for k < 32, one flag for all later ones (rows past 4096) --
+// and only those take the deposit loop.
 template <int U, bool A1>
-__device__ __forceinline__ void evaporate_row(const UpdateArgs &a, int lane, int q4, float4 *tau4,
-                                              const float4 *heur4, float4 *tot4)
+__device__ __forceinline__ void update_row_stream(const UpdateArgs &a, int i, int lane, int q4, float4 *tau4,
+                                                  const float4 *heur4, float4 *tot4, int *s_col, float *s_amt)
 {
+    const int R = a.ras_ranks, n = a.n;
+    if (lane < R) {
+        s_col[lane] = __ldg(a.succ + (size_t)lane * n + i);
+        s_amt[lane] = __ldg(a.d_tau + lane);
+    }
+    __syncwarp();
+    uint32_t depk = 0;
+    bool depfar = false;
+    for (int r = 0; r < R; r++) {
+        const int c = s_col[r];
+        if (c >= 0 && ((c >> 2) & 31) == lane) {
+            if (c < 4096) depk |= 1u << (c >> 7);
+            else depfar = true;
+        }
+    }
     const float evap = a.evap;
     float4 *tp = tau4 + lane, *op = tot4 + lane;
     const float4 *hp = heur4 + lane;
-    for (int left = q4 - lane; left > 0; left -= 32 * U, tp += 32 * U, op += 32 * U, hp += 32 * U) {
+    int k0 = 0;
+    for (int left = q4 - lane; left > 0; left -= 32 * U, tp += 32 * U, op += 32 * U, hp += 32 * U, k0 += U) {
         float4 t[U], h[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -294,6 +293,19 @@ __device__ __forceinline__ void evaporate_row(const UpdateArgs &a, int lane, int
                 o.y = __fmul_rn(evap, t[u].y);
                 o.z = __fmul_rn(evap, t[u].z);
                 o.w = __fmul_rn(evap, t[u].w);
+                if (k0 + u < 32 ? (depk >> (k0 + u)) & 1u : depfar) { // kernel.cl:747-776, elite order
+                    const int c4 = 4 * (lane + 32 * (k0 + u));
+                    for (int r = 0; r < R; r++) {
+                        const unsigned d = (unsigned)(s_col[r] - c4);
+                        if (d < 4u) {
+                            const float dt = s_amt[r];
+                            if (d == 0) o.x = __fadd_rn(o.x, dt);
+                            else if (d == 1) o.y = __fadd_rn(o.y, dt);
+                            else if (d == 2) o.z = __fadd_rn(o.z, dt);
+                            else o.w = __fadd_rn(o.w, dt);
+                        }
+                    }
+                }
                 if (A1) {
                     tot.x = __fmul_rn(o.x, h[u].x);
                     tot.y = __fmul_rn(o.y, h[u].y);
@@ -310,6 +322,7 @@ __device__ __forceinline__ void evaporate_row(const UpdateArgs &a, int lane, int
             }
         }
     }
+    __syncwarp(); // s_col / s_amt are reused by the warp's next row
 }
 
 // Depot row: every column may receive deposits (depot -> customer edges of
@@ -317,13 +330,11 @@ __device__ __forceinline__ void evaporate_row(const UpdateArgs &a, int lane, int
 __device__ __forceinline__ void update_depot_row(const UpdateArgs &a, int lane, int q4, float4 *tau4,
                                                  const float4 *heur4, float4 *tot4)
 {
-    const int sr[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
-    const float dr[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int q = lane; q < q4; q += 32) {
         const float4 t = tau4[q], h = heur4[q];
         float v0 = __fmul_rn(a.evap, t.x), v1 = __fmul_rn(a.evap, t.y);
         float v2 = __fmul_rn(a.evap, t.z), v3 = __fmul_rn(a.evap, t.w);
-        deposit4(a, 0, 4 * q, sr, dr, v0, v1, v2, v3);
+        deposit4_depot(a, 4 * q, v0, v1, v2, v3);
         float4 o, tot;
         o.x = v0; o.y = v1; o.z = v2; o.w = v3;
         tot.x = __fmul_rn(pow_rule(v0, a.alpha, a.alpha_int), h.x);
@@ -336,10 +347,14 @@ __device__ __forceinline__ void update_depot_row(const UpdateArgs &a, int lane, 
 }
 
 // One warp, row i of instance a.  Columns are walked as float4 (ld is a
-// multiple of 32; columns n..ld-1 stay zero).
-__device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, float trail, int lane)
+// multiple of 32; columns n..ld-1 stay zero).  s_col / s_amt: the warp's
+// deposit slots (32 entries each).
+__device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, float trail, int lane, int *s_col,
+                                         float *s_amt)
 {
     const int n = a.n, q4 = (n + 3) >> 2;
+    // the row's candidate ids, fetched with the row's first loads (ROW_GATHER reads them after the row)
+    const int cid = a.chc && lane < a.K ? (int)__ldg(a.nn16 + (size_t)i * a.Kp + lane) : 0;
     const size_t off = (size_t)i * a.ld;
     const float4 *heur4 = reinterpret_cast<const float4 *>(a.heur + off);
     float4 *tau4 = reinterpret_cast<float4 *>(a.tau + off);
@@ -396,55 +411,33 @@ __device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, f
         if (i == 0) {
             update_depot_row(a, lane, q4, tau4, heur4, tot4);
         } else {
-            if (a.alpha_int == 1) evaporate_row<kU, true>(a, lane, q4, tau4, heur4, tot4);
-            else evaporate_row<1, false>(a, lane, q4, tau4, heur4, tot4);
-            // deposit (kernel.cl:747-776): lane r < R owns the successor of
-            // customer i in elite r's tour.  It re-reads the evaporated value
-            // this warp just wrote and adds every elite's deposit on that edge
-            // in elite order, so lanes of elites sharing the edge write the same
-            // value; total_info of the column is recomputed from the result.
-            const int R = a.ras_ranks;
-            int c = -1;
-            if (lane < R) c = __ldg(a.succ + (size_t)lane * n + i);
-            __syncwarp();
-            if (c >= 0) {
-                float v = a.tau[off + c];
-                for (int r = 0; r < R; r++)
-                    if (__ldg(a.succ + (size_t)r * n + i) == c) v = __fadd_rn(v, __ldg(a.d_tau + r));
-                a.total[off + c] = __fmul_rn(pow_rule(v, a.alpha, a.alpha_int), a.heur[off + c]);
-                a.tau[off + c] = v;
-            }
+            if (a.alpha_int == 1) update_row_stream<kU, true>(a, i, lane, q4, tau4, heur4, tot4, s_col, s_amt);
+            else update_row_stream<1, false>(a, i, lane, q4, tau4, heur4, tot4, s_col, s_amt);
         }
     }
     if (a.chc) { // compact candidate table: chc[i][j] = 1 / total[i][nn[i][j]] (the race's reciprocal weight)
         // the row was written by this warp; __syncwarp orders those stores before
         // the re-reads below (they hit L2, the lines were just written)
         __syncwarp();
-        for (int j = lane; j < a.K; j += 32)
-            a.chc[(size_t)i * a.Kp + j] = __fdiv_rn(1.0f, a.total[off + a.nn16[(size_t)i * a.Kp + j]]);
+        if (lane < a.K) a.chc[(size_t)i * a.Kp + lane] = __fdiv_rn(1.0f, a.total[off + cid]);
     }
 }
 
+// Global row g (over the instances' rows in order) belongs to instance
+// row_inst[g] (null: a single instance); row_base[b] is instance b's first.
 template <int MODE>
-__global__ void __launch_bounds__(256, 4) rows_kernel(const UpdateArgs *args, const int *row_base, int n_inst,
-                                                      int total_rows, float trail)
+__global__ void __launch_bounds__(kRowWarps * 32, 4) rows_kernel(const UpdateArgs *args, const int *row_base,
+                                                                 const int *row_inst, int total_rows, float trail)
 {
     constexpr int mode = MODE;
-    const int lane = threadIdx.x & 31;
+    __shared__ int s_col[kRowWarps][32];
+    __shared__ float s_amt[kRowWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    int b = 0;
     for (int g = gw; g < total_rows; g += nw) {
-        if (n_inst > 1) { // instance of global row g: binary search over the first rows
-            int lo = 0, hi = n_inst;
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (__ldg(row_base + mid) <= g) lo = mid;
-                else hi = mid;
-            }
-            b = lo;
-        }
-        row_pass(args[b], g - __ldg(row_base + b), mode, trail, lane);
+        const int b = row_inst ? __ldg(row_inst + g) : 0;
+        row_pass(args[b], g - __ldg(row_base + b), mode, trail, lane, s_col[warp], s_amt[warp]);
     }
 }
 
@@ -472,31 +465,31 @@ cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, siz
     return cudaGetLastError();
 }
 
-cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, int n_inst, int total_rows, int mode,
-                        float trail, int sm_count, cudaStream_t st)
+cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, const int *d_row_inst, int total_rows,
+                        int mode, float trail, int sm_count, cudaStream_t st)
 {
-    int blocks = (total_rows + 7) / 8; // 8 warps (rows) per CTA
+    int blocks = (total_rows + kRowWarps - 1) / kRowWarps; // one warp per row
     const int cap = sm_count * 4;      // grid-stride beyond 4 CTAs (32 warps) per SM
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     switch (mode) {
-    case ROW_HEUR: rows_kernel<ROW_HEUR><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail); break;
+    case ROW_HEUR: rows_kernel<ROW_HEUR><<<blocks, kRowWarps * 32, 0, st>>>(d_args, d_row_base, d_row_inst, total_rows, trail); break;
     case ROW_INIT_TRAIL:
-        rows_kernel<ROW_INIT_TRAIL><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        rows_kernel<ROW_INIT_TRAIL><<<blocks, kRowWarps * 32, 0, st>>>(d_args, d_row_base, d_row_inst, total_rows, trail);
         break;
     case ROW_INIT_BSF:
-        rows_kernel<ROW_INIT_BSF><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        rows_kernel<ROW_INIT_BSF><<<blocks, kRowWarps * 32, 0, st>>>(d_args, d_row_base, d_row_inst, total_rows, trail);
         break;
     case ROW_UPDATE:
-        rows_kernel<ROW_UPDATE><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        rows_kernel<ROW_UPDATE><<<blocks, kRowWarps * 32, 0, st>>>(d_args, d_row_base, d_row_inst, total_rows, trail);
         break;
     case ROW_PRIOR:
-        rows_kernel<ROW_PRIOR><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        rows_kernel<ROW_PRIOR><<<blocks, kRowWarps * 32, 0, st>>>(d_args, d_row_base, d_row_inst, total_rows, trail);
         break;
     case ROW_TOTAL:
-        rows_kernel<ROW_TOTAL><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail);
+        rows_kernel<ROW_TOTAL><<<blocks, kRowWarps * 32, 0, st>>>(d_args, d_row_base, d_row_inst, total_rows, trail);
         break;
-    default: rows_kernel<ROW_GATHER><<<blocks, 256, 0, st>>>(d_args, d_row_base, n_inst, total_rows, trail); break;
+    default: rows_kernel<ROW_GATHER><<<blocks, kRowWarps * 32, 0, st>>>(d_args, d_row_base, d_row_inst, total_rows, trail); break;
     }
     return cudaGetLastError();
 }

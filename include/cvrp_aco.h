@@ -263,9 +263,9 @@ int aco_write_solution(aco_solver *s, const char *path);
  * tours and lengths (best-so-far slot included), the lane seeds, the
  * best-so-far records and the iteration counter -- after aco_init.
  * aco_load_checkpoint restores it into a solver created with the same
- * instance and parameters (ACO_ERR_INVALID otherwise; a prior must be set
- * again before loading); total_info and the candidate table are recomputed
- * from tau.  The iterations after a load are bit-identical to the ones the
+ * instance data, seeds and parameters and holding the same prior (the file
+ * records a hash of each instance's data and prior; ACO_ERR_INVALID
+ * otherwise); total_info and the candidate table are recomputed from tau.  The iterations after a load are bit-identical to the ones the
  * saving solver would have run.  Record times restart from the load. */
 int aco_save_checkpoint(aco_solver *s, const char *path);
 int aco_load_checkpoint(aco_solver *s, const char *path);

@@ -85,3 +85,25 @@ def test_batch_resume_is_bit_exact(gpu, tmp_path):
         R.iterate(2)
         got = [R.solutions(b) + R.pheromone(b) for b in range(3)]
     assert all(np.array_equal(x, y) for g, w in zip(got, want) for x, y in zip(g, w))
+
+
+def test_checkpoint_rejects_another_instance_seed_or_prior(gpu, tmp_path):
+    """A checkpoint names the instance it was saved for (a hash of its data),
+    its seeds, its stages and its prior: a solver for another instance of the
+    same size, with other seeds, another local-search stage or another prior
+    does not load it."""
+    a, b = I.gen_mixed(21, 70), I.gen_mixed(22, 70)
+    pa, pb = Problem.from_instance(a), Problem.from_instance(b)
+    path = str(tmp_path / "ck.bin")
+    with Solver(pa, params(a.n, 24, MODE_THROUGHPUT)) as S:
+        S.init()
+        S.save_checkpoint(path)
+    for prob, kw in ((pb, {}), (pa, {"rnd_seed": 9}), (pa, {"ls_flag": 3})):
+        with Solver(prob, params(a.n, 24, MODE_THROUGHPUT, **kw)) as R, pytest.raises(AcoError):
+            R.load_checkpoint(path)
+    with Solver(pa, params(a.n, 24, MODE_THROUGHPUT)) as R:  # prior set after the save: refused
+        R.set_prior(np.full((a.n, a.n), 0.5, np.float32))
+        with pytest.raises(AcoError):
+            R.load_checkpoint(path)
+        R.set_prior(None)  # back to the plain colony: accepted
+        R.load_checkpoint(path)
