@@ -221,8 +221,9 @@ def kernel_rooflines(phase_ms, steps, row_bytes, clk, peak_hbm, peak_src, worklo
                       "frac": ach / issue_peak if ach is not None else None,
                       "warp_instructions_per_launch": inst,
                       "peak_source": f"148 SMs x 4 issue slots x {mhz:.0f} MHz (sampled)",
-                      "smem_frac_ncu": profile_figure("smem_pipe_frac", f"{ks[0]}@{workload_tag}"),
-                      "issue_active_ncu": profile_figure("issue_active_frac", f"{ks[0]}@{workload_tag}"),
+                      # fractions of the same kernel on the 64-instance cut of the batch (multi-pass capture)
+                      "smem_frac_ncu": profile_figure("smem_pipe_frac", f"{ks[0]}@batch64"),
+                      "issue_active_ncu": profile_figure("issue_active_frac", f"{ks[0]}@batch64"),
                       "traffic": sum(v for v in (profile_figure("dram_bytes_per_launch", f"{k2}@{workload_tag}")
                                                  for k2 in ks) if v is not None) or None})
         else:
