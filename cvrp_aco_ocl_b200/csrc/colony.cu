@@ -381,7 +381,12 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         long long cap = 0;
         for (const InstHost &ih : inst) {
             n_max = std::max(n_max, ih.n);
-            cap += (long long)ih.A * std::min(ih.n - 1, 64);
+            // routes per tour: at least total demand / capacity; twice that plus a margin,
+            // and never more than one per customer
+            long long dem = 0;
+            for (int i = 1; i < ih.n; i++) dem += ih.demand[i];
+            const long long per = ih.capacity > 0 ? 2 * ((dem + ih.capacity - 1) / ih.capacity) + 16 : ih.n - 1;
+            cap += (long long)ih.A * std::min<long long>(ih.n - 1, per);
             if (!ih.device_prep) // coordinate formulas are symmetric; a given matrix is checked
                 for (int i = 0; i < ih.n && sym; i++)
                     for (int j = 0; j < i; j++)

@@ -423,30 +423,34 @@ __device__ __forceinline__ void draw_warp(uint32_t xs, float *ring, const int *f
 }
 
 // The route list entries of one finished ant (warp-wide): route r is the
-// positions [depot r, depot r+1) of its tour; routes of at most 32 nodes are
-// listed for the route-level 2-opt, longer ones flag the ant for the per-ant
-// kernel (and so does a full list, for all of its routes).
+// positions [depot r, depot r+1) of its tour, listed as {ant, first position |
+// nodes << 16} for the route-level 2-opt, which improves routes of at most
+// kListedRoute nodes (its local node ids are bytes).  An ant with a longer
+// route, or whose routes do not fit the list, lists none and is flagged
+// (ls_needed 2) for the per-ant kernel, which improves all of its routes.
+constexpr int kListedRoute = 255;
+
 __device__ __forceinline__ void emit_routes(const ConstructArgs &a, const uint16_t *tbuf, int size, int g, int lane)
 {
     const unsigned FULL = 0xffffffffu;
-    int nshort = 0, prev = 0;
-    bool longr = false;
+    int nr = 0, prev = 0;
+    bool toolong = false;
     for (int base = 0; base < size; base += 32) { // count
         const int p = base + lane;
         unsigned m = __ballot_sync(FULL, p >= 1 && p < size && tbuf[p < size ? p : 0] == 0);
         while (m) {
             const int q = base + __ffs(m) - 1;
             m &= m - 1;
-            if (q - prev <= 32) nshort++;
-            else longr = true;
+            nr++;
+            toolong = toolong || q - prev > kListedRoute;
             prev = q;
         }
     }
     int rbase = 0;
-    if (lane == 0 && nshort > 0) rbase = atomicAdd(a.route_ctr, nshort);
+    if (lane == 0 && !toolong) rbase = atomicAdd(a.route_ctr, nr);
     rbase = __shfl_sync(FULL, rbase, 0);
-    const bool fits = rbase + nshort <= a.route_cap;
-    if (fits && nshort > 0) { // write
+    const bool fits = !toolong && rbase + nr <= a.route_cap;
+    if (fits) { // write
         int k = 0;
         prev = 0;
         for (int base = 0; base < size; base += 32) {
@@ -455,21 +459,18 @@ __device__ __forceinline__ void emit_routes(const ConstructArgs &a, const uint16
             while (m) {
                 const int q = base + __ffs(m) - 1;
                 m &= m - 1;
-                if (q - prev <= 32) {
-                    if (lane == (k & 31)) a.route_desc[rbase + k] = make_int2(g, prev | ((q - prev) << 20));
-                    k++;
-                }
+                if (lane == (k & 31)) a.route_desc[rbase + k] = make_int2(g, prev | ((q - prev) << 16));
+                k++;
                 prev = q;
             }
         }
+    } else if (!toolong) { // entries of this reservation below the capacity are read: mark them empty
+        for (int k = lane; k < nr && rbase + k < a.route_cap; k += 32) a.route_desc[rbase + k] = make_int2(-1, 0);
     }
-    if (!fits) // entries of this reservation below the capacity are read: mark them empty
-        for (int k = lane; k < nshort && rbase + k < a.route_cap; k += 32) a.route_desc[rbase + k] = make_int2(-1, 0);
     if (lane == 0) {
-        a.route_rem[g] = fits ? nshort : 0;
-        const uint8_t need = (uint8_t)(!fits ? 2 : (longr ? 1 : 0));
-        a.ls_needed[g] = need;
-        if (need) { // one entry per ant and construct: the list holds every ant of the colony
+        a.route_rem[g] = fits ? nr : 0;
+        a.ls_needed[g] = (uint8_t)(fits ? 0 : 2);
+        if (!fits) { // one entry per ant and construct: the list holds every ant of the colony
             const int k = atomicAdd(a.ls_list_ctr, 1);
             a.ls_list[k] = g;
         }

@@ -48,10 +48,11 @@ struct ConstructArgs {
     int nn_ls, pass_limit, ant_base;
     uint8_t *ls_needed;    // total ants of the colony
     // route list for the route-level 2-opt (null: not used): every route of at
-    // most 32 nodes as {global ant, first position | nodes << 20}; route_ctr[0]
+    // most 255 nodes as {global ant, first position | nodes << 16}; route_ctr[0]
     // counts the entries (capacity route_cap), route_rem[g] the entries of ant g.
-    // ls_needed[g]: 1 = the ant also has longer routes, 2 = none of its routes
-    // listed (the list was full) -- the per-ant kernel does those.
+    // ls_needed[g]: 2 = none of its routes listed (a longer route, or the list
+    // was full) -- the per-ant kernel does those; 1 (fused construct only) = the
+    // ant's routes of more than 32 nodes are left to the per-ant kernel.
     int2 *route_desc;
     int *route_ctr, *route_rem;
     int route_cap;

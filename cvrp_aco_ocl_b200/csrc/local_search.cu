@@ -515,19 +515,160 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
 } // namespace
 
 // ---------------------------------------------------------------------------
-// Route-level 2-opt (throughput construct): every route of at most 32 nodes
-// of every ant is one entry of the list the construct kernel wrote, and the
+// Route-level 2-opt (throughput construct): every route of every ant (of at
+// most 255 nodes) is one entry of the list the construct kernel wrote, and the
 // warps of a persistent grid take entries from a counter, so the routes of
 // one ant spread over all SMs instead of queueing in one CTA.  A route needs
 // no state of its ant beyond its own nodes: its membership test is a per-warp
 // node -> local index map in shared memory, set for the route and cleared
-// after it.  The warp that improves an ant's last listed route sums the ant's
+// after it.  Routes of at most 32 nodes run in registers (two_opt.cuh), longer
+// ones through two_opt_route_local.  The warp that improves an ant's last listed route sums the ant's
 // tour length (kernel.cl:534-538) from the distances of its final tour edges,
 // which equal the 2-opt's edge lengths for a symmetric matrix (the only case
 // this kernel is used for); ants flagged for the per-ant kernel get their
 // length there.
 // ---------------------------------------------------------------------------
 constexpr int kRouteRows = 4; // tile rows loaded per round (register budget of two CTAs per SM)
+
+// Routes of 33..255 nodes in the route-level kernel: kernel.cl:126-277 with
+// the route's state in the warp's shared memory (the area of the register
+// path's distance tile) and local node ids: nodes[k] is the global node of
+// local id k (0: the depot), tk[p] the local id at route position p, pk[k] the
+// position of local id k, dq[p] dist_tour_wrk of position p, dlb[k] the
+// don't-look bits; loc[node] is the local id of a customer of the route (0:
+// not in it).  Positions are scanned in order; for each examined node, the
+// warp evaluates 32 entries of its neighbour list at a time, and the first
+// entry that ends the search (past the radius, or an improving move) decides,
+// as in the sequential code; the exchange reverses position ranges pairwise.
+__device__ int two_opt_route_local(int lane, int R, const float *dist, int ld, const int *nn, int nn_ls,
+                                   const uint8_t *loc, const uint16_t *nodes, uint8_t *tk, uint8_t *pk, uint8_t *dlb,
+                                   float *dq, int pass_limit)
+{
+    auto D = [&](int a, int b) { return __ldg(dist + (size_t)a * ld + b); };
+    int passes = 0;
+    bool imp = true;
+    while (imp) {
+        if (pass_limit > 0 && passes >= pass_limit) return ACO_ERR_LS_LIMIT;
+        passes++;
+        imp = false;
+        for (int l = 0; l < R; l++) {
+            const int k1 = tk[l];
+            if (dlb[k1]) continue;
+            const int n1 = nodes[k1];
+            int h1 = 0, h2 = 0, h3 = 0, h4 = 0;
+            bool found = false;
+            {   // successor search (kernel.cl:180-198)
+                const int ks1 = tk[l + 1 < R ? l + 1 : 0];
+                const float radius = D(n1, nodes[ks1]);
+                for (int h0 = 0; h0 < nn_ls; h0 += 32) {
+                    const int h = h0 + lane;
+                    const int n2 = h < nn_ls ? __ldg(nn + (size_t)n1 * nn_ls + h) : 0;
+                    const int kk2 = loc[n2];
+                    bool cond = false, okm = false;
+                    int ks2 = 0;
+                    if (kk2 != 0) {
+                        const float d12 = D(n1, n2);
+                        cond = __fsub_rn(radius, d12) > kEps;
+                        if (cond) {
+                            const int p2 = pk[kk2];
+                            ks2 = tk[p2 + 1 < R ? p2 + 1 : 0];
+                            const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), D(nodes[ks1], nodes[ks2])), dq[p2]);
+                            okm = g < -kEps;
+                        }
+                    }
+                    const unsigned stop = __ballot_sync(FULL, kk2 != 0 && (!cond || okm));
+                    if (stop) {
+                        const int f = __ffs(stop) - 1;
+                        if (__shfl_sync(FULL, (int)cond, f)) {
+                            found = true;
+                            h1 = k1;
+                            h2 = ks1;
+                            h3 = __shfl_sync(FULL, kk2, f);
+                            h4 = __shfl_sync(FULL, ks2, f);
+                        }
+                        break;
+                    }
+                }
+            }
+            if (!found) { // predecessor search (kernel.cl:202-230)
+                const int kp1 = tk[l > 0 ? l - 1 : R - 1];
+                const float radius = D(nodes[kp1], n1);
+                for (int h0 = 0; h0 < nn_ls; h0 += 32) {
+                    const int h = h0 + lane;
+                    const int n2 = h < nn_ls ? __ldg(nn + (size_t)n1 * nn_ls + h) : 0;
+                    const int kk2 = loc[n2];
+                    bool cond = false, okm = false;
+                    int kpp2 = 0;
+                    if (kk2 != 0) {
+                        const float d12 = D(n1, n2);
+                        cond = __fsub_rn(radius, d12) > kEps;
+                        if (cond) {
+                            const int p2 = pk[kk2];
+                            kpp2 = tk[p2 > 0 ? p2 - 1 : R - 1];
+                            if (!(kpp2 == k1 || kp1 == kk2)) {
+                                const float g =
+                                    __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), D(nodes[kp1], nodes[kpp2])), dq[p2 - 1]);
+                                okm = g < -kEps;
+                            }
+                        }
+                    }
+                    const unsigned stop = __ballot_sync(FULL, kk2 != 0 && (!cond || okm));
+                    if (stop) {
+                        const int f = __ffs(stop) - 1;
+                        if (__shfl_sync(FULL, (int)cond, f)) {
+                            found = true;
+                            h1 = kp1;
+                            h2 = k1;
+                            h3 = __shfl_sync(FULL, kpp2, f);
+                            h4 = __shfl_sync(FULL, kk2, f);
+                        }
+                        break;
+                    }
+                }
+            }
+            if (!found) {
+                if (lane == 0) dlb[k1] = 1; // kernel.cl:232
+                __syncwarp();
+                continue;
+            }
+            // exchange (kernel.cl:235-270)
+            imp = true;
+            int p1 = pk[h1], p3 = pk[h3];
+            if (p3 < p1) {
+                int t = h1; h1 = h3; h3 = t;
+                t = h2; h2 = h4; h4 = t;
+                t = p1; p1 = p3; p3 = t;
+            }
+            const int i = p1, jj = p3, a = pk[h2];
+            const float d13 = D(nodes[h1], nodes[h3]), d24 = D(nodes[h2], nodes[h4]);
+            __syncwarp();
+            if (lane == 0) {
+                dlb[h1] = 0;
+                dlb[h2] = 0;
+                dlb[h3] = 0;
+                dlb[h4] = 0;
+                dq[i] = d13;
+                dq[jj] = d24;
+            }
+            for (int k = lane; k < (jj - i - 1) / 2; k += 32) { // dist_tour_wrk (i, jj) reversed
+                const int x = i + 1 + k, y = jj - 1 - k;
+                const float t = dq[x];
+                dq[x] = dq[y];
+                dq[y] = t;
+            }
+            for (int k = lane; k < (jj - a + 1) / 2; k += 32) { // positions [a, jj] reversed
+                const int x = a + k, y = jj - k;
+                const uint8_t tx = tk[x], ty = tk[y];
+                tk[x] = ty;
+                tk[y] = tx;
+                pk[ty] = (uint8_t)x;
+                pk[tx] = (uint8_t)y;
+            }
+            __syncwarp();
+        }
+    }
+    return ACO_OK;
+}
 
 __host__ __device__ inline size_t route_warp_bytes(int n_max)
 {
@@ -555,10 +696,32 @@ __global__ void __launch_bounds__(512, 2) route_opt_kernel(const LocalSearchArgs
         if (idx >= total) break;
         const int2 d = desc[idx];
         if (d.x < 0) continue; // an empty entry
-        const int g = d.x, rb = d.y & 0xFFFFF, R = d.y >> 20;
+        const int g = d.x, rb = d.y & 0xFFFF, R = d.y >> 16;
         const int b = __ldg(ant_inst + g), ant = g - __ldg(ant_base + b);
         const LocalSearchArgs a = args[b];
         int *gt = a.solutions + (size_t)ant * a.T;
+        if (R > kRL) { // 33..255 nodes: the route-local generic path in the warp's tile area
+            uint16_t *nodes = reinterpret_cast<uint16_t *>(wbase);
+            uint8_t *tk = wbase + 512, *pk = tk + 256, *dlb = pk + 256;
+            float *dq = reinterpret_cast<float *>(wbase + 1280);
+            for (int k = lane; k < R; k += 32) {
+                const int node = gt[rb + k];
+                nodes[k] = (uint16_t)node;
+                tk[k] = (uint8_t)k;
+                pk[k] = (uint8_t)k;
+                dlb[k] = (uint8_t)(k == 0 && rb != 0 ? 1 : 0); // the depot's bit: clear entering route 0 only
+                if (k >= 1) loc[node] = (uint8_t)k;
+            }
+            __syncwarp();
+            for (int k = lane; k < R; k += 32) dq[k] = __ldg(a.dist + (size_t)nodes[k] * a.ld + nodes[k + 1 < R ? k + 1 : 0]);
+            __syncwarp();
+            const int st = two_opt_route_local(lane, R, a.dist, a.ld, a.nn_list, a.nn_ls, loc, nodes, tk, pk, dlb, dq,
+                                               a.pass_limit);
+            if (st != ACO_OK && lane == 0) set_status(a.status, st);
+            for (int k = lane; k < R; k += 32) gt[rb + k] = nodes[tk[k]];
+            for (int k = 1 + lane; k < R; k += 32) loc[nodes[k]] = 0;
+            __syncwarp();
+        } else {
         const int v = lane < R ? gt[rb + lane] : 0;
         if (lane >= 1 && lane < R) loc[v] = (uint8_t)lane; // customers only (kernel.cl:293-300)
         __syncwarp();
@@ -606,6 +769,7 @@ __global__ void __launch_bounds__(512, 2) route_opt_kernel(const LocalSearchArgs
         if (lane < R) gt[rb + lane] = node;
         if (lane >= 1 && lane < R) loc[v] = 0;
         __syncwarp();
+        }
         __threadfence();
         int last = 0;
         if (lane == 0) last = atomicSub(rem + g, 1) == 1;

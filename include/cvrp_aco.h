@@ -104,7 +104,7 @@ typedef struct aco_params {
                              (at most 8 ants per CTA), -1 = the ant's warp draws, 0 = automatic (helper warps
                              while there are at most 4 ants per SM); same results either way */
     int route_ls;         /* throughput mode with 2-opt, symmetric distances: 1 = the construct lists every route
-                             of at most 32 nodes and one persistent kernel improves them all, spread over the SMs;
+                             (of at most 255 nodes) and one persistent kernel improves them all, spread over the SMs;
                              -1 = one CTA per group of ants; 0 = automatic (the list above 4 ants per SM); same
                              results either way */
     int wait_limit;       /* polls of an mbarrier before a device wait gives up with ACO_ERR_TIMEOUT (0 = the
