@@ -575,6 +575,8 @@ def main():
     ap.add_argument("--learned-count", type=int, default=LEARNED_COUNT)
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT,
                     help="instances per GPU of the headline batch (smaller counts for profiling captures)")
+    ap.add_argument("--only", choices=["single", "large", "parity", "learned"],
+                    help="run this extra section alone and print it as the line (profiling captures)")
     args = ap.parse_args()
     BATCH_COUNT = args.batch_count
     if args.impl == "ours":
@@ -582,6 +584,13 @@ def main():
     ws, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, ws, rank)
+        return
+    if args.only:
+        import torch
+        torch.cuda.set_device(local)
+        fn = {"single": run_single, "large": run_large, "parity": run_parity}.get(args.only)
+        line = fn(args, local) if fn else run_learned(args)
+        print(json.dumps(line, default=float))
         return
     run_ours(args, ws, rank, local)
 

@@ -70,7 +70,7 @@ class AcoParams(ctypes.Structure):
         ("ns_rounds", ctypes.c_int),
         ("ls_ants", ctypes.c_int),
         ("draw_warps", ctypes.c_int),
-        ("route_ls", ctypes.c_int), ("wait_limit", ctypes.c_int),
+        ("route_ls", ctypes.c_int), ("wait_limit", ctypes.c_int), ("ls_best", ctypes.c_int),
     ]
 
 

@@ -390,7 +390,7 @@ class Batch:
             setattr(params, k, v)
         if tune_table is not None:  # one launch shape for the batch: the entry of the median size
             sizes = sorted(p.num_node for p in self.problems)
-            tune_table.apply(params, sizes[len(sizes) // 2])
+            tune_table.apply(params, sizes[len(sizes) // 2], batch=True)
         self.params = params
         cis, self._keep = [], []
         for p in self.problems:

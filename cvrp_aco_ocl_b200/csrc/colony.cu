@@ -714,6 +714,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         c.adv = ih.adv_d; c.nn16 = ih.nn16_d; c.cand32 = ih.cand32_d; c.chc = ih.chc_d; c.K = ih.K; c.Kp = ih.Kp;
         c.smat = ih.smat ? 1 : 0; c.packed = ih.packed ? 1 : 0; c.gtab = ih.gtab ? 1 : 0;
         c.nn_list = ih.nnls_d; c.nn_ls = ih.nn_ls; c.pass_limit = p.ls_pass_limit; c.ant_base = ant_base[b];
+        c.ls_best = p.ls_best;
         c.ls_needed = ls_needed_d_;
         c.route_desc = use_routes_ ? route_desc_d_ : nullptr;
         c.route_ctr = route_ctr_d_;
@@ -727,6 +728,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         l = LocalSearchArgs{};
         l.n = n; l.ld = ih.ld; l.n_ants = ih.A; l.T = ih.T; l.nn_ls = ih.nn_ls; l.rmax = 32;
         l.pass_limit = p.ls_pass_limit; l.dist = ih.dist_d; l.nn_list = ih.nnls_d; l.solutions = ih.sol_d;
+        l.best = p.ls_best;
         l.lens = ih.lens_d; l.status = status_d;
         StatsArgs &s = sargs[b];
         s = StatsArgs{};

@@ -379,7 +379,8 @@ __device__ void fused_ls_warp(const ConstructArgs &a, unsigned char *smem, const
             __syncwarp();
             int tq = lane < R ? lane : 0, pk = lane < R ? lane : 0;
             float dq = lane < R ? tile[lane * kRL + (lane + 1 < R ? lane + 1 : 0)] : 0.f; // dist_tour_wrk
-            const int st = two_opt_route_regs(lane, R, r == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
+            const int st = a.ls_best ? two_opt_route_best(lane, R, tile, lnn, tq, pk, dq, a.pass_limit)
+                                     : two_opt_route_regs(lane, R, r == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
             if (st != ACO_OK) status = st;
             const int node = __shfl_sync(kFullMask, v, tq);
             if (lane < R) {

@@ -46,6 +46,7 @@ struct ConstructArgs {
     // pass limit, and per global ant whether the 2-opt kernel still has to run
     const int *nn_list;    // n x nn_ls
     int nn_ls, pass_limit, ant_base;
+    int ls_best;           // the fused 2-opt improves best-first (aco_params.ls_best)
     uint8_t *ls_needed;    // total ants of the colony
     // route list for the route-level 2-opt (null: not used): every route of at
     // most 255 nodes as {global ant, first position | nodes << 16}; route_ctr[0]
@@ -68,6 +69,7 @@ struct ConstructArgs {
 
 struct LocalSearchArgs {
     int n, ld, n_ants, T, nn_ls, rmax, pass_limit;
+    int best;              // 1: best-improvement 2-opt for routes of at most 32 nodes (aco_params.ls_best)
     const float *dist;     // n x ld
     const int *nn_list;    // n x nn_ls
     int *solutions;

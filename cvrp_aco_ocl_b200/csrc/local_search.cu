@@ -448,7 +448,8 @@ __global__ void __launch_bounds__(1024) local_search_kernel(const LocalSearchArg
             int pk = lane < R ? lane : 0;
             // edge lengths: position q -> q+1, the last one back to the next depot (node 0 = local 0)
             float dq = lane < R ? tile[lane * kRL + (lane + 1 < R ? lane + 1 : 0)] : 0.f;
-            st = two_opt_route_regs(lane, R, r == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
+            st = a.best ? two_opt_route_best(lane, R, tile, lnn, tq, pk, dq, a.pass_limit)
+                        : two_opt_route_regs(lane, R, r == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
             const int node = __shfl_sync(FULL, v, tq);
             if (lane < R) {
                 tour[rb + lane] = (uint16_t)node;
@@ -763,7 +764,8 @@ __global__ void __launch_bounds__(512, 2) route_opt_kernel(const LocalSearchArgs
         // edge lengths: position q -> q+1, the last one back to the next depot (node 0 = local 0)
         int tq = lane < R ? lane : 0, pk = lane < R ? lane : 0;
         float dq = lane < R ? tile[lane * kRL + (lane + 1 < R ? lane + 1 : 0)] : 0.f;
-        const int st = two_opt_route_regs(lane, R, rb == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
+        const int st = a.best ? two_opt_route_best(lane, R, tile, lnn, tq, pk, dq, a.pass_limit)
+                              : two_opt_route_regs(lane, R, rb == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
         if (st != ACO_OK && lane == 0) set_status(a.status, st);
         const int node = __shfl_sync(FULL, v, tq);
         if (lane < R) gt[rb + lane] = node;

@@ -101,6 +101,7 @@ int check_params(const aco_params &p, int n)
     if (p.draw_warps < -1 || p.draw_warps > 1) return ACO_ERR_INVALID;
     if (p.route_ls < -1 || p.route_ls > 1) return ACO_ERR_INVALID;
     if (p.wait_limit < 0) return ACO_ERR_INVALID;
+    if (p.ls_best < 0 || p.ls_best > 1) return ACO_ERR_INVALID;
     if (!(p.rho > 0.0f && p.rho <= 1.0f)) return ACO_ERR_INVALID;
     if (p.n_ants > 56 * 1024) return ACO_ERR_INVALID; // the statistics kernel holds n_ants lengths in shared memory
     return ACO_OK;
@@ -854,39 +855,82 @@ int autotune(const InstanceSpec *specs, int count, const aco_params &p0, int ite
 {
     if (iters < 1 || !out) return ACO_ERR_INVALID;
     const bool thr = p0.mode == ACO_MODE_THROUGHPUT;
+    // The baseline is the configuration as given (its 0 fields chosen by the
+    // create-time model); a candidate replaces it only when it is faster by more
+    // than kMargin, so that timing noise does not pick a worse shape.
+    constexpr float kMargin = 0.98f;
+    // the per-ant 2-opt CTA shape: its time varies with the instance more than the margin
+    constexpr float kMarginLs = 0.95f;
     aco_params best = p0;
     float best_ph[4] = {0, 0, 0, 0};
     float best_c = INFINITY;
     bool any = false;
-    // construct: ants per CTA x (warps per ant | matrix staging)
-    std::vector<std::pair<int, int>> cands;
+    if (time_config(specs, count, p0, iters, best_ph) == ACO_OK) {
+        best_c = best_ph[0] * kMargin;
+        any = true;
+    }
+    // construct: ants per CTA x (warps per ant | matrix staging x helper draw warps)
+    struct Cand {
+        int apc, second, draw;
+    };
+    std::vector<Cand> cands;
     if (thr) {
         for (int apc : {1, 2, 4, 8, 16})
-            for (int stage : {0, -1}) cands.push_back({apc, stage});
+            for (int stage : {0, -1})
+                for (int draw : {-1, 1}) {
+                    if (p0.draw_warps != 0 && draw != p0.draw_warps) continue;
+                    if (draw == 1 && apc > 8) continue; // a helper warp per ant: at most 8 ants per CTA
+                    cands.push_back({apc, stage, draw});
+                }
     } else {
         for (int wpa : {1, 2, 4, 8})
             for (int apc : {1, 2, 4, 8})
-                if (wpa * apc <= 16 && 32 * wpa <= p0.nloc) cands.push_back({apc, wpa});
+                if (wpa * apc <= 16 && 32 * wpa <= p0.nloc) cands.push_back({apc, wpa, 0});
     }
     for (const auto &cd : cands) {
         aco_params q = p0;
-        q.ants_per_block = cd.first;
-        if (thr) q.stage_matrix = cd.second;
-        else q.warps_per_ant = cd.second;
+        q.ants_per_block = cd.apc;
+        if (thr) {
+            q.stage_matrix = cd.second;
+            q.draw_warps = cd.draw;
+        } else {
+            q.warps_per_ant = cd.second;
+        }
         if (q.ls_warps == 0 && best.ls_warps != 0) q.ls_warps = best.ls_warps;
         float ph[4];
         if (time_config(specs, count, q, iters, ph) != ACO_OK) continue; // e.g. shared memory does not fit
         if (ph[0] < best_c) {
-            best_c = ph[0];
+            best_c = ph[0] * kMargin;
             best = q;
             std::memcpy(best_ph, ph, sizeof(ph));
             any = true;
         }
     }
     if (!any) return ACO_ERR_INVALID;
-    // 2-opt CTA shape (ants x warps) with the chosen construct
-    if (p0.ls_flag && (p0.ls_warps == 0 || p0.ls_ants == 0)) {
-        float best_l = best_ph[1];
+    best_c = best_ph[0];
+    // throughput mode: the route list (every route improved by one persistent kernel over
+    // the SMs) against the per-ant kernel alone, with the chosen construct
+    if (thr && (p0.ls_flag & 1) && p0.route_ls == 0) {
+        int best_r = best.route_ls;
+        float best_t = (best_ph[0] + best_ph[1]) * kMargin;
+        for (int r : {-1, 1}) {
+            aco_params q = best;
+            q.route_ls = r;
+            float ph[4];
+            if (time_config(specs, count, q, iters, ph) != ACO_OK) continue;
+            if (ph[0] + ph[1] < best_t) {
+                best_t = (ph[0] + ph[1]) * kMargin;
+                best_r = r;
+                std::memcpy(best_ph, ph, sizeof(ph));
+            }
+        }
+        best.route_ls = best_r;
+        best_c = best_ph[0];
+    }
+    // 2-opt CTA shape (ants x warps) with the chosen construct; with the route
+    // list the per-ant kernel only takes the ants the list does not hold
+    if (p0.ls_flag && (p0.ls_warps == 0 || p0.ls_ants == 0) && best.route_ls != 1) {
+        float best_l = best_ph[1] * kMarginLs;
         int best_a = p0.ls_ants, best_w = p0.ls_warps;
         for (int an : {1, 2, 4}) {
             if (p0.ls_ants != 0 && an != p0.ls_ants) continue;
@@ -899,7 +943,7 @@ int autotune(const InstanceSpec *specs, int count, const aco_params &p0, int ite
                 float ph[4];
                 if (time_config(specs, count, q, iters, ph) != ACO_OK) continue;
                 if (ph[1] < best_l) {
-                    best_l = ph[1];
+                    best_l = ph[1] * kMarginLs;
                     best_a = an;
                     best_w = w;
                     std::memcpy(best_ph, ph, sizeof(ph));

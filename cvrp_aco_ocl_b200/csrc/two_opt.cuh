@@ -167,5 +167,61 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
     return ACO_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Best improvement (a non-parity option: the reference improves first in scan
+// order): every 2-opt move of the route -- reverse positions i+1..j, 0 <= i <
+// j <= R-1, the position after R-1 being the depot at 0 -- is evaluated at once
+// from the route's distance tile, lane j taking the pairs (i, j) of one i at a
+// time; a warp argmin picks the most negative change of the tour length (ties:
+// the lowest (i, j)), which is applied while it is below -EPSILON.  tpos: 32
+// bytes of the warp's shared memory for the local node at every position.  At
+// most move_limit moves (then ACO_ERR_LS_LIMIT).
+// ---------------------------------------------------------------------------
+__device__ int two_opt_route_best(int lane, int R, const float *tile, uint8_t *tpos, int &tq, int &pk, float &dq,
+                                  int move_limit)
+{
+    const unsigned FULLM = 0xffffffffu;
+    for (int moves = 0;; moves++) {
+        if (lane < R) tpos[lane] = (uint8_t)tq;
+        __syncwarp();
+        unsigned long long best = ~0ull;
+        const int j = lane, tj = lane < R ? tpos[lane] : 0, tj1 = lane + 1 < R ? tpos[lane + 1] : tpos[0];
+        for (int i = 0; i + 1 < R; i++) {
+            if (j > i && j < R) {
+                const int ti = tpos[i], ti1 = tpos[i + 1];
+                const float add = __fadd_rn(tile[ti * kRL + tj], tile[ti1 * kRL + tj1]);
+                const float rem = __fadd_rn(tile[ti * kRL + ti1], tile[tj * kRL + tj1]);
+                const uint32_t b = __float_as_uint(__fsub_rn(add, rem));
+                const uint32_t ord = (b & 0x80000000u) ? ~b : (b | 0x80000000u); // ascending as the floats
+                const unsigned long long key = ((unsigned long long)ord << 32) | (unsigned)(i << 8 | j);
+                best = key < best ? key : best;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(FULLM, best, o);
+            best = w < best ? w : best;
+        }
+        __syncwarp();
+        if (best == ~0ull) break;
+        const uint32_t ord = (uint32_t)(best >> 32);
+        const uint32_t b = (ord & 0x80000000u) ? (ord & 0x7fffffffu) : ~ord;
+        if (!(__uint_as_float(b) < -kEps)) break;
+        if (move_limit > 0 && moves >= move_limit) return ACO_ERR_LS_LIMIT;
+        const int i = (int)((best >> 8) & 0xffu), jj = (int)(best & 0xffu);
+        // the exchange of the first-improvement path with h1..h4 = the nodes at i, i+1, jj, jj+1
+        const int h1 = tpos[i], h2 = tpos[i + 1], h3 = tpos[jj], h4 = jj + 1 < R ? tpos[jj + 1] : tpos[0];
+        const int a = i + 1;
+        const float d13 = tile[h1 * kRL + h3], d24 = tile[h2 * kRL + h4];
+        const float dsrc = __shfl_sync(FULLM, dq, (lane > i && lane < jj) ? i + jj - lane : lane);
+        if (lane == jj) dq = d24;
+        else if (lane == i) dq = d13;
+        else if (lane > i && lane < jj) dq = dsrc;
+        const int tsrc = __shfl_sync(FULLM, tq, (lane >= a && lane <= jj) ? a + jj - lane : lane);
+        if (lane >= a && lane <= jj) tq = tsrc;
+        if (pk >= a && pk <= jj) pk = a + jj - pk;
+    }
+    return ACO_OK;
+}
+
 } // namespace
 } // namespace aco

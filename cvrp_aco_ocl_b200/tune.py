@@ -26,7 +26,7 @@ from typing import Dict, List, Optional, Sequence, Tuple
 from . import _lib
 from ._lib import AcoInstance, AcoParams, check, lib
 
-SHAPE_FIELDS = ("ants_per_block", "warps_per_ant", "ls_warps", "stage_matrix", "ls_ants")
+SHAPE_FIELDS = ("ants_per_block", "warps_per_ant", "ls_warps", "stage_matrix", "ls_ants", "draw_warps", "route_ls")
 
 
 @dataclasses.dataclass
@@ -42,6 +42,9 @@ class TuneEntry:
     ms_per_iter: float
     nn_ants: int = 0  # list length the entry was timed with (0 = not recorded)
     ls_ants: int = 0  # ants per 2-opt CTA (0 = the library's default)
+    draw_warps: int = 0  # helper draw warps (0 = the library's default)
+    route_ls: int = 0    # route-level 2-opt (0 = the library's default)
+    batch: int = 0       # 1: tuned on a batch of instances in [n_lo, n_hi] (for Batch), 0: on one instance
 
 
 class TuneTable:
@@ -70,18 +73,20 @@ class TuneTable:
         self.entries.append(e)
         self.entries.sort(key=lambda x: (x.mode, x.n_lo, x.ants))
 
-    def lookup(self, n: int, mode: int, ants: int) -> Optional[TuneEntry]:
-        """The entry of this mode whose node range holds n, with the nearest ant
-        count (ratio distance); None when no range holds n."""
-        hits = [e for e in self.entries if e.mode == mode and e.n_lo <= n <= e.n_hi]
+    def lookup(self, n: int, mode: int, ants: int, batch: bool = False) -> Optional[TuneEntry]:
+        """The entry of this mode and kind (batch or single instance) whose node
+        range holds n, with the nearest ant count (ratio distance); None when no
+        range holds n."""
+        hits = [e for e in self.entries
+                if e.mode == mode and bool(e.batch) == batch and e.n_lo <= n <= e.n_hi]
         if not hits:
             return None
         return min(hits, key=lambda e: abs((e.ants / max(ants, 1)) - 1.0))
 
-    def apply(self, params: AcoParams, n: int) -> AcoParams:
+    def apply(self, params: AcoParams, n: int, batch: bool = False) -> AcoParams:
         """Fill the launch-shape fields the caller left at 0 (autotuned) from the
-        entry for n; fields set by the caller are kept."""
-        e = self.lookup(n, params.mode, params.n_ants if params.n_ants > 0 else n)
+        entry for n (a batch: its median size); fields set by the caller are kept."""
+        e = self.lookup(n, params.mode, params.n_ants if params.n_ants > 0 else n, batch)
         if e is None:
             return params
         for f in SHAPE_FIELDS:
@@ -129,27 +134,63 @@ def size_ranges(sizes: Sequence[int]) -> List[Tuple[int, int]]:
 
 def build_table(sizes: Sequence[int], ants: int, mode: int = _lib.MODE_THROUGHPUT, iters: int = 3,
                 seed: int = 1, nn_ants: int = 25, table: Optional[TuneTable] = None, log=None) -> TuneTable:
-    """Tune one synthetic instance (the mixed generator) per size and record
-    the winners over the size ranges of `size_ranges`."""
+    """Tune two synthetic instances per size (the mixed and the large
+    generator) and record, over the size ranges of `size_ranges`, the fields
+    both choose alike; a field they choose differently stays 0 (the library's
+    create-time model), since the shape depends on the instance there."""
     from .aco import Problem, default_params
-    from .instances import gen_mixed
+    from .instances import gen_large, gen_mixed
 
     table = table or TuneTable()
     for (lo, hi), n in zip(size_ranges(sizes), sorted(set(int(v) for v in sizes))):
-        prob = Problem.from_instance(gen_mixed(seed + n, n - 1))
-        p = default_params(n)
-        p.mode, p.n_ants = mode, ants
-        p.nn_ants = min(nn_ants, n - 2)
-        p.nn_ls = min(p.nn_ls, 25)
-        p.seed_time, p.rnd_seed = 1796300000, seed
         t0 = time.perf_counter()
-        out, ms = autotune(prob, p, iters)
-        e = TuneEntry(mode, lo, hi, ants, out.ants_per_block, out.warps_per_ant, out.ls_warps, out.stage_matrix,
-                      ms, p.nn_ants, out.ls_ants)
+        outs, mss = [], []
+        for gen in (gen_mixed, gen_large):
+            prob = Problem.from_instance(gen(seed + n, n - 1))
+            p = default_params(n)
+            p.mode, p.n_ants = mode, ants
+            p.nn_ants = min(nn_ants, n - 2)
+            p.nn_ls = min(p.nn_ls, 25)
+            p.seed_time, p.rnd_seed = 1796300000, seed
+            out, ms = autotune(prob, p, iters)
+            outs.append(out)
+            mss.append(ms)
+        agree = {f: (getattr(outs[0], f) if getattr(outs[0], f) == getattr(outs[1], f) else 0) for f in SHAPE_FIELDS}
+        ms = sum(mss) / len(mss)
+        e = TuneEntry(mode, lo, hi, ants, agree["ants_per_block"], agree["warps_per_ant"], agree["ls_warps"],
+                      agree["stage_matrix"], ms, min(nn_ants, n - 2), agree["ls_ants"], agree["draw_warps"],
+                      agree["route_ls"])
         table.add(e)
         if log:
             log(f"n={n} [{lo},{hi}] ants={ants}: apc={e.ants_per_block} wpa={e.warps_per_ant} "
                 f"ls_warps={e.ls_warps} ls_ants={e.ls_ants} stage={e.stage_matrix} {ms:.3f} ms/iter ({time.perf_counter() - t0:.1f} s)")
+    return table
+
+
+def build_batch_entry(seed: int, count: int, n_min: int, n_max: int, ants: int, nn_ants: int = 25, iters: int = 3,
+                      table: Optional[TuneTable] = None, log=None) -> TuneTable:
+    """Tune the launch shape of a batch (gen_batch(seed, count, n_min, n_max),
+    the batched workload's generator) and record it as the batch entry for
+    customer counts in [n_min, n_max]."""
+    from .aco import Problem, default_params
+    from .instances import gen_batch
+
+    table = table or TuneTable()
+    probs = [Problem.from_instance(x) for x in gen_batch(seed, count, n_min, n_max)]
+    p = default_params(n_max + 1)
+    p.mode, p.n_ants, p.nn_ants, p.nn_ls = _lib.MODE_THROUGHPUT, ants, nn_ants, min(25, n_min - 1)
+    p.seed_time, p.rnd_seed = 1796300000, seed
+    t0 = time.perf_counter()
+    out, ms = autotune_batch(probs, p, iters)
+    e = TuneEntry(_lib.MODE_THROUGHPUT, n_min + 1, n_max + 1, ants, out.ants_per_block, out.warps_per_ant,
+                  out.ls_warps, out.stage_matrix, ms, nn_ants, out.ls_ants, out.draw_warps, out.route_ls, batch=1)
+    table.entries = [x for x in table.entries if not (x.batch and x.n_lo == e.n_lo and x.n_hi == e.n_hi
+                                                      and x.ants == e.ants)]
+    table.entries.append(e)
+    table.entries.sort(key=lambda x: (x.mode, x.batch, x.n_lo, x.ants))
+    if log:
+        log(f"batch of {count} [{e.n_lo},{e.n_hi}] ants={ants}: apc={e.ants_per_block} stage={e.stage_matrix} "
+            f"draw={e.draw_warps} route_ls={e.route_ls} {ms:.3f} ms/iter ({time.perf_counter() - t0:.1f} s)")
     return table
 
 
@@ -177,23 +218,75 @@ def tune_candidate_length(problem, params: AcoParams, ks: Sequence[int] = (16, 2
     return best, costs
 
 
+DEFAULT_TABLE = __import__("os").path.join(__import__("os").path.dirname(__file__), "tune_b200.json")
+
+
+def compare(table: TuneTable, iters: int = 20) -> Dict[str, Dict[str, float]]:
+    """Device ms per iteration of three workloads with the table's shapes and
+    with the library's create-time model (every shape field 0): one instance of
+    200 customers with 200 ants (25-NN lists), one of 1000 customers with 256
+    ants (30-NN), and the batch of 512 instances of 100-1000 customers with 128
+    ants each (25-NN).  Same seeds and iterations for both; results are
+    bit-identical, only time differs."""
+    from . import instances as I
+    from .aco import Batch, Problem, Solver, default_params
+
+    def single(inst, ants, k, tuned):
+        p = default_params(inst.n)
+        p.mode, p.n_ants, p.nn_ants, p.nn_ls = _lib.MODE_THROUGHPUT, ants, k, k
+        p.seed_time, p.rnd_seed = 1796300000, 4242
+        with Solver(Problem.from_instance(inst), p, tune_table=table if tuned else None) as S:
+            S.init()
+            S.iterate(3)
+            return S.time_iterations(iters) / iters
+
+    def batch(tuned):
+        p = default_params(1001)
+        p.mode, p.n_ants, p.nn_ants, p.nn_ls = _lib.MODE_THROUGHPUT, 128, 25, 25
+        p.seed_time, p.rnd_seed = 1796300000, 4242
+        probs = [Problem.from_instance(x) for x in I.gen_batch(512, 512, 100, 1000)]
+        with Batch(probs, p, tune_table=table if tuned else None) as B:
+            B.init()
+            B.iterate(3)
+            return float(B.time_phases(5).sum()) / 5
+
+    c2, c3 = I.gen_mixed(2026, 200), I.gen_large(3031, 1000)
+    out = {}
+    for name, fn in (("single_200x200", lambda t: single(c2, 200, 25, t)),
+                     ("large_1000x256", lambda t: single(c3, 256, 30, t)),
+                     ("batch_512x128", batch)):
+        model, tuned = fn(False), fn(True)
+        out[name] = {"model_ms": model, "table_ms": tuned, "table_over_model": tuned / model}
+    return out
+
+
 def main():
-    ap = argparse.ArgumentParser(description="Build a launch-shape table for this GPU.")
+    ap = argparse.ArgumentParser(description="Build a launch-shape table for this GPU, or compare one with the "
+                                             "library's create-time model.")
     ap.add_argument("--sizes", default="101,201,501,1001")
     ap.add_argument("--ants", type=int, default=128)
     ap.add_argument("--mode", choices=["throughput", "parity"], default="throughput")
-    ap.add_argument("--iters", type=int, default=3)
-    ap.add_argument("--out", required=True)
+    ap.add_argument("--iters", type=int, default=6)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="tune a batch of this many instances of 100-1000 customers instead of single sizes")
+    ap.add_argument("--compare", action="store_true", help="time the table against the model and print JSON")
+    ap.add_argument("--out", default=DEFAULT_TABLE)
     a = ap.parse_args()
     mode = _lib.MODE_THROUGHPUT if a.mode == "throughput" else _lib.MODE_PARITY
     import os
     table = TuneTable.load(a.out) if os.path.exists(a.out) else TuneTable()
+    if a.compare:
+        print(json.dumps(compare(table), indent=1))
+        return
     try:
         import torch
         table.device = torch.cuda.get_device_name(0)
     except Exception:
         pass
-    build_table([int(v) for v in a.sizes.split(",")], a.ants, mode, a.iters, table=table, log=print)
+    if a.batch > 0:
+        build_batch_entry(512, a.batch, 100, 1000, a.ants, iters=a.iters, table=table, log=print)
+    else:
+        build_table([int(v) for v in a.sizes.split(",")], a.ants, mode, a.iters, table=table, log=print)
     table.save(a.out)
 
 

@@ -110,6 +110,11 @@ typedef struct aco_params {
     int wait_limit;       /* polls of an mbarrier before a device wait gives up with ACO_ERR_TIMEOUT (0 = the
                              default, 2^24 polls, about a second); no reference counterpart (kernel.cl has no
                              bounded waits) */
+    int ls_best;          /* 2-opt move choice: 0 = first improvement in scan order with don't-look bits, the
+                             reference's (kernel.cl:126-277; default); 1 = best improvement, a non-parity option:
+                             every move of a route of at most 32 nodes evaluated from its distance tile and the
+                             best applied (a warp argmin) until none improves; longer routes keep first
+                             improvement.  For symmetric distances. */
 } aco_params;
 
 /* One best-so-far record {iteration, length, seconds since init} (problem.h:62-66). */
@@ -272,14 +277,17 @@ int aco_load_checkpoint(aco_solver *s, const char *path);
 
 /* ---- autotuner (no reference counterpart) -----------------------------------
  * Times launch configurations on the instance(s) and returns the fastest in
- * *out (a copy of *p with ants_per_block, ls_warps, stage_matrix -- and
- * warps_per_ant in ACO_MODE_PARITY -- set explicitly).  Every configuration
- * computes the same tours, lengths and pheromone bit for bit; only speed
- * differs.  Each candidate runs on a fresh solver from the same seeds:
- * aco_init, 2 warm-up iterations, then `iters` timed iterations (per-kernel
- * CUDA events).  The construct candidates (ants per CTA x staging) are timed
- * first with the default 2-opt shape, then the 2-opt CTA widths with the best
- * construct.  ms_out (optional) = the chosen configuration's time per
+ * *out (a copy of *p with ants_per_block, stage_matrix, draw_warps, route_ls,
+ * ls_ants, ls_warps -- and warps_per_ant in ACO_MODE_PARITY -- set where they
+ * were 0).  Every configuration computes the same tours, lengths and
+ * pheromone bit for bit; only speed differs.  Each candidate runs on a fresh
+ * solver from the same seeds: aco_init, 2 warm-up iterations, then `iters`
+ * timed iterations (per-kernel CUDA events).  The configuration as given (its
+ * 0 fields chosen by the library's create-time model) is the baseline; the
+ * construct candidates (ants per CTA x staging x helper draw warps) are timed
+ * first, then the route list against the per-ant 2-opt kernel, then (without
+ * the list) the 2-opt CTA widths, and a candidate replaces the current choice
+ * only when it is more than 2% faster (5% for the 2-opt CTA shape).  ms_out (optional) = the chosen configuration's time per
  * iteration.  The candidate-list length (nn_ants) changes the search itself,
  * not only its speed, so it is not chosen here. */
 int aco_autotune(const aco_instance *inst, const aco_params *p, int iters, aco_params *out, float *ms_out);

@@ -38,9 +38,11 @@ def test_throughput_shapes_identical(gpu, n_cust):
     prob = Problem.from_instance(I.gen_mixed(90 + n_cust, n_cust))
     n = prob.num_node
     ref = run(prob, params(n, 96, MODE_THROUGHPUT))
-    for apc, stage, lsw in [(1, 0, 4), (4, -1, 32), (16, 0, 8), (2, -1, 1)]:
-        got = run(prob, params(n, 96, MODE_THROUGHPUT, ants_per_block=apc, stage_matrix=stage, ls_warps=lsw))
-        assert same(ref, got), (apc, stage, lsw)
+    for apc, stage, lsw, draw, route in [(1, 0, 4, 1, -1), (4, -1, 32, -1, 1), (16, 0, 8, -1, -1),
+                                          (2, -1, 1, 1, 1), (8, 0, 16, 1, -1)]:
+        got = run(prob, params(n, 96, MODE_THROUGHPUT, ants_per_block=apc, stage_matrix=stage, ls_warps=lsw,
+                               draw_warps=draw, route_ls=route))
+        assert same(ref, got), (apc, stage, lsw, draw, route)
 
 
 def test_parity_shapes_identical(gpu):
@@ -67,7 +69,8 @@ def test_autotune_single_and_result_unchanged(gpu):
     p = params(n, 200, MODE_THROUGHPUT)
     tuned, ms = autotune(prob, p, iters=2)
     assert ms > 0
-    assert 1 <= tuned.ants_per_block <= 16 and tuned.stage_matrix in (0, -1) and 0 <= tuned.ls_warps <= 32
+    # 0 = the create-time model's choice, kept unless a candidate is reliably faster
+    assert 0 <= tuned.ants_per_block <= 16 and tuned.stage_matrix in (0, -1) and 0 <= tuned.ls_warps <= 32
     assert same(run(prob, p), run(prob, tuned))
 
 
@@ -82,7 +85,7 @@ def test_autotune_batch_and_table(gpu, tmp_path):
     probs = [Problem.from_instance(I.gen_mixed(30 + k, m)) for k, m in enumerate([80, 150, 300, 120])]
     p = params(301, 32, MODE_THROUGHPUT)
     tuned, ms = autotune_batch(probs, p, iters=1)
-    assert ms > 0 and tuned.ants_per_block >= 1
+    assert ms > 0 and tuned.ants_per_block >= 0  # 0: the create-time model kept
     t = build_table([61, 201], ants=32, iters=1)
     path = tmp_path / "tune.json"
     t.save(str(path))

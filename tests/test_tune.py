@@ -91,3 +91,20 @@ def test_committed_table_loads():
     from cvrp_aco_ocl_b200 import tune
     t = TuneTable.load(os.path.join(os.path.dirname(tune.__file__), "tune_b200.json"))
     assert t.entries and all(e.ls_ants == 0 for e in t.entries)
+
+
+def test_batch_entries_serve_batches_only_and_fill_the_new_fields():
+    single = entry(lo=3, hi=2000, apc=1)
+    b = TuneEntry(MODE_THROUGHPUT, 101, 1001, 128, 16, 0, 0, 0, 20.0, 25, 0, -1, 1, batch=1)
+    t = TuneTable([single, b])
+    assert t.lookup(550, MODE_THROUGHPUT, 128).ants_per_block == 1
+    assert t.lookup(550, MODE_THROUGHPUT, 128, batch=True).ants_per_block == 16
+    assert t.lookup(50, MODE_THROUGHPUT, 128, batch=True) is None
+    p = default_params(1001)
+    p.mode, p.n_ants = MODE_THROUGHPUT, 128
+    t.apply(p, 550, batch=True)
+    assert (p.ants_per_block, p.draw_warps, p.route_ls) == (16, -1, 1)
+    q = default_params(1001)
+    q.mode, q.n_ants, q.route_ls = MODE_THROUGHPUT, 128, -1  # set by the caller: kept
+    t.apply(q, 550, batch=True)
+    assert q.route_ls == -1 and q.draw_warps == -1
