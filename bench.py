@@ -89,6 +89,13 @@ def batch_params(local: int):
     return p
 
 
+def tune_table():
+    """The committed launch-shape table of this GPU (cvrp_aco_ocl_b200/tune_b200.json); its 0
+    fields leave the choice to the library's create-time model."""
+    from cvrp_aco_ocl_b200.tune import DEFAULT_TABLE, TuneTable
+    return TuneTable.load(DEFAULT_TABLE) if os.path.exists(DEFAULT_TABLE) else None
+
+
 def config(ws: int):
     return {"workload": f"{BATCH_COUNT} independent CVRP instances per GPU, 100-1000 customers each (mixed and large "
                         f"generators alternately), {BATCH_ANTS} ants each, {NN_ANTS}-NN candidate lists, 2-opt on "
@@ -96,7 +103,8 @@ def config(ws: int):
             "instances": BATCH_COUNT * ws, "ants": BATCH_ANTS, "nn_ants": NN_ANTS, "nn_ls": NN_LS,
             "mode": "throughput", "ras_ranks": RANKS, "batch_seed": BATCH_SEED,
             "parallelism": f"instances sharded by cost over {ws} GPU(s)",
-            "l2": "inputs exceed L2 (about 3.4 GB of matrices per GPU): no flush"}
+            "l2": "inputs exceed L2 (about 3.4 GB of matrices per GPU): no flush",
+            "launch_shapes": "tune table (cvrp_aco_ocl_b200/tune_b200.json)"}
 
 
 def load_peaks():
@@ -246,7 +254,7 @@ def run_ours(args, ws, rank, local):
 
     insts, _ = batch_workload(ws, rank)
     probs = [Problem.from_instance(x) for x in insts]
-    B = Batch(probs, batch_params(local))
+    B = Batch(probs, batch_params(local), tune_table=tune_table())
     B.init()
     count, total_ants = B.size()
     stream = torch.cuda.ExternalStream(B.stream(), device=dev)
@@ -325,9 +333,10 @@ def run_e2e(args, ws, rank, local):
 
     insts, _ = batch_workload(ws, rank)
     probs = [Problem.from_instance(x) for x in insts]
+    table = tune_table()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    B = Batch(probs, batch_params(local))
+    B = Batch(probs, batch_params(local), tune_table=table)
     B.init()
     buf = np.zeros(B.lengths_total(), np.float32)
     prev = -1
@@ -366,7 +375,7 @@ def run_one_instance(args, local, inst, ants, k, label):
     from cvrp_aco_ocl_b200 import Problem, Solver
 
     dev = torch.device("cuda", local)
-    S = Solver(Problem.from_instance(inst), single_params(inst.n, ants, k, local, RND_SEED))
+    S = Solver(Problem.from_instance(inst), single_params(inst.n, ants, k, local, RND_SEED), tune_table=tune_table())
     S.init()
     stream = torch.cuda.ExternalStream(S.stream(), device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
