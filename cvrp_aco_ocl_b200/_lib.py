@@ -31,6 +31,7 @@ EXPORTED = [
     "aco_get_solutions", "aco_get_pheromone", "aco_get_seeds", "aco_get_elites", "aco_get_iteration",
     "aco_set_state", "aco_status", "aco_strerror", "aco_get_stream", "aco_launches_per_iteration",
     "aco_time_iterations", "aco_enqueue_iterations", "aco_enqueue_lengths", "aco_read_lengths", "aco_time_phases", "aco_get_config",
+    "aco_batch_get_config",
     "aco_pheromone_update_noalloc", "aco_batch_create", "aco_batch_init", "aco_batch_iterate",
     "aco_batch_enqueue_iterations", "aco_batch_status", "aco_batch_size", "aco_batch_get_best",
     "aco_batch_get_solutions", "aco_batch_get_pheromone", "aco_batch_time_phases", "aco_batch_get_stream",
@@ -71,6 +72,7 @@ class AcoParams(ctypes.Structure):
         ("ls_ants", ctypes.c_int),
         ("draw_warps", ctypes.c_int),
         ("route_ls", ctypes.c_int), ("wait_limit", ctypes.c_int), ("ls_best", ctypes.c_int),
+        ("construct_ctas", ctypes.c_int),
     ]
 
 
@@ -166,6 +168,7 @@ def lib() -> ctypes.CDLL:
                      "aco_batch_load_checkpoint"):
             getattr(L, name).argtypes = [vp, ctypes.c_char_p]
         L.aco_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
+        L.aco_batch_get_config.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
         L.aco_batch_enqueue_lengths.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
         L.aco_batch_read_lengths.argtypes = [vp, ctypes.c_longlong, vp, ctypes.c_size_t]
         L.aco_batch_get_best_all.argtypes = [vp, vp, ctypes.c_size_t, vp, vp]

@@ -492,6 +492,13 @@ class Batch:
         check(lib().aco_batch_time_phases(self.h, n_iter, ptr(ms)), "aco_batch_time_phases")
         return ms
 
+    def config(self) -> Tuple[int, int, int]:
+        """(ants per construct CTA, warps per ant, staging flags) of the batch's launches."""
+        a, w, f = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().aco_batch_get_config(self.h, ctypes.byref(a), ctypes.byref(w), ctypes.byref(f)),
+              "aco_batch_get_config")
+        return a.value, w.value, f.value
+
     def validate(self) -> Tuple[np.ndarray, int]:
         """Device check of every tour of every instance: invalid slots per
         instance and in total."""

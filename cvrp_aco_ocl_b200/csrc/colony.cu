@@ -29,6 +29,8 @@ namespace {
 
 // 227 KB per CTA minus room for the kernels' static shared memory
 constexpr size_t kSmemBudget = 226 * 1024;
+// two construct CTAs per SM: 228 KB an SM, 1 KB of it reserved per CTA
+constexpr size_t kWideBudget = 112 * 1024;
 constexpr int kRouteWarps = 16; // warps per CTA of the route-level 2-opt
 constexpr int kSwapLimitPerNode = 64; // accepted swaps per node and tour before ACO_ERR_LS_LIMIT
 
@@ -498,29 +500,34 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         else if (count == 1) cn_apc = std::max(1, std::min(8, (inst[0].A + sm_count - 1) / sm_count));
         else cn_apc = std::max(1, std::min(16, total_ants / (sm_count * 2)));
         // helper draw warps while the construct is latency bound (few ants per SM)
-        cn_draw = p.draw_warps > 0 || (p.draw_warps == 0 && total_ants <= 4 * sm_count);
+        cn_draw = p.draw_warps > 0 || (p.draw_warps == 0 && p.construct_ctas != 2 && total_ants <= 4 * sm_count);
         if (cn_draw) cn_apc = std::min(cn_apc, 8);
+        // two CTAs per SM (without helper draws or fused 2-opt) while there are
+        // at least 32 ants an SM: the construct is latency bound per ant, and
+        // twice the warps outweigh the tables that no longer fit in shared memory
+        cn_wide = false;
         // shared-memory plan of every instance for `apc` ants per CTA and `lsw`
-        // fused 2-opt warps (lsw > 0 needs the tables staged)
-        auto plan = [&](int apc, int lsw) {
+        // fused 2-opt warps (lsw > 0 needs the tables staged), within `budget` bytes a CTA
+        auto plan = [&](int apc, int lsw, size_t budget) {
             const bool draw = cn_draw && lsw == 0 && apc <= 8;
+            const bool wide = cn_wide && lsw == 0; // the two-CTA kernel stages no matrix, no table above 1024 nodes
             size_t mx = 0;
             for (InstHost &ih : inst) {
                 bool packable = true;
                 for (int i = 0; i < ih.n; i++)
                     if (ih.demand[i] < 0 || ih.demand[i] > 0xFFFF) packable = false;
-                ih.smat = p.stage_matrix >= 0 && ih.n <= 1024 && packable &&
-                          construct_nn_smem(ih.n, ih.K, ih.Kp, apc, true, true, false, lsw, draw) <= kSmemBudget;
+                ih.smat = !wide && p.stage_matrix >= 0 && ih.n <= 1024 && packable &&
+                          construct_nn_smem(ih.n, ih.K, ih.Kp, apc, true, true, false, lsw, draw) <= budget;
                 ih.packed =
-                    packable && construct_nn_smem(ih.n, ih.K, ih.Kp, apc, ih.smat, true, false, lsw, draw) <= kSmemBudget;
+                    packable && construct_nn_smem(ih.n, ih.K, ih.Kp, apc, ih.smat, true, false, lsw, draw) <= budget;
                 ih.gtab = false;
                 size_t need = construct_nn_smem(ih.n, ih.K, ih.Kp, apc, ih.smat, ih.packed, false, lsw, draw);
-                if (need > kSmemBudget) {
+                if (need > budget || (wide && ih.n > 1024)) {
                     ih.gtab = true; // the candidate table stays in global memory (read through L2)
                     ih.packed = packable;
                     need = construct_nn_smem(ih.n, ih.K, ih.Kp, apc, false, ih.packed, true, lsw, draw);
                 }
-                if (need > kSmemBudget) return false;
+                if (need > budget) return false;
                 mx = std::max(mx, need);
             }
             cn_smem = mx;
@@ -534,16 +541,24 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
             // routes, so completed routes do not queue
             for (int apc = std::min(cn_apc, 4); apc >= 1 && cn_lsw == 0; apc--) {
                 const int lsw = 16 - apc;
-                if (plan(apc, lsw)) {
+                if (plan(apc, lsw, kSmemBudget)) {
                     cn_apc = apc;
                     cn_lsw = lsw;
                 }
             }
         }
         if (cn_lsw == 0) {
-            while (!plan(cn_apc, 0)) {
-                if (cn_apc > 1) cn_apc--;
-                else return ACO_ERR_INVALID; // candidate table of this size cannot be staged
+            cn_wide = !cn_draw && (p.construct_ctas == 2 || (p.construct_ctas == 0 && total_ants >= 32 * sm_count));
+            const int apc0 = cn_apc;
+            while (!plan(cn_apc, 0, cn_wide ? kWideBudget : kSmemBudget)) {
+                if (cn_apc > 1) {
+                    cn_apc--;
+                } else if (cn_wide) { // not even one ant fits half an SM: one CTA per SM
+                    cn_wide = false;
+                    cn_apc = apc0;
+                } else {
+                    return ACO_ERR_INVALID; // candidate table of this size cannot be staged
+                }
             }
         }
         cn_draw = cn_draw && cn_lsw == 0 && cn_apc <= 8; // as the last plan sized the shared memory
@@ -1002,7 +1017,7 @@ int Colony::construct(bool in_iteration)
     // inside an iteration the 2-opt follows and, with the route list, writes every tour length
     const bool lens_later = in_iteration && routes_pending_ && (p.ls_flag & 1);
     CK(launch_construct_nn(cargs_d_, items_d_, n_items, queue_d_, cn_apc, cn_smem, sm_count, fin_any, st, lsw,
-                           cn_draw, lens_later));
+                           cn_draw, lens_later, cn_wide && lsw == 0));
     return ACO_OK;
 }
 

@@ -115,6 +115,7 @@ public:
     bool cp_stage = false;
     int cn_apc = 1, cn_lsw = 0; // throughput construct: ants per CTA, fused 2-opt warps (0 = separate kernel)
     bool cn_draw = false;       // throughput construct: helper warps make the race draws
+    bool cn_wide = false;       // throughput construct: two CTAs per SM (64 registers, half the shared memory each)
     StatsArgs stats_one_{};     // a single instance's statistics arguments, passed by value
     size_t cn_smem = 0;
     int ls_warps = 1, ls_apc = 1, ls_nmax = 0; // 2-opt: warps and ants per CTA, largest instance

@@ -902,6 +902,9 @@ template <bool FIN, bool DRAW>
 __device__ __forceinline__ bool construct_nn_plain(const ConstructArgs &a, int apc, int ant0, unsigned char *smem,
                                                    uint32_t phase, bool ll)
 {
+    if (a.gtab && a.n <= 1024)
+        return a.packed ? construct_nn_item<FIN, false, true, true, true, false, DRAW>(a, apc, ant0, smem, phase, 0, ll)
+                        : construct_nn_item<FIN, false, false, true, true, false, DRAW>(a, apc, ant0, smem, phase, 0, ll);
     if (a.gtab)
         return a.packed ? construct_nn_item<FIN, false, true, false, true, false, DRAW>(a, apc, ant0, smem, phase, 0, ll)
                         : construct_nn_item<FIN, false, false, false, true, false, DRAW>(a, apc, ant0, smem, phase, 0, ll);
@@ -916,7 +919,25 @@ __device__ __forceinline__ bool construct_nn_plain(const ConstructArgs &a, int a
                     : construct_nn_item<FIN, false, false, false, false, false, DRAW>(a, apc, ant0, smem, phase, 0, ll);
 }
 
-// KIND: 0 = plain, 1 = helper-warp draws, 2 = fused 2-opt (lsw improving warps)
+// The item of the two-CTA kernel: no staged distance matrix (it does not fit
+// half of the shared memory at the sizes where it pays) and no staged table
+// above 1024 nodes, which keeps every path within 64 registers.
+template <bool FIN>
+__device__ __forceinline__ bool construct_nn_wide(const ConstructArgs &a, int apc, int ant0, unsigned char *smem,
+                                                  uint32_t phase, bool ll)
+{
+    if (a.n > 1024)
+        return a.packed ? construct_nn_item<FIN, false, true, false, true>(a, apc, ant0, smem, phase, 0, ll)
+                        : construct_nn_item<FIN, false, false, false, true>(a, apc, ant0, smem, phase, 0, ll);
+    if (a.gtab)
+        return a.packed ? construct_nn_item<FIN, false, true, true, true>(a, apc, ant0, smem, phase, 0, ll)
+                        : construct_nn_item<FIN, false, false, true, true>(a, apc, ant0, smem, phase, 0, ll);
+    return a.packed ? construct_nn_item<FIN, false, true, true, false>(a, apc, ant0, smem, phase, 0, ll)
+                    : construct_nn_item<FIN, false, false, true, false>(a, apc, ant0, smem, phase, 0, ll);
+}
+
+// KIND: 0 = plain, 1 = helper-warp draws, 2 = fused 2-opt (lsw improving warps),
+// 3 = plain at two CTAs per SM
 template <bool FIN, int KIND>
 __device__ __forceinline__ void construct_nn_body(const ConstructArgs *args, const int2 *items, int n_items, int *queue,
                                                   int apc, int lsw, bool lens_later)
@@ -947,6 +968,8 @@ __device__ __forceinline__ void construct_nn_body(const ConstructArgs *args, con
                                       : construct_nn_item<FIN, true, false, true, false, true>(a, apc, ant0, smem, phase, lsw);
             else ok = a.packed ? construct_nn_item<FIN, false, true, true, false, true>(a, apc, ant0, smem, phase, lsw)
                                : construct_nn_item<FIN, false, false, true, false, true>(a, apc, ant0, smem, phase, lsw);
+        } else if (KIND == 3) {
+            ok = construct_nn_wide<FIN>(a, apc, ant0, smem, phase, lens_later && a.route_desc != nullptr);
         } else {
             ok = construct_nn_plain<FIN, KIND == 1>(a, apc, ant0, smem, phase, lens_later && a.route_desc != nullptr);
         }
@@ -971,6 +994,18 @@ __global__ void __launch_bounds__(512, 1) construct_nn_kernel(const ConstructArg
                                                            int *queue, int apc, int lsw, int lens_later)
 {
     construct_nn_body<FIN, KIND>(args, items, n_items, queue, apc, lsw, lens_later != 0);
+}
+
+// Two CTAs per SM at 64 registers a thread: 32 ant warps an SM instead of 16,
+// twice the warps to cover the latency of the candidate-table reads, which on
+// the large instances of a batch come through L2 (tables beyond half of the
+// SM's shared memory are not staged).
+template <bool FIN>
+__global__ void __launch_bounds__(512, 2) construct_nn_wide_kernel(const ConstructArgs *args, const int2 *items,
+                                                                   int n_items, int *queue, int apc, int lsw,
+                                                                   int lens_later)
+{
+    construct_nn_body<FIN, 3>(args, items, n_items, queue, apc, lsw, lens_later != 0);
 }
 
 // The helper-warp variant runs one CTA per SM (few ants, latency bound): its
@@ -1018,11 +1053,13 @@ size_t construct_nn_smem(int n, int K, int Kp, int apc, bool stage_total, bool p
 
 cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue, int apc,
                                 size_t smem, int sm_count, bool finite_maxd, cudaStream_t st, int ls_warps, bool draw,
-                                bool lens_later)
+                                bool lens_later, bool wide)
 {
     if (ls_warps > 0) draw = false;
+    if (ls_warps > 0 || draw) wide = false;
     auto kern = ls_warps > 0 ? (finite_maxd ? construct_nn_kernel<true, 2> : construct_nn_kernel<false, 2>)
                 : draw       ? (finite_maxd ? construct_nn_draw_kernel<true> : construct_nn_draw_kernel<false>)
+                : wide       ? (finite_maxd ? construct_nn_wide_kernel<true> : construct_nn_wide_kernel<false>)
                              : (finite_maxd ? construct_nn_kernel<true, 0> : construct_nn_kernel<false, 0>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

@@ -149,9 +149,11 @@ cudaError_t launch_construct_parity(const ConstructArgs &a, int warps_per_ant, i
 // lens_later: the route-level 2-opt follows in the same iteration and writes
 // the lengths of every ant it gets from the route list; the construct leaves
 // them out for instances that have the list.
+// wide (no helper draws, no fused 2-opt): the 64-register kernel that runs two
+// CTAs per SM; `smem` must then leave room for the second CTA.
 cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items, int n_items, int *d_queue,
                                 int ants_per_cta, size_t smem, int sm_count, bool finite_maxd, cudaStream_t st,
-                                int ls_warps = 0, bool draw = false, bool lens_later = false);
+                                int ls_warps = 0, bool draw = false, bool lens_later = false, bool wide = false);
 // 2-opt: one CTA of `warps` warps per ant; d_ant_inst[g] = instance of global ant g,
 // d_ant_base[b] = first global ant of instance b.
 // Route-level 2-opt over the construct's route list (d_ctr: {entries, next,

@@ -102,6 +102,7 @@ int check_params(const aco_params &p, int n)
     if (p.route_ls < -1 || p.route_ls > 1) return ACO_ERR_INVALID;
     if (p.wait_limit < 0) return ACO_ERR_INVALID;
     if (p.ls_best < 0 || p.ls_best > 1) return ACO_ERR_INVALID;
+    if (p.construct_ctas < 0 || p.construct_ctas > 2) return ACO_ERR_INVALID;
     if (!(p.rho > 0.0f && p.rho <= 1.0f)) return ACO_ERR_INVALID;
     if (p.n_ants > 56 * 1024) return ACO_ERR_INVALID; // the statistics kernel holds n_ants lengths in shared memory
     return ACO_OK;
@@ -409,6 +410,19 @@ int ring_read(Colony &c, LenRing &lr, long long ticket, float *lens, size_t cap)
     std::memcpy(&status, src + lr.words, sizeof(int));
     return status; // the device status word when the copy was queued
 }
+
+// The launch shape a colony planned (aco_get_config, aco_batch_get_config).
+int get_config(const Colony &c, int *ants_per_block, int *warps_per_ant, int *staging_flags)
+{
+    const bool thr = c.p.mode == ACO_MODE_THROUGHPUT;
+    if (ants_per_block) *ants_per_block = thr ? c.cn_apc : c.cp_apc;
+    if (warps_per_ant) *warps_per_ant = thr ? 1 : c.cp_wpa;
+    if (staging_flags)
+        *staging_flags = (thr ? (c.inst[0].smat ? 1 : 0) : (c.cp_stage ? 1 : 0)) | 2 | (thr && c.cn_draw ? 4 : 0) |
+                         (thr && c.cn_wide && c.cn_lsw == 0 ? 8 : 0);
+    return ACO_OK;
+}
+
 } // namespace
 
 int aco_enqueue_lengths(aco_solver *s, long long *ticket)
@@ -639,15 +653,14 @@ int aco_time_phases(aco_solver *s, int n_iter, float *ms4)
 
 int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *staging_flags)
 {
-    if (!s) return ACO_ERR_INVALID;
-    const Colony &c = s->c;
-    const bool thr = c.p.mode == ACO_MODE_THROUGHPUT;
-    if (ants_per_block) *ants_per_block = thr ? c.cn_apc : c.cp_apc;
-    if (warps_per_ant) *warps_per_ant = thr ? 1 : c.cp_wpa;
-    if (staging_flags)
-        *staging_flags = (thr ? (c.inst[0].smat ? 1 : 0) : (c.cp_stage ? 1 : 0)) | 2 | (thr && c.cn_draw ? 4 : 0);
-    return ACO_OK;
+    return s ? get_config(s->c, ants_per_block, warps_per_ant, staging_flags) : ACO_ERR_INVALID;
 }
+
+int aco_batch_get_config(aco_batch *b, int *ants_per_block, int *warps_per_ant, int *staging_flags)
+{
+    return b ? get_config(b->c, ants_per_block, warps_per_ant, staging_flags) : ACO_ERR_INVALID;
+}
+
 
 int aco_validate(aco_solver *s, int *flags, int *n_invalid)
 {
@@ -869,9 +882,10 @@ int autotune(const InstanceSpec *specs, int count, const aco_params &p0, int ite
         best_c = best_ph[0] * kMargin;
         any = true;
     }
-    // construct: ants per CTA x (warps per ant | matrix staging x helper draw warps)
+    // construct: ants per CTA x (warps per ant | matrix staging x (helper draw warps |
+    // CTAs per SM))
     struct Cand {
-        int apc, second, draw;
+        int apc, second, draw, ctas;
     };
     std::vector<Cand> cands;
     if (thr) {
@@ -880,12 +894,17 @@ int autotune(const InstanceSpec *specs, int count, const aco_params &p0, int ite
                 for (int draw : {-1, 1}) {
                     if (p0.draw_warps != 0 && draw != p0.draw_warps) continue;
                     if (draw == 1 && apc > 8) continue; // a helper warp per ant: at most 8 ants per CTA
-                    cands.push_back({apc, stage, draw});
+                    if (draw == 1) {
+                        cands.push_back({apc, stage, draw, 1});
+                        continue;
+                    }
+                    for (int ctas : {1, 2})
+                        if (p0.construct_ctas == 0 || ctas == p0.construct_ctas) cands.push_back({apc, stage, draw, ctas});
                 }
     } else {
         for (int wpa : {1, 2, 4, 8})
             for (int apc : {1, 2, 4, 8})
-                if (wpa * apc <= 16 && 32 * wpa <= p0.nloc) cands.push_back({apc, wpa, 0});
+                if (wpa * apc <= 16 && 32 * wpa <= p0.nloc) cands.push_back({apc, wpa, 0, 0});
     }
     for (const auto &cd : cands) {
         aco_params q = p0;
@@ -893,6 +912,7 @@ int autotune(const InstanceSpec *specs, int count, const aco_params &p0, int ite
         if (thr) {
             q.stage_matrix = cd.second;
             q.draw_warps = cd.draw;
+            q.construct_ctas = cd.ctas;
         } else {
             q.warps_per_ant = cd.second;
         }

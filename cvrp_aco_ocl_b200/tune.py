@@ -26,7 +26,8 @@ from typing import Dict, List, Optional, Sequence, Tuple
 from . import _lib
 from ._lib import AcoInstance, AcoParams, check, lib
 
-SHAPE_FIELDS = ("ants_per_block", "warps_per_ant", "ls_warps", "stage_matrix", "ls_ants", "draw_warps", "route_ls")
+SHAPE_FIELDS = ("ants_per_block", "warps_per_ant", "ls_warps", "stage_matrix", "ls_ants", "draw_warps", "route_ls",
+                "construct_ctas")
 
 
 @dataclasses.dataclass
@@ -45,6 +46,7 @@ class TuneEntry:
     draw_warps: int = 0  # helper draw warps (0 = the library's default)
     route_ls: int = 0    # route-level 2-opt (0 = the library's default)
     batch: int = 0       # 1: tuned on a batch of instances in [n_lo, n_hi] (for Batch), 0: on one instance
+    construct_ctas: int = 0  # construct CTAs per SM (0 = the library's default)
 
 
 class TuneTable:
@@ -159,11 +161,11 @@ def build_table(sizes: Sequence[int], ants: int, mode: int = _lib.MODE_THROUGHPU
         ms = sum(mss) / len(mss)
         e = TuneEntry(mode, lo, hi, ants, agree["ants_per_block"], agree["warps_per_ant"], agree["ls_warps"],
                       agree["stage_matrix"], ms, min(nn_ants, n - 2), agree["ls_ants"], agree["draw_warps"],
-                      agree["route_ls"])
+                      agree["route_ls"], construct_ctas=agree["construct_ctas"])
         table.add(e)
         if log:
             log(f"n={n} [{lo},{hi}] ants={ants}: apc={e.ants_per_block} wpa={e.warps_per_ant} "
-                f"ls_warps={e.ls_warps} ls_ants={e.ls_ants} stage={e.stage_matrix} {ms:.3f} ms/iter ({time.perf_counter() - t0:.1f} s)")
+                f"ls_warps={e.ls_warps} ls_ants={e.ls_ants} stage={e.stage_matrix} ctas={e.construct_ctas} {ms:.3f} ms/iter ({time.perf_counter() - t0:.1f} s)")
     return table
 
 
@@ -183,14 +185,15 @@ def build_batch_entry(seed: int, count: int, n_min: int, n_max: int, ants: int, 
     t0 = time.perf_counter()
     out, ms = autotune_batch(probs, p, iters)
     e = TuneEntry(_lib.MODE_THROUGHPUT, n_min + 1, n_max + 1, ants, out.ants_per_block, out.warps_per_ant,
-                  out.ls_warps, out.stage_matrix, ms, nn_ants, out.ls_ants, out.draw_warps, out.route_ls, batch=1)
+                  out.ls_warps, out.stage_matrix, ms, nn_ants, out.ls_ants, out.draw_warps, out.route_ls, batch=1,
+                  construct_ctas=out.construct_ctas)
     table.entries = [x for x in table.entries if not (x.batch and x.n_lo == e.n_lo and x.n_hi == e.n_hi
                                                       and x.ants == e.ants)]
     table.entries.append(e)
     table.entries.sort(key=lambda x: (x.mode, x.batch, x.n_lo, x.ants))
     if log:
         log(f"batch of {count} [{e.n_lo},{e.n_hi}] ants={ants}: apc={e.ants_per_block} stage={e.stage_matrix} "
-            f"draw={e.draw_warps} route_ls={e.route_ls} {ms:.3f} ms/iter ({time.perf_counter() - t0:.1f} s)")
+            f"draw={e.draw_warps} route_ls={e.route_ls} ctas={e.construct_ctas} {ms:.3f} ms/iter ({time.perf_counter() - t0:.1f} s)")
     return table
 
 

@@ -115,6 +115,11 @@ typedef struct aco_params {
                              every move of a route of at most 32 nodes evaluated from its distance tile and the
                              best applied (a warp argmin) until none improves; longer routes keep first
                              improvement.  For symmetric distances. */
+    int construct_ctas;   /* throughput construct without helper draws or fused 2-opt: 2 = two 512-thread CTAs per
+                             SM at 64 registers a thread, candidate tables that do not fit half of an SM's shared
+                             memory read through L2; 1 = one CTA per SM at up to 128 registers, tables staged where
+                             they fit; 0 = automatic (two while there are at least 32 ants per SM); same results
+                             either way */
 } aco_params;
 
 /* One best-so-far record {iteration, length, seconds since init} (problem.h:62-66). */
@@ -245,7 +250,8 @@ int aco_time_phases(aco_solver *s, int n_iter, float *ms4);
 /* the kernel configuration the solver picked: ants per CTA and warps per ant of
  * construct, and whether matrices are staged in shared memory (bit 0: total_info
  * in construct, bit 1: NN lists in 2-opt); bit 2: the throughput construct runs
- * with helper draw warps (construct_nn_draw_kernel). */
+ * with helper draw warps (construct_nn_draw_kernel); bit 3: it runs two CTAs per
+ * SM (construct_nn_wide_kernel). */
 int aco_get_config(aco_solver *s, int *ants_per_block, int *warps_per_ant, int *staging_flags);
 
 /* ---- validation and output -------------------------------------------------
@@ -314,6 +320,9 @@ int aco_batch_get_best(aco_batch *b, int idx, int *tour, int cap, int *tour_size
 int aco_batch_get_solutions(aco_batch *b, int idx, int *solutions, size_t cap_ints, float *lens, size_t cap_lens);
 int aco_batch_get_pheromone(aco_batch *b, int idx, float *tau, float *total_info, size_t cap);
 int aco_batch_time_phases(aco_batch *b, int n_iter, float *ms4);
+/* aco_get_config for a batch (its one construct launch over all instances; bit 0
+ * describes instance 0). */
+int aco_batch_get_config(aco_batch *b, int *ants_per_block, int *warps_per_ant, int *staging_flags);
 void *aco_batch_get_stream(aco_batch *b);
 /* number of kernel launches one batch iteration makes (graph nodes).  No reference counterpart. */
 int aco_batch_launches_per_iteration(aco_batch *b);

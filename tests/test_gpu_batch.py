@@ -54,21 +54,28 @@ def assert_same(B, b, S):
     assert np.array_equal(bb, bs) and lbb == lbs
 
 
-@pytest.mark.parametrize("sizes,A", [
-    ([40, 120, 200, 75, 333, 64], 48),       # uneven sizes, work items sorted by size
-    ([100, 100, 100, 100], 128),             # equal sizes
-    ([700, 30, 999], 40),                    # one instance past the smem matrix limit
+@pytest.mark.parametrize("sizes,A,kw", [
+    ([40, 120, 200, 75, 333, 64], 48, {}),   # uneven sizes, work items sorted by size
+    ([100, 100, 100, 100], 128, {}),         # equal sizes
+    ([700, 30, 999], 40, {}),                # one instance past the smem matrix limit
+    # two construct CTAs per SM (tables of up to ~350 nodes staged, the rest read
+    # through L2) against single solvers at one CTA per SM
+    ([40, 120, 200, 75, 333, 64, 700, 999], 48, {"construct_ctas": 2}),
+    ([150, 420, 1000], 96, {"construct_ctas": 2, "route_ls": 1}),
 ])
-def test_batch_members_match_single_solvers(gpu, sizes, A):
+def test_batch_members_match_single_solvers(gpu, sizes, A, kw):
     probs = mixed_problems(300 + len(sizes), sizes)
     rs0 = 9000 + A
-    p = batch_params(max(pr.num_node for pr in probs), A, rs0)
+    p = batch_params(max(pr.num_node for pr in probs), A, rs0, **kw)
     with Batch(probs, p) as B:
         assert B.size() == (len(probs), A * len(probs))
+        if kw.get("construct_ctas") == 2:
+            assert B.config()[2] & 8  # the two-CTA kernel runs
         B.init()
         B.iterate(3)
         for b, pr in enumerate(probs):
             with Solver(pr, batch_params(pr.num_node, A, rs0 + b)) as S:
+                assert not S.config()[2] & 8
                 S.init()
                 S.iterate(3)
                 assert_same(B, b, S)

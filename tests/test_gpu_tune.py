@@ -33,16 +33,21 @@ def same(a, b):
     return all(np.array_equal(x, y) for x, y in zip(a, b))
 
 
-@pytest.mark.parametrize("n_cust", [120, 400])
+@pytest.mark.parametrize("n_cust", [120, 400, 1100])
 def test_throughput_shapes_identical(gpu, n_cust):
     prob = Problem.from_instance(I.gen_mixed(90 + n_cust, n_cust))
     n = prob.num_node
     ref = run(prob, params(n, 96, MODE_THROUGHPUT))
-    for apc, stage, lsw, draw, route in [(1, 0, 4, 1, -1), (4, -1, 32, -1, 1), (16, 0, 8, -1, -1),
-                                          (2, -1, 1, 1, 1), (8, 0, 16, 1, -1)]:
+    # (ants per CTA, matrix staging, 2-opt warps, helper draws, route list, construct CTAs per SM)
+    shapes = [(1, 0, 4, 1, -1, 0), (4, -1, 32, -1, 1, 1), (16, 0, 8, -1, -1, 2), (2, -1, 1, 1, 1, 0),
+              (8, 0, 16, 1, -1, 0), (16, 0, 8, -1, 1, 2), (4, 0, 8, -1, -1, 2)]
+    for apc, stage, lsw, draw, route, ctas in shapes[:4] if n > 1024 else shapes:
+        with Solver(prob, params(n, 96, MODE_THROUGHPUT, ants_per_block=apc, stage_matrix=stage, ls_warps=lsw,
+                                 draw_warps=draw, route_ls=route, construct_ctas=ctas)) as S:
+            assert bool(S.config()[2] & 8) == (ctas == 2)
         got = run(prob, params(n, 96, MODE_THROUGHPUT, ants_per_block=apc, stage_matrix=stage, ls_warps=lsw,
-                               draw_warps=draw, route_ls=route))
-        assert same(ref, got), (apc, stage, lsw, draw, route)
+                               draw_warps=draw, route_ls=route, construct_ctas=ctas))
+        assert same(ref, got), (apc, stage, lsw, draw, route, ctas)
 
 
 def test_parity_shapes_identical(gpu):
