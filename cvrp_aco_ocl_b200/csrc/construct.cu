@@ -507,7 +507,12 @@ __device__ __forceinline__ int min_open_demand(const int *s_dem, uint32_t vis, c
 
 // The feasible customer of the full row with the largest total_info (ties:
 // lowest index), -1 if none: the step's path when no listed candidate fits.
-template <bool FIN, bool REGVIS>
+// PRUNE (register visited set only): test the demands first, from shared
+// memory, and read row values only for the nodes that fit; a route's last step
+// (nothing fits) then ends without reading the row.  Measured: it pays where the
+// row is read from L2 by few warps (the helper-warp kernel on large instances)
+// and costs where the row is staged or many warps share the SM.
+template <bool FIN, bool REGVIS, bool PRUNE = false>
 __device__ __forceinline__ int best_of_row(const float *row, const int *s_dem, const float *s_d0, const float *drow,
                                            uint32_t vis, const uint32_t *vism, int n, int words, int lane, int load,
                                            int cap, float rdist, float serv, float maxd)
@@ -515,12 +520,30 @@ __device__ __forceinline__ int best_of_row(const float *row, const int *s_dem, c
     const unsigned FULL = 0xffffffffu;
     uint32_t bk = 0u, bi = 0xffffffffu;
     if (REGVIS) {
-        // Only the lane's unvisited nodes, lowest first (so a strict > keeps the
-        // lowest index of a lane's equal values), four a round with their loads
-        // issued first; rounds until the lane with the most unvisited nodes is done.
-        uint32_t open = open_bits(vis, n, lane);
-        const int rounds = ((int)__reduce_max_sync(FULL, (unsigned)__popc(open)) + 3) >> 2;
         const int capleft = cap - load;
+        uint32_t open = open_bits(vis, n, lane);
+        if (PRUNE) { // the lane's unvisited nodes whose demand fits, eight a round
+            uint32_t fit = 0u;
+            const int rounds = ((int)__reduce_max_sync(FULL, (unsigned)__popc(open)) + 7) >> 3;
+            for (int r = 0; r < rounds; r++) {
+                int kb[8], dm[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    kb[u] = open ? __ffs(open) - 1 : 0;
+                    dm[u] = open ? s_dem[lane + 32 * kb[u]] : 0x7fffffff; // no node: does not fit
+                    open &= open - 1u;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++) fit |= (dm[u] <= capleft ? 1u : 0u) << kb[u];
+            }
+            if (!__any_sync(FULL, fit != 0u)) return -1;
+            open = fit;
+        }
+        // Only the lane's unvisited (PRUNE: and fitting) nodes, lowest first (so a
+        // strict > keeps the lowest index of a lane's equal values), four a round
+        // with their loads issued first; rounds until the lane with the most such
+        // nodes is done.
+        const int rounds = ((int)__reduce_max_sync(FULL, (unsigned)__popc(open)) + 3) >> 2;
         for (int r = 0; r < rounds; r++) {
             int idx[4], dm[4];
             float rv[4], dv[4];
@@ -531,7 +554,7 @@ __device__ __forceinline__ int best_of_row(const float *row, const int *s_dem, c
                 const int ic = i >= 0 ? i : 0;
                 idx[u] = i;
                 rv[u] = row[ic];
-                dm[u] = i >= 0 ? s_dem[ic] : 0x7fffffff; // no node: fails the capacity test
+                dm[u] = i < 0 ? 0x7fffffff : PRUNE ? 0 : s_dem[ic]; // no node: fails the capacity test
                 if (FIN) dv[u] = __ldg(drow + ic);
             }
 #pragma unroll
@@ -767,7 +790,7 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 nxt = (int)(pick & 0xFFFFu);
                 nd = (int)(pick >> 16);
             } else if (DRAW) {
-                nxt = best_of_row<FIN, REGVIS>(SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld, s_dem, s_d0,
+                nxt = best_of_row<FIN, REGVIS, !SMAT>(SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld, s_dem, s_d0,
                                                a.dist + (size_t)cur * ld, vis, vism, n, words, lane, load, cap, rdist,
                                                a.serv_time, a.max_dist);
                 if (nxt >= 0) nd = s_dem[nxt];

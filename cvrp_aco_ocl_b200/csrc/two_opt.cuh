@@ -22,6 +22,32 @@ constexpr int kRL = 32; // largest route (nodes, depot included) of the register
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
+// The 2-opt move that replaces edges (h1,h2) and (h3,h4) by (h1,h3) and (h2,h4)
+// (kernel.cl:235-270) on the lane-per-position state: the positions between
+// the two edges are reversed and dist_tour_wrk follows them.
+__device__ __forceinline__ void route_exchange(int lane, const float *tile, int h1, int h2, int h3, int h4, int &tq,
+                                               int &pk, float &dq)
+{
+    const unsigned FULLM = 0xffffffffu;
+    int p1 = __shfl_sync(FULLM, pk, h1), p3 = __shfl_sync(FULLM, pk, h3);
+    if (p3 < p1) {
+        int t = h1; h1 = h3; h3 = t;
+        t = h2; h2 = h4; h4 = t;
+        t = p1; p1 = p3; p3 = t;
+    }
+    const int i = p1, jj = p3, a = __shfl_sync(FULLM, pk, h2);
+    const float d13 = tile[h1 * kRL + h3], d24 = tile[h2 * kRL + h4];
+    // dist_tour_wrk: [i] = d(h1,h3), [jj] = d(h2,h4), (i, jj) reversed
+    const float dsrc = __shfl_sync(FULLM, dq, (lane > i && lane < jj) ? i + jj - lane : lane);
+    if (lane == jj) dq = d24; // written after [i], as kernel.cl:249-250
+    else if (lane == i) dq = d13;
+    else if (lane > i && lane < jj) dq = dsrc;
+    // tour positions [a, jj] reversed; positions of the moved nodes mirrored
+    const int tsrc = __shfl_sync(FULLM, tq, (lane >= a && lane <= jj) ? a + jj - lane : lane);
+    if (lane >= a && lane <= jj) tq = tsrc;
+    if (pk >= a && pk <= jj) pk = a + jj - pk;
+}
+
 // ---------------------------------------------------------------------------
 // Register path: routes of at most 32 nodes.
 // ---------------------------------------------------------------------------
@@ -139,23 +165,7 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
             // exchange (kernel.cl:235-270)
             imp = true;
             dlb &= ~((1u << h1) | (1u << h2) | (1u << h3) | (1u << h4));
-            int p1 = __shfl_sync(FULLM, pk, h1), p3 = __shfl_sync(FULLM, pk, h3);
-            if (p3 < p1) {
-                int t = h1; h1 = h3; h3 = t;
-                t = h2; h2 = h4; h4 = t;
-                t = p1; p1 = p3; p3 = t;
-            }
-            const int i = p1, jj = p3, a = __shfl_sync(FULLM, pk, h2);
-            const float d13 = tile[h1 * kRL + h3], d24 = tile[h2 * kRL + h4];
-            // dist_tour_wrk: [i] = d(h1,h3), [jj] = d(h2,h4), (i, jj) reversed
-            const float dsrc = __shfl_sync(FULLM, dq, (lane > i && lane < jj) ? i + jj - lane : lane);
-            if (lane == jj) dq = d24; // written after [i], as kernel.cl:249-250
-            else if (lane == i) dq = d13;
-            else if (lane > i && lane < jj) dq = dsrc;
-            // tour positions [a, jj] reversed; positions of the moved nodes mirrored
-            const int tsrc = __shfl_sync(FULLM, tq, (lane >= a && lane <= jj) ? a + jj - lane : lane);
-            if (lane >= a && lane <= jj) tq = tsrc;
-            if (pk >= a && pk <= jj) pk = a + jj - pk;
+            route_exchange(lane, tile, h1, h2, h3, h4, tq, pk, dq);
             by_node();
             open = __ballot_sync(FULLM, lane < R && !((dlb >> tq) & 1u)) & rmask; // the tour and bits changed
             const uint32_t ahead = q1 >= 31 ? 0u : (open & ~((2u << q1) - 1u)); // the scan goes on after q1
