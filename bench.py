@@ -65,6 +65,11 @@ PHASE_KERNELS = {"construct": "construct_nn_kernel", "two_opt": "route_opt_kerne
                  "stats": "stats_kernel", "rows": "rows_kernel"}
 
 
+def construct_kernel(flags: int) -> str:
+    """The throughput construct kernel a colony launches, from aco_batch_get_config's flags."""
+    return "construct_nn_wide_kernel" if flags & 8 else "construct_nn_draw_kernel" if flags & 4 else "construct_nn_kernel"
+
+
 def dist_env():
     return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
         int(os.environ.get("LOCAL_RANK", "0"))
@@ -201,7 +206,7 @@ def timed_launches(enqueue, stream, steps, dev):
 
 
 # --------------------------------------------------------------------------
-def kernel_rooflines(phase_ms, steps, row_bytes, clk, peak_hbm, peak_src, workload_tag):
+def kernel_rooflines(phase_ms, steps, row_bytes, clk, peak_hbm, peak_src, workload_tag, kernels=None):
     """Per phase: launch time, share and the bound that limits it.  The pheromone
     pass is HBM-bound (16 bytes per matrix element); the construct and the 2-opt
     are issue-bound (many independent warp-serial chains, no bandwidth near a
@@ -209,19 +214,20 @@ def kernel_rooflines(phase_ms, steps, row_bytes, clk, peak_hbm, peak_src, worklo
     profiles/) / the live launch time, against 148 SMs x 4 schedulers x the SM
     clock sampled during the timed region."""
     out = {}
+    kernels = dict(PHASE_KERNELS, **(kernels or {}))
     total = float(sum(phase_ms))
     mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
     issue_peak = 148 * 4 * mhz * 1e6 / 1e9  # G warp-instructions/s
     for k, name in enumerate(PHASES):
         launch_ms = float(phase_ms[k]) / steps
-        e = {"kernel": PHASE_KERNELS[name], "launch_ms": launch_ms, "share": float(phase_ms[k]) / total}
+        e = {"kernel": kernels[name], "launch_ms": launch_ms, "share": float(phase_ms[k]) / total}
         if name == "rows":
             ach = row_bytes / (launch_ms / 1e3) / 1e9
             e.update({"bound": "hbm", "achieved": ach, "peak": peak_hbm, "unit": "GB/s", "frac": ach / peak_hbm,
                       "algorithmic_bytes_per_launch": row_bytes, "peak_source": peak_src,
                       "traffic": profile_figure("dram_bytes_per_launch", f"rows_kernel@{workload_tag}")})
         elif name in ("construct", "two_opt"):
-            ks = PHASE_KERNELS[name].split("+")
+            ks = kernels[name].split("+")
             insts = [profile_figure("warp_inst_per_launch", f"{k2}@{workload_tag}") for k2 in ks]
             inst = sum(insts) if all(v is not None for v in insts) else None
             ach = inst / (launch_ms / 1e3) / 1e9 if inst is not None else None
@@ -281,11 +287,13 @@ def run_ours(args, ws, rank, local):
     # per-phase device time, same batch and stream, phase by phase with events between
     n_phase = max(3, args.steps // 2)
     phase_ms = B.time_phases(n_phase)
+    ckern = construct_kernel(B.config()[2])
     B.close()
     row_bytes = sum(16 * p.num_node * p.num_node for p in probs)
     peak, peak_src = load_peaks()
     clocks = clk.summary()
-    kern = kernel_rooflines(phase_ms, n_phase, row_bytes, clocks, peak, peak_src, "batch512")
+    kern = kernel_rooflines(phase_ms, n_phase, row_bytes, clocks, peak, peak_src, "batch512",
+                            {"construct": ckern})
     dom = max(kern, key=lambda k: kern[k]["share"])
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
