@@ -316,7 +316,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     };
     struct Offs {
         size_t dist, heur, tau, total, chc, dem, key, jump, adv, cand32, nn16, nnls, seeds, sol, elites, succ,
-            dep, dtau, rec, nbsf, iter, xy, nnfull;
+            dep, dtau, rec, nbsf, iter, xy;
     };
     std::vector<Offs> offs(count);
     for (int b = 0; b < count; b++) {
@@ -342,7 +342,6 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         o.nbsf = take(4);
         o.iter = take(4);
         o.xy = ih.device_prep ? take((size_t)2 * ih.n4 * 4) : 0;
-        o.nnfull = ih.device_prep ? take((size_t)ih.n * std::max(1, ih.depth) * 4) : 0;
     }
     const size_t o_status = take(4), o_t0 = take(8), o_queue = take(8); // construct queue: next item, CTAs done
     const size_t o_wait = take(4); // poll limit of the device waits
@@ -369,6 +368,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     const size_t o_invalid = take((size_t)count * 4);
     const size_t o_cargs = take(sizeof(ConstructArgs) * count), o_largs = take(sizeof(LocalSearchArgs) * count);
     const size_t o_sargs = take(sizeof(StatsArgs) * count), o_uargs = take(sizeof(UpdateArgs) * count);
+    const size_t o_pargs = take(sizeof(PrepArgs) * count);
     // construct work items {instance, first ant}, larger instances first
     // (set after cn_apc is known; sized for apc = 1)
     const size_t o_items = take((size_t)total_ants * sizeof(int2));
@@ -434,7 +434,6 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         ih.nbsf_d = (int *)(base + o.nbsf); ih.iter_d = (int *)(base + o.iter);
         if (ih.device_prep) {
             ih.xy_d = (float *)(base + o.xy);
-            ih.nnfull_d = (int *)(base + o.nnfull);
         }
     }
     status_d = (int *)(base + o_status);
@@ -458,6 +457,7 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     largs_d_ = (LocalSearchArgs *)(base + o_largs);
     sargs_d_ = (StatsArgs *)(base + o_sargs);
     uargs_d_ = (UpdateArgs *)(base + o_uargs);
+    PrepArgs *pargs_d = (PrepArgs *)(base + o_pargs);
     items_d_ = (int2 *)(base + o_items);
     sw_items_d_ = (int2 *)(base + o_sw_items);
     ns_items_d_ = (int2 *)(base + o_ns_items);
@@ -672,17 +672,21 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
         }
     }
     ok = ok && stage.flush(res->pool, sm_count, st) == cudaSuccess;
+    std::vector<PrepArgs> pargs(count);
+    int n_prep = 2; // the longest row the batched list kernel stages
     for (int b = 0; b < count; b++) {
         InstHost &ih = inst[b];
         const int n = ih.n;
-        if (ih.device_prep) { // distances, lists and tables on the device (prep.cu)
-            ok = ok && launch_dist(n, ih.xy_d, ih.xy_d + ih.n4, ih.dist_type, ih.dist_d, ih.ld, sm_count, st) ==
-                           cudaSuccess;
-            if (ih.depth > 0) {
-                ok = ok && launch_nn(n, ih.dist_d, ih.ld, ih.depth, ih.nnfull_d, status_d, st) == cudaSuccess;
-                ok = ok && launch_tables(n, ih.nnfull_d, ih.depth, ih.K, ih.Kp, ih.nn_ls, ih.dem_d, ih.nn16_d,
-                                         ih.cand32_d, ih.nnls_d, sm_count, st) == cudaSuccess;
-            }
+        // distances, lists, tables (device_prep) and seeds: one launch each for the
+        // whole batch after the uploads (prep.cu)
+        PrepArgs &pa = pargs[b];
+        pa = PrepArgs{};
+        pa.n = n; pa.ld = ih.ld; pa.depth = ih.depth; pa.K = ih.K; pa.Kp = ih.Kp; pa.nn_ls = ih.nn_ls;
+        pa.dist_type = ih.dist_type; pa.device_prep = ih.device_prep ? 1 : 0; pa.n_ants = ih.A;
+        pa.x = ih.xy_d; pa.y = ih.xy_d ? ih.xy_d + ih.n4 : nullptr; pa.dist = ih.dist_d; pa.demand = ih.dem_d;
+        pa.nn16 = ih.nn16_d; pa.cand32 = ih.cand32_d; pa.nnls = ih.nnls_d; pa.seeds = ih.seeds_d;
+        if (ih.device_prep) {
+            n_prep = std::max(n_prep, n);
         } else {
             ok = ok && cudaMemcpy2DAsync(ih.dist_d, (size_t)ih.ld * 4, ih.dist.data(), (size_t)n * 4, (size_t)n * 4,
                                          n, cudaMemcpyHostToDevice, st) == cudaSuccess;
@@ -718,8 +722,6 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
                 for (int j = 0; j < ih.nn_ls; j++) nnls[(size_t)i * ih.nn_ls + j] = ih.nn[(size_t)i * ih.depth + j];
             up(ih.nnls_d, nnls.data(), nnls.size() * 4);
         }
-        // instance b of a batch: rnd_seed + b
-        ok = ok && launch_seeds(p.seed_time, p.rnd_seed + b, ih.A, ih.nloc, ih.seeds_d, sm_count, st) == cudaSuccess;
 
         ConstructArgs &c = cargs_h_[b];
         c = ConstructArgs{};
@@ -774,8 +776,11 @@ int Colony::create(const InstanceSpec *specs, int count, const aco_params &pin)
     up(items_d_, items.data(), items.size() * sizeof(int2));
     up(sw_items_d_, swi.data(), swi.size() * sizeof(int2));
     up(ns_items_d_, nsi.data(), nsi.size() * sizeof(int2));
+    up(pargs_d, pargs.data(), sizeof(PrepArgs) * count);
     ok = ok && stage.flush(res->pool, sm_count, st) == cudaSuccess;
     if (!ok) return ACO_ERR_CUDA;
+    CK(launch_prep_batch(pargs_d, row_base_d_, row_inst_d_, total_rows, n_prep, ant_base_d_, ant_inst_d_, total_ants,
+                         p.nloc, p.seed_time, p.rnd_seed, status_d, sm_count, st));
     rc = run_rows(ROW_HEUR, 0.f);
     if (rc != ACO_OK) return rc;
     CK(cudaStreamSynchronize(st));
@@ -1128,12 +1133,7 @@ int Colony::init()
 {
     int rc = set_device();
     if (rc != ACO_OK) return rc;
-    const float inf = INFINITY;
-    for (InstHost &ih : inst) {
-        CK(cudaMemcpyAsync(ih.lens_d + ih.A, &inf, sizeof(float), cudaMemcpyHostToDevice, st));
-        CK(cudaMemsetAsync(ih.nbsf_d, 0, sizeof(int), st));
-        CK(cudaMemsetAsync(ih.iter_d, 0, sizeof(int), st));
-    }
+    CK(launch_reset_slots(sargs_d_, (int)inst.size(), st));
     CK(cudaMemsetAsync(status_d, 0, sizeof(int), st));
     CK(launch_t0(t0_d_, st));
     t_init = std::chrono::steady_clock::now();

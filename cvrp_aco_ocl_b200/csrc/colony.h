@@ -50,8 +50,7 @@ struct InstHost {
     int *succ_d = nullptr, *nbsf_d = nullptr, *iter_d = nullptr;
     uint32_t *key_d = nullptr, *jump_d = nullptr, *adv_d = nullptr, *cand32_d = nullptr, *dep_d = nullptr;
     uint16_t *nn16_d = nullptr;
-    float *xy_d = nullptr; // device preprocessing: coordinates, then full lists (n x depth)
-    int *nnfull_d = nullptr;
+    float *xy_d = nullptr; // device preprocessing: coordinates (x, then y at n4)
     float *lens_d = nullptr, *dtau_d = nullptr;
     aco_record *rec_d = nullptr;
 };

@@ -129,7 +129,6 @@ enum RowMode {
 // Staged host -> device uploads: the pieces of one blob copied to their
 // destinations by one kernel.
 // The ants' lane seeds on the device (same values as make_seeds on the host).
-cudaError_t launch_seeds(int seed_time, int rnd_seed, int n_ants, int nloc, int *seeds, int sm_count, cudaStream_t st);
 
 struct ScatterPiece {
     unsigned long long dst, src_off, bytes;
@@ -180,6 +179,8 @@ cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, siz
 // d_row_inst[g] = the instance of global row g (null: one instance).
 cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, const int *d_row_inst, int total_rows,
                         int mode, float trail, int sm_count, cudaStream_t st);
+// lens[A] = +inf, num_bsf = 0, iteration = 0 of every instance (init_aco).
+cudaError_t launch_reset_slots(const StatsArgs *d_args, int count, cudaStream_t st);
 cudaError_t launch_t0(unsigned long long *t0, cudaStream_t st);
 
 // Shared-memory bytes of the launches (the host picks configurations that fit
@@ -222,7 +223,26 @@ size_t nn_rows_per_cta(int n);
 cudaError_t launch_dist(int n, const float *x, const float *y, int dist_type, float *dist, int ld, int sm_count,
                         cudaStream_t st);
 cudaError_t launch_nn(int n, const float *dist, int ld, int depth, int *nn, int *status, cudaStream_t st);
-cudaError_t launch_tables(int n, const int *nn, int depth, int K, int Kp, int nn_ls, const int *demand, uint16_t *nn16,
-                          uint32_t *cand32, int *nnls, int sm_count, cudaStream_t st);
+
+// One instance's inputs and outputs of the batched preprocessing.
+struct PrepArgs {
+    int n, ld, depth, K, Kp, nn_ls, dist_type;
+    int device_prep; // 0: distances and lists came from the host (skipped here, seeds still made)
+    int n_ants;
+    const float *x, *y;
+    float *dist;
+    const int *demand;
+    uint16_t *nn16;   // n x Kp: first K of the list, padded with node 0
+    uint32_t *cand32; // n x Kp: the same with the demand in the high half
+    int *nnls;        // n x nn_ls: the 2-opt list
+    int *seeds;       // n_ants x nloc
+};
+// Every instance of a batch in one launch per step (global row g: row g -
+// row_base[b] of instance b = row_inst[g]; global ant g: ant g - ant_base[b] of
+// b = ant_inst[g]): distances, then the lists (the reference's quicksort per
+// row) with the candidate and 2-opt tables, then the lane seeds (rnd_seed + b).
+cudaError_t launch_prep_batch(const PrepArgs *d_args, const int *d_row_base, const int *d_row_inst, int total_rows,
+                              int n_max, const int *d_ant_base, const int *d_ant_inst, int total_ants, int nloc,
+                              int seed_time, int rnd_seed, int *status, int sm_count, cudaStream_t st);
 
 } // namespace aco

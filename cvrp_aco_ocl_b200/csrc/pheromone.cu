@@ -443,6 +443,17 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) rows_kernel(const UpdateArg
 
 __global__ void t0_kernel(unsigned long long *t0) { *t0 = globaltimer_ns(); }
 
+// init_aco's per-instance resets: no best-so-far yet (+inf), no records, iteration 0.
+__global__ void reset_slots_kernel(const StatsArgs *args, int count)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < count; b += gridDim.x * blockDim.x) {
+        const StatsArgs a = args[b];
+        a.lens[a.n_ants] = __int_as_float(0x7f800000);
+        *a.num_bsf = 0;
+        *a.iteration = 0;
+    }
+}
+
 } // namespace
 
 cudaError_t launch_stats(const StatsArgs *d_args, int n_inst, int do_elites, size_t smem, cudaStream_t st,
@@ -491,6 +502,12 @@ cudaError_t launch_rows(const UpdateArgs *d_args, const int *d_row_base, const i
         break;
     default: rows_kernel<ROW_GATHER><<<blocks, kRowWarps * 32, 0, st>>>(d_args, d_row_base, d_row_inst, total_rows, trail); break;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_slots(const StatsArgs *d_args, int count, cudaStream_t st)
+{
+    reset_slots_kernel<<<(count + 255) / 256, 256, 0, st>>>(d_args, count);
     return cudaGetLastError();
 }
 

@@ -116,21 +116,55 @@ __global__ void nn_kernel(int n, const float *dist, int ld, int depth, int rows_
 }
 
 
-// Candidate and 2-opt tables from the lists: nn16 / cand32 (first K, padded
-// with node 0 to Kp) and the 2-opt list (first nn_ls).
-__global__ void tables_kernel(int n, const int *nn, int depth, int K, int Kp, int nn_ls, const int *demand,
-                              uint16_t *nn16, uint32_t *cand32, int *nnls)
+// Distances of every instance's rows, a warp per row (same bits as dist_kernel).
+__global__ void dist_rows_kernel(const PrepArgs *pa, const int *row_base, const int *row_inst, int total_rows)
 {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * Kp + n * nn_ls; e += gridDim.x * blockDim.x) {
-        if (e < n * Kp) {
-            const int i = e / Kp, j = e - i * Kp;
-            const int c = j < K ? nn[(size_t)i * depth + j] : 0;
-            nn16[e] = (uint16_t)c;
-            cand32[e] = (uint32_t)c | ((uint32_t)(demand[c] & 0xFFFF) << 16);
-        } else {
-            const int f = e - n * Kp, i = f / nn_ls, j = f - i * nn_ls;
-            nnls[f] = nn[(size_t)i * depth + j];
+    const int lane = threadIdx.x & 31;
+    const int w0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int g = w0; g < total_rows; g += nw) {
+        const int b = row_inst[g];
+        const PrepArgs &a = pa[b];
+        if (!a.device_prep) continue;
+        const int i = g - row_base[b];
+        float *row = a.dist + (size_t)i * a.ld;
+        for (int j = lane; j < a.n; j += 32) row[j] = dist_of(a.x, a.y, a.dist_type, i, j);
+    }
+}
+
+// Lists and tables of every instance's rows: a warp per row stages it, its
+// first lane sorts it (sort_row, as nn_kernel), and the lanes write the
+// candidate tables (first K, padded with node 0 to Kp; demand in the high half
+// of cand32) and the 2-opt list (first nn_ls) straight from the sorted row.
+__global__ void lists_rows_kernel(const PrepArgs *pa, const int *row_base, const int *row_inst, int total_rows,
+                                  int rows_per_cta, int n_max, int *status)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *v = reinterpret_cast<float *>(sm) + (size_t)w * 2 * n_max;
+    int *idx = reinterpret_cast<int *>(v + n_max);
+    for (int g = blockIdx.x * rows_per_cta + w; g < total_rows; g += gridDim.x * rows_per_cta) {
+        const int b = row_inst[g];
+        const PrepArgs &a = pa[b];
+        if (!a.device_prep || a.depth <= 0) continue;
+        const int n = a.n, i = g - row_base[b];
+        for (int k = lane; k < n; k += 32) {
+            v[k] = a.dist[(size_t)i * a.ld + k];
+            idx[k] = k;
         }
+        __syncwarp();
+        if (lane == 0) {
+            v[i] = __int_as_float(0x7f800000); // the node itself and the depot never make the list
+            v[0] = __int_as_float(0x7f800000);
+            sort_row(v, idx, n, a.depth, status);
+        }
+        __syncwarp();
+        for (int j = lane; j < a.Kp; j += 32) {
+            const int c = j < a.K ? idx[j] : 0;
+            a.nn16[(size_t)i * a.Kp + j] = (uint16_t)c;
+            a.cand32[(size_t)i * a.Kp + j] = (uint32_t)c | ((uint32_t)(a.demand[c] & 0xFFFF) << 16);
+        }
+        for (int j = lane; j < a.nn_ls; j += 32) a.nnls[(size_t)i * a.nn_ls + j] = idx[j];
+        __syncwarp(); // the row's buffers are reused by the warp's next row
     }
 }
 
@@ -170,29 +204,25 @@ cudaError_t launch_nn(int n, const float *dist, int ld, int depth, int *nn, int 
 // with m = i mod A and r_i the (i+1)-th ran01 draw from rnd_seed, in fp32 as
 // written and converted as x86 cvttss2si does (NaN and out-of-range values give
 // INT_MIN).  Draw i+1 is x0 * 16807^(i+1) mod (2^31 - 1), so every seed is
-// computed independently.
-__global__ void seeds_kernel(int seed_time, uint32_t x0, int n_ants, long long total, int *seeds)
+// computed independently.  Instance b of a batch draws from rnd_seed + b (int
+// arithmetic, as the host adds it).
+__global__ void seeds_kernel(const PrepArgs *pa, const int *ant_base, const int *ant_inst, long long total, int nloc,
+                             int seed_time, int rnd_seed)
 {
-    const float t0 = (float)seed_time, a = (float)n_ants;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const float m = (float)(int)(i % n_ants);
-        const float r = pm_uniform(pm_mul(x0, pm_pow16807(i + 1)));
-        const float v = __fadd_rn(t0, __fmul_rn(__fmul_rn(m, __fadd_rn(m, r)), a));
-        seeds[i] = (v >= -2147483648.0f && v < 2147483648.0f) ? __float2int_rz(v) : (int)0x80000000;
+    const float t0 = (float)seed_time;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)(e / nloc), l = (int)(e - (long long)g * nloc);
+        const int b = ant_inst[g];
+        const PrepArgs &a = pa[b];
+        const long long i = (long long)(g - ant_base[b]) * nloc + l;
+        long long r = (long long)(int)((unsigned)rnd_seed + (unsigned)b) % 2147483647ll;
+        if (r < 0) r += 2147483647ll;
+        const float m = (float)(int)(i % a.n_ants);
+        const float u = pm_uniform(pm_mul((uint32_t)r, pm_pow16807(i + 1)));
+        const float v = __fadd_rn(t0, __fmul_rn(__fmul_rn(m, __fadd_rn(m, u)), (float)a.n_ants));
+        a.seeds[i] = (v >= -2147483648.0f && v < 2147483648.0f) ? __float2int_rz(v) : (int)0x80000000;
     }
-}
-
-cudaError_t launch_seeds(int seed_time, int rnd_seed, int n_ants, int nloc, int *seeds, int sm_count, cudaStream_t st)
-{
-    long long r = (long long)rnd_seed % 2147483647ll;
-    if (r < 0) r += 2147483647ll;
-    const long long total = (long long)n_ants * nloc;
-    long long blocks = (total + 255) / 256;
-    if (blocks > sm_count * 8) blocks = sm_count * 8;
-    if (blocks < 1) blocks = 1;
-    seeds_kernel<<<(unsigned)blocks, 256, 0, st>>>(seed_time, (uint32_t)r, n_ants, total, seeds);
-    return cudaGetLastError();
 }
 
 // Scatter of staged uploads: piece k copies bytes [src_off, src_off + bytes)
@@ -230,12 +260,29 @@ cudaError_t launch_scatter(const ScatterPiece *d_pieces, int count, const unsign
     return cudaGetLastError();
 }
 
-cudaError_t launch_tables(int n, const int *nn, int depth, int K, int Kp, int nn_ls, const int *demand, uint16_t *nn16,
-                          uint32_t *cand32, int *nnls, int sm_count, cudaStream_t st)
+cudaError_t launch_prep_batch(const PrepArgs *d_args, const int *d_row_base, const int *d_row_inst, int total_rows,
+                              int n_max, const int *d_ant_base, const int *d_ant_inst, int total_ants, int nloc,
+                              int seed_time, int rnd_seed, int *status, int sm_count, cudaStream_t st)
 {
-    const int total = n * Kp + n * nn_ls;
-    const int blocks = std::max(1, std::min((total + 255) / 256, sm_count * 8));
-    tables_kernel<<<blocks, 256, 0, st>>>(n, nn, depth, K, Kp, nn_ls, demand, nn16, cand32, nnls);
+    if (total_rows > 0) {
+        const int blocks = std::min((total_rows + 7) / 8, sm_count * 8); // a warp per row, 8 a CTA
+        dist_rows_kernel<<<std::max(blocks, 1), 256, 0, st>>>(d_args, d_row_base, d_row_inst, total_rows);
+        int rows = (int)nn_rows_per_cta(n_max);
+        if (rows < 1) return cudaErrorInvalidValue;
+        if (rows > 8) rows = 8;
+        const size_t smem = (size_t)rows * 8 * n_max;
+        cudaError_t e = cudaFuncSetAttribute(lists_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int lblocks = std::min((total_rows + rows - 1) / rows, sm_count * 16);
+        lists_rows_kernel<<<std::max(lblocks, 1), 32 * rows, smem, st>>>(d_args, d_row_base, d_row_inst, total_rows,
+                                                                         rows, n_max, status);
+    }
+    const long long total = (long long)total_ants * nloc;
+    if (total > 0) {
+        long long blocks = (total + 255) / 256;
+        if (blocks > sm_count * 8) blocks = sm_count * 8;
+        seeds_kernel<<<(unsigned)blocks, 256, 0, st>>>(d_args, d_ant_base, d_ant_inst, total, nloc, seed_time, rnd_seed);
+    }
     return cudaGetLastError();
 }
 
