@@ -9,9 +9,11 @@
 // device reproduces the host bits.  GEO goes through cos/acos, whose last bits
 // differ between math libraries; it stays on the host.
 //
-// Lists: one warp per row stages it and its first lane runs the reference's quicksort (middle pivot
-// swapped to the left end, Lomuto partition with strict <, both halves
-// recursed) on its row in shared memory.  Only positions below the list depth
+// Lists: one warp per row stages it; when the list's nodes and the next one have
+// distinct distances the warp extracts them by repeated warp minima, otherwise
+// its first lane runs the reference's quicksort (middle pivot swapped to the
+// left end, Lomuto partition with strict <, both halves recursed) on its row in
+// shared memory.  Only positions below the list depth
 // are needed, so ranges starting at or beyond it are skipped; the ranges are
 // disjoint, so the order they are processed in does not matter and the
 // smaller one goes first (explicit stack of at most log2(n) + 1 entries).
@@ -91,8 +93,51 @@ __device__ void sort_row(float *v, int *idx, int n, int depth, int *status)
     }
 }
 
-// One warp per row: the lanes stage the row, lane 0 runs the sort alone (no
-// divergence between rows sorted by the same warp), the lanes write the list.
+// The first `depth` entries of a staged row's list, warp-wide.  When the
+// depth + 1 smallest values are all distinct, every correct sort puts the same
+// nodes in the first depth positions, so the warp extracts them in depth + 1
+// rounds of a 64-bit warp minimum over (value bits, index) -- values are >= 0,
+// so their bits order as the floats.  Otherwise (a tie decides which node comes
+// first, as with integer coordinates) lane 0 runs the reference's quicksort,
+// whose partition order settles ties exactly as the host's.  On return idx[0,
+// depth) holds the list.
+__device__ void row_list(float *v, int *idx, int n, int depth, int lane, int *status)
+{
+    const unsigned FULLM = 0xffffffffu;
+    if (depth < 32) {
+        unsigned long long prev = 0ull, mine = ~0ull;
+        bool first = true, odd = false; // odd: a negative value, -0 or NaN (their bits do not order as the floats)
+        for (int r = 0; r <= depth; r++) {
+            unsigned long long best = ~0ull;
+            for (int i = lane; i < n; i += 32) {
+                const uint32_t b = __float_as_uint(v[i]);
+                if (first) odd = odd || b > 0x7f800000u;
+                const unsigned long long k = ((unsigned long long)b << 32) | (unsigned)i;
+                if ((first || k > prev) && k < best) best = k;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long w = __shfl_xor_sync(FULLM, best, o);
+                best = w < best ? w : best;
+            }
+            if (lane == r) mine = best;
+            prev = best;
+            first = false;
+        }
+        // lanes 0..depth hold the depth + 1 smallest in order: a tie among them ends the fast path
+        const unsigned nxt = __shfl_down_sync(FULLM, (unsigned)(mine >> 32), 1);
+        const bool tie = lane < depth && (unsigned)(mine >> 32) == nxt;
+        if (!__any_sync(FULLM, tie || odd)) {
+            if (lane < depth) idx[lane] = (int)(mine & 0xffffffffu);
+            __syncwarp();
+            return;
+        }
+    }
+    if (lane == 0) sort_row(v, idx, n, depth, status);
+    __syncwarp();
+}
+
+// One warp per row: the lanes stage the row and pick its list (row_list), the
+// lanes write the list.
 __global__ void nn_kernel(int n, const float *dist, int ld, int depth, int rows_per_cta, int *nn, int *status)
 {
     extern __shared__ __align__(16) unsigned char sm[];
@@ -109,9 +154,9 @@ __global__ void nn_kernel(int n, const float *dist, int ld, int depth, int rows_
     if (lane == 0) {
         v[row] = __int_as_float(0x7f800000); // the node itself and the depot never make the list
         v[0] = __int_as_float(0x7f800000);
-        sort_row(v, idx, n, depth, status);
     }
     __syncwarp();
+    row_list(v, idx, n, depth, lane, status);
     for (int i = lane; i < depth; i += 32) nn[(size_t)row * depth + i] = idx[i];
 }
 
@@ -155,9 +200,9 @@ __global__ void lists_rows_kernel(const PrepArgs *pa, const int *row_base, const
         if (lane == 0) {
             v[i] = __int_as_float(0x7f800000); // the node itself and the depot never make the list
             v[0] = __int_as_float(0x7f800000);
-            sort_row(v, idx, n, a.depth, status);
         }
         __syncwarp();
+        row_list(v, idx, n, a.depth, lane, status);
         for (int j = lane; j < a.Kp; j += 32) {
             const int c = j < a.K ? idx[j] : 0;
             a.nn16[(size_t)i * a.Kp + j] = (uint16_t)c;
@@ -206,22 +251,30 @@ cudaError_t launch_nn(int n, const float *dist, int ld, int depth, int *nn, int 
 // INT_MIN).  Draw i+1 is x0 * 16807^(i+1) mod (2^31 - 1), so every seed is
 // computed independently.  Instance b of a batch draws from rnd_seed + b (int
 // arithmetic, as the host adds it).
-__global__ void seeds_kernel(const PrepArgs *pa, const int *ant_base, const int *ant_inst, long long total, int nloc,
+constexpr int kSeedRun = 16; // consecutive seeds of one ant a thread makes (nloc a multiple of it)
+
+__global__ void seeds_kernel(const PrepArgs *pa, const int *ant_base, const int *ant_inst, long long runs, int nloc,
                              int seed_time, int rnd_seed)
 {
     const float t0 = (float)seed_time;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+    const int per_ant = nloc / kSeedRun;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < runs;
          e += (long long)gridDim.x * blockDim.x) {
-        const int g = (int)(e / nloc), l = (int)(e - (long long)g * nloc);
+        const int g = (int)(e / per_ant), c = (int)(e - (long long)g * per_ant);
         const int b = ant_inst[g];
         const PrepArgs &a = pa[b];
-        const long long i = (long long)(g - ant_base[b]) * nloc + l;
+        const long long i0 = (long long)(g - ant_base[b]) * nloc + (long long)c * kSeedRun;
         long long r = (long long)(int)((unsigned)rnd_seed + (unsigned)b) % 2147483647ll;
         if (r < 0) r += 2147483647ll;
-        const float m = (float)(int)(i % a.n_ants);
-        const float u = pm_uniform(pm_mul((uint32_t)r, pm_pow16807(i + 1)));
-        const float v = __fadd_rn(t0, __fmul_rn(__fmul_rn(m, __fadd_rn(m, u)), (float)a.n_ants));
-        a.seeds[i] = (v >= -2147483648.0f && v < 2147483648.0f) ? __float2int_rz(v) : (int)0x80000000;
+        uint32_t x = pm_mul((uint32_t)r, pm_pow16807(i0 + 1)); // draw i0 + 1; the next ones one step apart
+        const float av = (float)a.n_ants;
+        for (int k = 0; k < kSeedRun; k++) {
+            const long long i = i0 + k;
+            const float m = (float)(int)(i % a.n_ants);
+            const float v = __fadd_rn(t0, __fmul_rn(__fmul_rn(m, __fadd_rn(m, pm_uniform(x))), av));
+            a.seeds[i] = (v >= -2147483648.0f && v < 2147483648.0f) ? __float2int_rz(v) : (int)0x80000000;
+            x = pm_mul(x, 16807u);
+        }
     }
 }
 
@@ -277,11 +330,12 @@ cudaError_t launch_prep_batch(const PrepArgs *d_args, const int *d_row_base, con
         lists_rows_kernel<<<std::max(lblocks, 1), 32 * rows, smem, st>>>(d_args, d_row_base, d_row_inst, total_rows,
                                                                          rows, n_max, status);
     }
-    const long long total = (long long)total_ants * nloc;
-    if (total > 0) {
-        long long blocks = (total + 255) / 256;
+    if (nloc % kSeedRun != 0) return cudaErrorInvalidValue;
+    const long long runs = (long long)total_ants * (nloc / kSeedRun);
+    if (runs > 0) {
+        long long blocks = (runs + 255) / 256;
         if (blocks > sm_count * 8) blocks = sm_count * 8;
-        seeds_kernel<<<(unsigned)blocks, 256, 0, st>>>(d_args, d_ant_base, d_ant_inst, total, nloc, seed_time, rnd_seed);
+        seeds_kernel<<<(unsigned)blocks, 256, 0, st>>>(d_args, d_ant_base, d_ant_inst, runs, nloc, seed_time, rnd_seed);
     }
     return cudaGetLastError();
 }

@@ -48,6 +48,39 @@ def test_device_distances_and_lists_equal_host(gpu, maker, dist_type):
         assert np.array_equal(dev_nn, compute_nn_lists(host_d, nn_ls, nn_ants))
 
 
+def test_device_lists_of_arbitrary_matrices(gpu):
+    """The warp's fast path (distinct smallest values) and the quicksort fallback
+    give the host's lists on matrices with negative values, -0, NaN and ties."""
+    import torch
+    rng = np.random.default_rng(5)
+    n = 150
+    ld = (n + 31) // 32 * 32
+    cases = []
+    m = rng.uniform(0, 100, (n, n)).astype(np.float32)
+    cases.append(m.copy())                                   # distinct values: fast path on every row
+    m2 = m.copy()
+    m2[::3, 5] = -1.5                                        # negative entries
+    m2[1::4, 7] = np.float32(-0.0)                           # -0 against +0
+    m2[2::5, 9] = 0.0
+    cases.append(m2)
+    m3 = np.round(m / 10).astype(np.float32)                 # many ties
+    cases.append(m3)
+    m4 = m.copy()
+    m4[::7, 11] = np.nan
+    cases.append(m4)
+    for hm in cases:
+        dd = torch.zeros((n, ld), dtype=torch.float32, device="cuda")
+        dd[:, :n] = torch.tensor(hm, device="cuda")
+        depth = ctypes.c_int()
+        nn = torch.zeros(n * 25, dtype=torch.int32, device="cuda")
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        check(lib().aco_compute_nn_lists_device(n, dd.data_ptr(), ld, 25, 25, nn.data_ptr(), ctypes.byref(depth),
+                                                st), "nn")
+        torch.cuda.synchronize()
+        got = nn.cpu().numpy()[: n * depth.value].reshape(n, depth.value)
+        assert np.array_equal(got, compute_nn_lists(hm, 25, 25))
+
+
 def test_geo_is_left_to_the_host(gpu):
     from cvrp_aco_ocl_b200 import AcoError
     with pytest.raises(AcoError):
