@@ -1,7 +1,9 @@
 """What the trained edge prior buys: on held-out instances (seeds outside the
 training set) the colony with the shipped network's prior reaches shorter
 FP64-checked tours than the plain colony after the same number of
-iterations.  The plain colony is the yardstick and the fallback."""
+iterations, and comes within 1% of the plain colony's final best in at most
+half of its wall time (the metric's second half, here on a small case).  The
+plain colony is the yardstick and the fallback."""
 import numpy as np
 import pytest
 
@@ -43,3 +45,15 @@ def test_prior_beats_plain_at_equal_iterations(gpu):
     gains = [(p - l) / p for p, l in zip(plain, learned)]
     assert sum(g > 0 for g in gains) >= 2, gains
     assert np.mean(gains) > 0.005, gains
+
+
+def test_time_to_equal_cost_gate_small_case(gpu):
+    """Held-out n = 500 instances, 128 ants, 25-NN lists in both arms; the plain
+    colony runs 300 iterations and its FP64-rechecked best (+1%) is the target;
+    the learned colony's clock includes graph build, network forward and prior
+    upload.  Gate: median time ratio <= 0.5, every tour feasible."""
+    from cvrp_aco_ocl_b200.learned_eval import time_to_equal_cost
+    res = time_to_equal_cost(PR.EdgeScorer.load(), 500, 3, 300, 128, 25)
+    assert res["all_feasible"], res
+    assert res["median_ratio"] is not None and res["median_ratio"] <= 0.5, res
+
