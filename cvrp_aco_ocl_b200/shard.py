@@ -29,7 +29,7 @@ from typing import Dict, List, Optional, Sequence, Tuple
 
 # a, b: ns per ant and node, ns per ant and node^2; bw: bytes per ns of the pheromone pass
 # (measured on a B200 by fit(): batches of 101..1001 nodes, 128 ants, 25-NN lists)
-COST_MODEL = {"a_ns": 0.4377, "b_ns": 0.000284, "bw_bytes_per_ns": 4500.0}
+COST_MODEL = {"a_ns": 0.4181, "b_ns": 0.000172, "bw_bytes_per_ns": 4544.0}
 
 
 def instance_cost(n: int, ants: int, model: Optional[Dict[str, float]] = None) -> float:
