@@ -96,9 +96,10 @@ __device__ void sort_row(float *v, int *idx, int n, int depth, int *status)
 // The first `depth` entries of a staged row's list, warp-wide.  When the
 // depth + 1 smallest values are all distinct, every correct sort puts the same
 // nodes in the first depth positions, so the warp extracts them in depth + 1
-// rounds of a 64-bit warp minimum over (value bits, index) -- values are >= 0,
-// so their bits order as the floats.  Otherwise (a tie decides which node comes
-// first, as with integer coordinates) lane 0 runs the reference's quicksort,
+// rounds of a 64-bit warp minimum over (value bits, index) -- for values from
+// +0 to +inf the bits order as the floats.  Otherwise (a tie decides which node
+// comes first, as with integer coordinates, or a row holds a negative value,
+// -0 or NaN) lane 0 runs the reference's quicksort,
 // whose partition order settles ties exactly as the host's.  On return idx[0,
 // depth) holds the list.
 __device__ void row_list(float *v, int *idx, int n, int depth, int lane, int *status)
@@ -176,10 +177,10 @@ __global__ void dist_rows_kernel(const PrepArgs *pa, const int *row_base, const 
     }
 }
 
-// Lists and tables of every instance's rows: a warp per row stages it, its
-// first lane sorts it (sort_row, as nn_kernel), and the lanes write the
-// candidate tables (first K, padded with node 0 to Kp; demand in the high half
-// of cand32) and the 2-opt list (first nn_ls) straight from the sorted row.
+// Lists and tables of every instance's rows: a warp per row stages it and picks
+// its list (row_list, as nn_kernel), and the lanes write the candidate tables
+// (first K, padded with node 0 to Kp; demand in the high half of cand32) and
+// the 2-opt list (first nn_ls) straight from the list.
 __global__ void lists_rows_kernel(const PrepArgs *pa, const int *row_base, const int *row_inst, int total_rows,
                                   int rows_per_cta, int n_max, int *status)
 {
