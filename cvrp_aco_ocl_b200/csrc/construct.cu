@@ -1086,15 +1086,18 @@ cudaError_t launch_construct_nn(const ConstructArgs *d_args, const int2 *d_items
                              : (finite_maxd ? construct_nn_kernel<true, 0> : construct_nn_kernel<false, 0>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    int per_sm = (int)(228 * 1024 / (smem + 1024));
-    if (per_sm < 1) per_sm = 1;
-    int blocks = sm_count * per_sm;
-    if (blocks > n_items) blocks = n_items;
-    if (blocks < 1) blocks = 1;
     int warps = apc < 8 ? 8 : apc; // helper warps share the staging of each item
     if (draw && warps < 2 * apc) warps = 2 * apc;
     if (ls_warps > 0) warps = apc + ls_warps;
     if (warps > 16) return cudaErrorInvalidValue;
+    // a persistent grid: the CTAs that are resident at once (registers and shared memory)
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    int blocks = sm_count * per_sm;
+    if (blocks > n_items) blocks = n_items;
+    if (blocks < 1) blocks = 1;
     kern<<<blocks, warps * 32, smem, st>>>(d_args, d_items, n_items, d_queue, apc, ls_warps, lens_later ? 1 : 0);
     return cudaGetLastError();
 }
