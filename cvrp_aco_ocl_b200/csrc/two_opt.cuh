@@ -137,19 +137,20 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
             const unsigned pstop = __ballot_sync(FULLM, act && (!pc || pok));
             const unsigned smove = __ballot_sync(FULLM, sok), pmove = __ballot_sync(FULLM, pok);
             // the next open position if this examination makes no move, and its head
-            const uint32_t rest = q1 >= 31 ? 0u : (open & ~((2u << q1) - 1u)); // positions > q1
-            const int qn = rest ? __ffs(rest) - 1 : 0;
+            const uint32_t rest = open & ~((2u << q1) - 1u); // positions > q1 (2u << 31 wraps to 0: none)
+            const int qn = __ffs(rest) - 1;                   // -1 when none (the head is then unused)
             const Head hn = head(qn);
-            const int sf = sstop ? __ffs(sstop) - 1 : 0, pf = pstop ? __ffs(pstop) - 1 : 0;
             const bool sfound = (sstop & (0u - sstop) & smove) != 0u; // the lowest stop is a move
             const bool pfound = (pstop & (0u - pstop) & pmove) != 0u;
             int h1, h2, h3, h4;
             if (sfound) {
+                const int sf = __ffs(sstop) - 1;
                 h1 = k1;
                 h2 = ks1;
                 h3 = __shfl_sync(FULLM, k2, sf);
                 h4 = __shfl_sync(FULLM, ks2, sf);
             } else if (pfound) {
+                const int pf = __ffs(pstop) - 1;
                 h1 = kp1;
                 h2 = k1;
                 h3 = __shfl_sync(FULLM, kpp2, pf);
@@ -168,7 +169,7 @@ __device__ int two_opt_route_regs(int lane, int R, bool first_route, const float
             route_exchange(lane, tile, h1, h2, h3, h4, tq, pk, dq);
             by_node();
             open = __ballot_sync(FULLM, lane < R && !((dlb >> tq) & 1u)) & rmask; // the tour and bits changed
-            const uint32_t ahead = q1 >= 31 ? 0u : (open & ~((2u << q1) - 1u)); // the scan goes on after q1
+            const uint32_t ahead = open & ~((2u << q1) - 1u); // the scan goes on after q1
             if (!ahead) break;
             q1 = __ffs(ahead) - 1;
             h = head(q1);
