@@ -63,7 +63,8 @@ def test_invalid_shapes_rejected(gpu):
     from cvrp_aco_ocl_b200 import AcoError
     prob = Problem.from_instance(I.gen_mixed(6, 60))
     n = prob.num_node
-    for kw in (dict(ls_warps=33), dict(stage_matrix=1), dict(mode=MODE_PARITY, ants_per_block=8, warps_per_ant=4)):
+    for kw in (dict(ls_warps=33), dict(stage_matrix=1), dict(mode=MODE_PARITY, ants_per_block=8, warps_per_ant=4),
+               dict(construct_ctas=3), dict(construct_ctas=-1)):
         with pytest.raises(AcoError):
             Solver(prob, params(n, 32, kw.pop("mode", MODE_THROUGHPUT), **kw))
 
