@@ -305,10 +305,12 @@ int aco_batch_autotune(const aco_instance *insts, int count, const aco_params *p
  * ACO_MODE_THROUGHPUT only; every instance has n <= 1024 nodes and its own
  * device state (pheromone, tours, best-so-far, records); instance b uses the
  * seeds of rnd_seed + b.  Lists deeper than an instance allows are clamped to
- * n-2 for it.  One iteration is four launches for the whole batch: a persistent
- * construct kernel over a device work queue of (instance, ant group) items,
- * 2-opt (one CTA per ant), statistics (one CTA per instance) and the row pass
- * over every instance's matrices; replayed as one CUDA graph. */
+ * n-2 for it.  One iteration is four or five launches for the whole batch: a
+ * persistent construct kernel over a device work queue of (instance, ant group)
+ * items, the route-level 2-opt over the construct's route list (with more than
+ * 4 ants per SM) and the per-ant 2-opt for the ants it does not hold,
+ * statistics (one CTA per instance) and the row pass over every instance's
+ * matrices; replayed as one CUDA graph. */
 typedef struct aco_batch aco_batch;
 int aco_batch_create(const aco_instance *insts, int count, const aco_params *params, aco_batch **out);
 int aco_batch_init(aco_batch *b);
