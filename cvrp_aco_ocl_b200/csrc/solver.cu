@@ -726,7 +726,7 @@ int aco_batch_create(const aco_instance *insts, int count, const aco_params *par
     int n_min = INT_MAX;
     std::vector<InstanceSpec> specs(count);
     for (int b = 0; b < count; b++) {
-        if (!spec_ok(insts[b]) || insts[b].n > 1024) return ACO_ERR_INVALID;
+        if (!spec_ok(insts[b])) return ACO_ERR_INVALID;
         n_min = std::min(n_min, insts[b].n);
         specs[b] = spec_of(insts[b]);
     }
@@ -1004,7 +1004,7 @@ int aco_batch_autotune(const aco_instance *insts, int count, const aco_params *p
     std::vector<InstanceSpec> specs(count);
     int n_min = INT_MAX;
     for (int b = 0; b < count; b++) {
-        if (!spec_ok(insts[b]) || insts[b].n > 1024) return ACO_ERR_INVALID;
+        if (!spec_ok(insts[b])) return ACO_ERR_INVALID;
         n_min = std::min(n_min, insts[b].n);
         specs[b] = spec_of(insts[b]);
     }

@@ -302,8 +302,8 @@ int aco_batch_autotune(const aco_instance *insts, int count, const aco_params *p
 
 /* ---- batches: many independent instances in the same launches --------------
  * No reference counterpart (the reference solves one instance per process).
- * ACO_MODE_THROUGHPUT only; every instance has n <= 1024 nodes and its own
- * device state (pheromone, tours, best-so-far, records); instance b uses the
+ * ACO_MODE_THROUGHPUT only; every instance has its own device state
+ * (pheromone, tours, best-so-far, records); instance b uses the
  * seeds of rnd_seed + b.  Lists deeper than an instance allows are clamped to
  * n-2 for it.  One iteration is four or five launches for the whole batch: a
  * persistent construct kernel over a device work queue of (instance, ant group)

@@ -62,6 +62,8 @@ def assert_same(B, b, S):
     # through L2) against single solvers at one CTA per SM
     ([40, 120, 200, 75, 333, 64, 700, 999], 48, {"construct_ctas": 2}),
     ([150, 420, 1000], 96, {"construct_ctas": 2, "route_ls": 1}),
+    # instances beyond 1024 nodes (register visited set off, candidate tables through L2) beside small ones
+    ([1100, 300, 1500, 64], 40, {}),
 ])
 def test_batch_members_match_single_solvers(gpu, sizes, A, kw):
     probs = mixed_problems(300 + len(sizes), sizes)
@@ -155,15 +157,16 @@ def test_batch_tours_valid(gpu):
                 assert abs(oracle.tour_length_f64(dist, t) - float(lens[a])) <= 1e-5 * float(lens[a])
 
 
-def test_batch_rejects_parity_mode_and_large_instances(gpu):
+def test_batch_rejects_parity_mode_and_bad_instances(gpu):
     probs = mixed_problems(1, [50, 60])
     p = batch_params(61, 8, 1)
     p.mode = 0
     with pytest.raises(AcoError):
         Batch(probs, p)
-    big = mixed_problems(2, [1100])
+    bad = mixed_problems(2, [40, 50])
+    bad[1].demand[3] = bad[1].vehicle_capacity + 1  # a customer no vehicle can serve
     with pytest.raises(AcoError):
-        Batch(big, batch_params(1101, 8, 1))
+        Batch(bad, batch_params(51, 8, 1))
 
 
 def test_pipelined_length_readback(gpu):
