@@ -505,6 +505,35 @@ __device__ __forceinline__ int min_open_demand(const int *s_dem, uint32_t vis, c
     return (int)__reduce_min_sync(0xffffffffu, (unsigned)m);
 }
 
+// The same with the number of unvisited customers that have it (0 when none
+// is left): visiting one of them lowers the count, and only when it reaches 0
+// can the smallest demand have changed.
+template <bool REGVIS>
+__device__ __forceinline__ int min_open_demand_count(const int *s_dem, uint32_t vis, const uint32_t *vism, int n,
+                                                     int words, int lane, int &count)
+{
+    int m = 0x7fffffff, c = 0;
+    if (REGVIS) {
+        for (uint32_t o = open_bits(vis, n, lane); o; o &= o - 1u) {
+            const int d = s_dem[lane + 32 * (__ffs(o) - 1)];
+            c = d < m ? 1 : c + (d == m ? 1 : 0);
+            m = min(m, d);
+        }
+    } else {
+        for (int k = 0; k < words; k++) {
+            const int i = lane + 32 * k;
+            if (i > 0 && i < n && !((vism[k] >> lane) & 1u)) {
+                const int d = s_dem[i];
+                c = d < m ? 1 : c + (d == m ? 1 : 0);
+                m = min(m, d);
+            }
+        }
+    }
+    const int gm = (int)__reduce_min_sync(0xffffffffu, (unsigned)m);
+    count = (int)__reduce_add_sync(0xffffffffu, (unsigned)(m == gm ? c : 0));
+    return gm;
+}
+
 // The feasible customer of the full row with the largest total_info (ties:
 // lowest index), -1 if none: the step's path when no listed candidate fits.
 // PRUNE (register visited set only): test the demands first, from shared
@@ -602,25 +631,26 @@ __device__ __forceinline__ int best_of_row(const float *row, const int *s_dem, c
 }
 
 struct FallbackPick {
-    int nxt, mind; // nxt -1: no customer fits
+    int nxt, mind, mcnt; // nxt -1: no customer fits
 };
 
 // best_of_row out of line, for the kernel without helper warps (many ants per
 // SM), with a shortcut: mind is the smallest demand among unvisited customers
-// (refreshed here when stale); when even it does not fit, no customer does and
-// the row is not scanned.  Measured: the shortcut and the call pay off there,
+// and mcnt the number of them that have it (recounted here when it has dropped
+// to 0); when even mind does not fit, no customer does and the row is not
+// scanned.  Measured: the shortcut and the call pay off there,
 // while in the helper-warp kernel (one ant warp per SMSP, latency bound) the
 // plain inline scan is faster, so that kernel keeps it.
 template <bool FIN, bool REGVIS>
 __device__ __noinline__ FallbackPick fallback_pick(const float *row, const int *s_dem, const float *s_d0,
                                                    const float *drow, uint32_t vis, const uint32_t *vism, int n,
                                                    int words, int lane, int load, int cap, float rdist, float serv,
-                                                   float maxd, int mind, bool stale)
+                                                   float maxd, int mind, int mcnt)
 {
-    if (stale) mind = min_open_demand<REGVIS>(s_dem, vis, vism, n, words, lane);
-    if (mind > cap - load) return {-1, mind};
+    if (mcnt <= 0) mind = min_open_demand_count<REGVIS>(s_dem, vis, vism, n, words, lane, mcnt);
+    if (mind > cap - load) return {-1, mind, mcnt};
     return {best_of_row<FIN, REGVIS>(row, s_dem, s_d0, drow, vis, vism, n, words, lane, load, cap, rdist, serv, maxd),
-            mind};
+            mind, mcnt};
 }
 
 // lens_later: the route-level 2-opt follows and writes every listed ant's
@@ -728,11 +758,11 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             __syncwarp();
         }
         if (lane == 0) tbuf[0] = 0;
-        // smallest demand among the unvisited customers (fallback_pick): visits
-        // only raise it, so it is refreshed lazily, on the fallback path, after
-        // the customer holding it has been visited
-        int mind = DRAW ? 0 : min_open_demand<REGVIS>(s_dem, vis, vism, n, words, lane);
-        bool mind_stale = false;
+        // smallest demand among the unvisited customers and how many have it
+        // (fallback_pick): visits only raise it, so it is recounted lazily, on the
+        // fallback path, once every customer holding it has been visited
+        int mcnt = 1;
+        int mind = DRAW ? 0 : min_open_demand_count<REGVIS>(s_dem, vis, vism, n, words, lane, mcnt);
         // lane l draws from the ant's Park-Miller state l (nloc >= 32), one number a step
         int *seedp = a.seeds + (size_t)ant * a.nloc;
         uint32_t xs = pm_norm(seed0);
@@ -797,9 +827,9 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
             } else {
                 const FallbackPick fp = fallback_pick<FIN, REGVIS>(
                     SMAT ? s_mat + cur * n4 : a.total + (size_t)cur * ld, s_dem, s_d0, a.dist + (size_t)cur * ld, vis,
-                    vism, n, words, lane, load, cap, rdist, a.serv_time, a.max_dist, mind, mind_stale);
+                    vism, n, words, lane, load, cap, rdist, a.serv_time, a.max_dist, mind, mcnt);
                 mind = fp.mind;
-                mind_stale = false;
+                mcnt = fp.mcnt;
                 nxt = fp.nxt;
                 if (nxt >= 0) nd = s_dem[nxt];
             }
@@ -819,7 +849,7 @@ __device__ __forceinline__ bool construct_nn_item(const ConstructArgs &a, int ap
                 if (lane == 0) vism[nxt >> 5] |= 1u << (nxt & 31);
                 __syncwarp();
             }
-            if (!DRAW) mind_stale |= nxt != 0 && nd == mind; // the smallest may have gone
+            if (!DRAW && nxt != 0 && nd == mind) mcnt--; // one customer of the smallest demand fewer
             if (lane == 0) tbuf[step] = (uint16_t)nxt;
             if (LSF) {
                 if (nxt != 0) {
