@@ -156,57 +156,72 @@ __device__ int two_opt_route_generic(Route &c, int pass_limit)
             float radius = c.D(n1, s1);
             bool found = false;
             int h1 = 0, h2 = 0, h3 = 0, h4 = 0;
-            for (int h0 = 0; h0 < c.nn_ls; h0 += 32) {
-                const int h = h0 + lane;
-                const bool valid = h < c.nn_ls;
-                const int n2 = valid ? __ldg(c.nn + (size_t)n1 * c.nn_ls + h) : 0;
+            if (c.nn_ls <= 32) {
+                // one list of at most 32 entries: both searches from one load of it, the
+                // predecessor's result used only when the successor search finds no move
+                const int p1 = pos1 == rb ? c.tour[re] : c.tour[pos1 - 1];
+                const float rp = c.D(p1, n1);
+                const bool valid = lane < c.nn_ls;
+                const int n2 = valid ? __ldg(c.nn + (size_t)n1 * c.nn_ls + lane) : 0;
                 const bool inr = valid && c.in_route(n2);
-                bool cond = false, okm = false;
-                int s2 = 0;
+                bool sc = false, sok = false, pc = false, pok = false;
+                int s2 = 0, pp2 = 0;
                 if (inr) {
                     const float d12 = c.D(n1, n2);
-                    cond = __fsub_rn(radius, d12) > kEps;
-                    if (cond) {
-                        const int p2 = c.pos[n2];
+                    sc = __fsub_rn(radius, d12) > kEps;
+                    pc = __fsub_rn(rp, d12) > kEps;
+                    const int p2 = c.pos[n2];
+                    if (sc) {
                         s2 = p2 == re ? c.tour[rb] : c.tour[p2 + 1];
                         const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), c.D(s1, s2)), c.dt[p2]);
-                        okm = g < -kEps;
+                        sok = g < -kEps;
+                    }
+                    if (pc) {
+                        pp2 = p2 == rb ? c.tour[re] : c.tour[p2 - 1];
+                        if (!(pp2 == n1 || p1 == n2)) {
+                            const float g = __fsub_rn(__fadd_rn(__fadd_rn(-rp, d12), c.D(p1, pp2)), c.dt[p2 - 1]);
+                            pok = g < -kEps;
+                        }
                     }
                 }
-                const unsigned stop = __ballot_sync(FULL, inr && (!cond || okm));
-                if (stop) {
-                    const int f = __ffs(stop) - 1;
-                    if (__shfl_sync(FULL, (int)cond, f)) {
+                const unsigned sstop = __ballot_sync(FULL, inr && (!sc || sok));
+                const unsigned pstop = __ballot_sync(FULL, inr && (!pc || pok));
+                if (sstop) { // successor search
+                    const int f = __ffs(sstop) - 1;
+                    if (__shfl_sync(FULL, (int)sc, f)) {
                         found = true;
                         h1 = n1;
                         h2 = s1;
                         h3 = __shfl_sync(FULL, n2, f);
                         h4 = __shfl_sync(FULL, s2, f);
                     }
-                    break;
                 }
-            }
-            if (!found) {
-                const int p1 = pos1 == rb ? c.tour[re] : c.tour[pos1 - 1];
-                radius = c.D(p1, n1);
+                if (!found && pstop) { // predecessor search
+                    const int f = __ffs(pstop) - 1;
+                    if (__shfl_sync(FULL, (int)pc, f)) {
+                        found = true;
+                        h1 = p1;
+                        h2 = n1;
+                        h3 = __shfl_sync(FULL, pp2, f);
+                        h4 = __shfl_sync(FULL, n2, f);
+                    }
+                }
+            } else {
                 for (int h0 = 0; h0 < c.nn_ls; h0 += 32) {
                     const int h = h0 + lane;
                     const bool valid = h < c.nn_ls;
                     const int n2 = valid ? __ldg(c.nn + (size_t)n1 * c.nn_ls + h) : 0;
                     const bool inr = valid && c.in_route(n2);
                     bool cond = false, okm = false;
-                    int pp2 = 0;
+                    int s2 = 0;
                     if (inr) {
                         const float d12 = c.D(n1, n2);
                         cond = __fsub_rn(radius, d12) > kEps;
                         if (cond) {
                             const int p2 = c.pos[n2];
-                            pp2 = p2 == rb ? c.tour[re] : c.tour[p2 - 1];
-                            if (!(pp2 == n1 || p1 == n2)) {
-                                const float g =
-                                    __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), c.D(p1, pp2)), c.dt[p2 - 1]);
-                                okm = g < -kEps;
-                            }
+                            s2 = p2 == re ? c.tour[rb] : c.tour[p2 + 1];
+                            const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), c.D(s1, s2)), c.dt[p2]);
+                            okm = g < -kEps;
                         }
                     }
                     const unsigned stop = __ballot_sync(FULL, inr && (!cond || okm));
@@ -214,12 +229,49 @@ __device__ int two_opt_route_generic(Route &c, int pass_limit)
                         const int f = __ffs(stop) - 1;
                         if (__shfl_sync(FULL, (int)cond, f)) {
                             found = true;
-                            h1 = p1;
-                            h2 = n1;
-                            h3 = __shfl_sync(FULL, pp2, f);
-                            h4 = __shfl_sync(FULL, n2, f);
+                            h1 = n1;
+                            h2 = s1;
+                            h3 = __shfl_sync(FULL, n2, f);
+                            h4 = __shfl_sync(FULL, s2, f);
                         }
                         break;
+                    }
+                }
+                if (!found) {
+                    const int p1 = pos1 == rb ? c.tour[re] : c.tour[pos1 - 1];
+                    radius = c.D(p1, n1);
+                    for (int h0 = 0; h0 < c.nn_ls; h0 += 32) {
+                        const int h = h0 + lane;
+                        const bool valid = h < c.nn_ls;
+                        const int n2 = valid ? __ldg(c.nn + (size_t)n1 * c.nn_ls + h) : 0;
+                        const bool inr = valid && c.in_route(n2);
+                        bool cond = false, okm = false;
+                        int pp2 = 0;
+                        if (inr) {
+                            const float d12 = c.D(n1, n2);
+                            cond = __fsub_rn(radius, d12) > kEps;
+                            if (cond) {
+                                const int p2 = c.pos[n2];
+                                pp2 = p2 == rb ? c.tour[re] : c.tour[p2 - 1];
+                                if (!(pp2 == n1 || p1 == n2)) {
+                                    const float g =
+                                        __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), c.D(p1, pp2)), c.dt[p2 - 1]);
+                                    okm = g < -kEps;
+                                }
+                            }
+                        }
+                        const unsigned stop = __ballot_sync(FULL, inr && (!cond || okm));
+                        if (stop) {
+                            const int f = __ffs(stop) - 1;
+                            if (__shfl_sync(FULL, (int)cond, f)) {
+                                found = true;
+                                h1 = p1;
+                                h2 = n1;
+                                h3 = __shfl_sync(FULL, pp2, f);
+                                h4 = __shfl_sync(FULL, n2, f);
+                            }
+                            break;
+                        }
                     }
                 }
             }
@@ -558,72 +610,124 @@ __device__ int two_opt_route_local(int lane, int R, const float *dist, int ld, c
             const int n1 = nodes[k1];
             int h1 = 0, h2 = 0, h3 = 0, h4 = 0;
             bool found = false;
-            {   // successor search (kernel.cl:180-198)
-                const int ks1 = tk[l + 1 < R ? l + 1 : 0];
-                const float radius = D(n1, nodes[ks1]);
-                for (int h0 = 0; h0 < nn_ls; h0 += 32) {
-                    const int h = h0 + lane;
-                    const int n2 = h < nn_ls ? __ldg(nn + (size_t)n1 * nn_ls + h) : 0;
-                    const int kk2 = loc[n2];
-                    bool cond = false, okm = false;
-                    int ks2 = 0;
-                    if (kk2 != 0) {
-                        const float d12 = D(n1, n2);
-                        cond = __fsub_rn(radius, d12) > kEps;
-                        if (cond) {
-                            const int p2 = pk[kk2];
-                            ks2 = tk[p2 + 1 < R ? p2 + 1 : 0];
-                            const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), D(nodes[ks1], nodes[ks2])), dq[p2]);
-                            okm = g < -kEps;
-                        }
+            if (nn_ls <= 32) {
+                // one list of at most 32 entries: both searches from one load of it, the
+                // predecessor's result used only when the successor search finds no move
+                const int ks1 = tk[l + 1 < R ? l + 1 : 0], kp1 = tk[l > 0 ? l - 1 : R - 1];
+                const int ns1 = nodes[ks1], np1 = nodes[kp1];
+                const float rs = D(n1, ns1), rp = D(np1, n1);
+                const int n2 = lane < nn_ls ? __ldg(nn + (size_t)n1 * nn_ls + lane) : 0;
+                const int kk2 = loc[n2];
+                bool sc = false, sok = false, pc = false, pok = false;
+                int ks2 = 0, kpp2 = 0;
+                if (kk2 != 0) {
+                    const float d12 = D(n1, n2);
+                    sc = __fsub_rn(rs, d12) > kEps;
+                    pc = __fsub_rn(rp, d12) > kEps;
+                    const int p2 = pk[kk2];
+                    if (sc) {
+                        ks2 = tk[p2 + 1 < R ? p2 + 1 : 0];
+                        const float g = __fsub_rn(__fadd_rn(__fadd_rn(-rs, d12), D(ns1, nodes[ks2])), dq[p2]);
+                        sok = g < -kEps;
                     }
-                    const unsigned stop = __ballot_sync(FULL, kk2 != 0 && (!cond || okm));
-                    if (stop) {
-                        const int f = __ffs(stop) - 1;
-                        if (__shfl_sync(FULL, (int)cond, f)) {
-                            found = true;
-                            h1 = k1;
-                            h2 = ks1;
-                            h3 = __shfl_sync(FULL, kk2, f);
-                            h4 = __shfl_sync(FULL, ks2, f);
+                    if (pc) {
+                        kpp2 = tk[p2 > 0 ? p2 - 1 : R - 1];
+                        if (!(kpp2 == k1 || kp1 == kk2)) {
+                            const float g = __fsub_rn(__fadd_rn(__fadd_rn(-rp, d12), D(np1, nodes[kpp2])), dq[p2 - 1]);
+                            pok = g < -kEps;
                         }
-                        break;
                     }
                 }
-            }
-            if (!found) { // predecessor search (kernel.cl:202-230)
-                const int kp1 = tk[l > 0 ? l - 1 : R - 1];
-                const float radius = D(nodes[kp1], n1);
-                for (int h0 = 0; h0 < nn_ls; h0 += 32) {
-                    const int h = h0 + lane;
-                    const int n2 = h < nn_ls ? __ldg(nn + (size_t)n1 * nn_ls + h) : 0;
-                    const int kk2 = loc[n2];
-                    bool cond = false, okm = false;
-                    int kpp2 = 0;
-                    if (kk2 != 0) {
-                        const float d12 = D(n1, n2);
-                        cond = __fsub_rn(radius, d12) > kEps;
-                        if (cond) {
-                            const int p2 = pk[kk2];
-                            kpp2 = tk[p2 > 0 ? p2 - 1 : R - 1];
-                            if (!(kpp2 == k1 || kp1 == kk2)) {
-                                const float g =
-                                    __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), D(nodes[kp1], nodes[kpp2])), dq[p2 - 1]);
+                const unsigned sstop = __ballot_sync(FULL, kk2 != 0 && (!sc || sok));
+                const unsigned pstop = __ballot_sync(FULL, kk2 != 0 && (!pc || pok));
+                if (sstop) { // successor search (kernel.cl:180-198)
+                    const int f = __ffs(sstop) - 1;
+                    if (__shfl_sync(FULL, (int)sc, f)) {
+                        found = true;
+                        h1 = k1;
+                        h2 = ks1;
+                        h3 = __shfl_sync(FULL, kk2, f);
+                        h4 = __shfl_sync(FULL, ks2, f);
+                    }
+                }
+                if (!found && pstop) { // predecessor search (kernel.cl:202-230)
+                    const int f = __ffs(pstop) - 1;
+                    if (__shfl_sync(FULL, (int)pc, f)) {
+                        found = true;
+                        h1 = kp1;
+                        h2 = k1;
+                        h3 = __shfl_sync(FULL, kpp2, f);
+                        h4 = __shfl_sync(FULL, kk2, f);
+                    }
+                }
+            } else {
+                {   // successor search (kernel.cl:180-198)
+                    const int ks1 = tk[l + 1 < R ? l + 1 : 0];
+                    const float radius = D(n1, nodes[ks1]);
+                    for (int h0 = 0; h0 < nn_ls; h0 += 32) {
+                        const int h = h0 + lane;
+                        const int n2 = h < nn_ls ? __ldg(nn + (size_t)n1 * nn_ls + h) : 0;
+                        const int kk2 = loc[n2];
+                        bool cond = false, okm = false;
+                        int ks2 = 0;
+                        if (kk2 != 0) {
+                            const float d12 = D(n1, n2);
+                            cond = __fsub_rn(radius, d12) > kEps;
+                            if (cond) {
+                                const int p2 = pk[kk2];
+                                ks2 = tk[p2 + 1 < R ? p2 + 1 : 0];
+                                const float g = __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), D(nodes[ks1], nodes[ks2])), dq[p2]);
                                 okm = g < -kEps;
                             }
                         }
-                    }
-                    const unsigned stop = __ballot_sync(FULL, kk2 != 0 && (!cond || okm));
-                    if (stop) {
-                        const int f = __ffs(stop) - 1;
-                        if (__shfl_sync(FULL, (int)cond, f)) {
-                            found = true;
-                            h1 = kp1;
-                            h2 = k1;
-                            h3 = __shfl_sync(FULL, kpp2, f);
-                            h4 = __shfl_sync(FULL, kk2, f);
+                        const unsigned stop = __ballot_sync(FULL, kk2 != 0 && (!cond || okm));
+                        if (stop) {
+                            const int f = __ffs(stop) - 1;
+                            if (__shfl_sync(FULL, (int)cond, f)) {
+                                found = true;
+                                h1 = k1;
+                                h2 = ks1;
+                                h3 = __shfl_sync(FULL, kk2, f);
+                                h4 = __shfl_sync(FULL, ks2, f);
+                            }
+                            break;
                         }
-                        break;
+                    }
+                }
+                if (!found) { // predecessor search (kernel.cl:202-230)
+                    const int kp1 = tk[l > 0 ? l - 1 : R - 1];
+                    const float radius = D(nodes[kp1], n1);
+                    for (int h0 = 0; h0 < nn_ls; h0 += 32) {
+                        const int h = h0 + lane;
+                        const int n2 = h < nn_ls ? __ldg(nn + (size_t)n1 * nn_ls + h) : 0;
+                        const int kk2 = loc[n2];
+                        bool cond = false, okm = false;
+                        int kpp2 = 0;
+                        if (kk2 != 0) {
+                            const float d12 = D(n1, n2);
+                            cond = __fsub_rn(radius, d12) > kEps;
+                            if (cond) {
+                                const int p2 = pk[kk2];
+                                kpp2 = tk[p2 > 0 ? p2 - 1 : R - 1];
+                                if (!(kpp2 == k1 || kp1 == kk2)) {
+                                    const float g =
+                                        __fsub_rn(__fadd_rn(__fadd_rn(-radius, d12), D(nodes[kp1], nodes[kpp2])), dq[p2 - 1]);
+                                    okm = g < -kEps;
+                                }
+                            }
+                        }
+                        const unsigned stop = __ballot_sync(FULL, kk2 != 0 && (!cond || okm));
+                        if (stop) {
+                            const int f = __ffs(stop) - 1;
+                            if (__shfl_sync(FULL, (int)cond, f)) {
+                                found = true;
+                                h1 = kp1;
+                                h2 = k1;
+                                h3 = __shfl_sync(FULL, kpp2, f);
+                                h4 = __shfl_sync(FULL, kk2, f);
+                            }
+                            break;
+                        }
                     }
                 }
             }
