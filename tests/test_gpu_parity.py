@@ -155,17 +155,20 @@ def test_throughput_route_length_limit_vs_oracle(gpu, draw):
         assert S.validate()[1] == 0
 
 
-@pytest.mark.parametrize("per_route,n_cust,A", [(12.0, 200, 100), (45.0, 200, 40), (2.0, 150, 24), (300.0, 600, 12)])
-def test_route_level_2opt_vs_oracle(gpu, per_route, n_cust, A):
+@pytest.mark.parametrize("per_route,n_cust,A,nn_ls", [(12.0, 200, 100, 25), (45.0, 200, 40, 25), (2.0, 150, 24, 25),
+                                                     (300.0, 600, 12, 25), (45.0, 200, 40, 60)])
+def test_route_level_2opt_vs_oracle(gpu, per_route, n_cust, A, nn_ls):
     """route_ls = 1: the construct lists every route of at most 255 nodes and one
     persistent kernel improves them, in registers up to 32 nodes (12 customers
-    a route), through the route-local path beyond (45 customers a route); many
-    short routes (2 customers a route) fill the list; an ant with a route of
-    more than 255 nodes (300 customers a route) lists none and goes to the
-    per-ant kernel.  Same bits as the oracle and as the per-ant kernel alone."""
+    a route), through the route-local path beyond (45 customers a route; with
+    2-opt lists of 25 entries both searches of an examination come from one load
+    of the list, with 60 entries they run one after the other); many short
+    routes (2 customers a route) fill the list; an ant with a route of more than
+    255 nodes (300 customers a route) lists none and goes to the per-ant kernel.
+    Same bits as the oracle and as the per-ant kernel alone."""
     inst = I.gen_mixed(900 + n_cust, n_cust, customers_per_route=per_route)
-    S, O = build_pair(inst, A, 256, 1796300000, 93, True, 25, mode=MODE_THROUGHPUT, nn_ants=25, route_ls=1)
-    p2 = params_for(inst.n, A, 256, 1796300000, 93, True, 25, mode=MODE_THROUGHPUT, nn_ants=25, route_ls=-1)
+    S, O = build_pair(inst, A, 256, 1796300000, 93, True, nn_ls, mode=MODE_THROUGHPUT, nn_ants=25, route_ls=1)
+    p2 = params_for(inst.n, A, 256, 1796300000, 93, True, nn_ls, mode=MODE_THROUGHPUT, nn_ants=25, route_ls=-1)
     prob = problem_of(inst.x, inst.y, inst.demand, inst.capacity)
     with S, Solver(prob, p2) as S2:
         S.init(); S2.init(); O.init_aco(throughput=True)
