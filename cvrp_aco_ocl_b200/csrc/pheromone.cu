@@ -317,8 +317,10 @@ __device__ __forceinline__ void update_row_stream(const UpdateArgs &a, int i, in
                     tot.z = __fmul_rn(pow_rule(o.z, a.alpha, a.alpha_int), h[u].z);
                     tot.w = __fmul_rn(pow_rule(o.w, a.alpha, a.alpha_int), h[u].w);
                 }
-                tp[32 * u] = o;
-                op[32 * u] = tot;
+                // tau is read again only in the next pass: evict first; total_info stays in L2
+                // for the candidate gather below and the next construct
+                __stcs(tp + 32 * u, o);
+                __stcg(op + 32 * u, tot);
             }
         }
     }
@@ -417,9 +419,9 @@ __device__ __forceinline__ void row_pass(const UpdateArgs &a, int i, int mode, f
     }
     if (a.chc) { // compact candidate table: chc[i][j] = 1 / total[i][nn[i][j]] (the race's reciprocal weight)
         // the row was written by this warp; __syncwarp orders those stores before
-        // the re-reads below (they hit L2, the lines were just written)
+        // the re-reads below, which read L2, where the lines were just written
         __syncwarp();
-        if (lane < a.K) a.chc[(size_t)i * a.Kp + lane] = __fdiv_rn(1.0f, a.total[off + cid]);
+        if (lane < a.K) a.chc[(size_t)i * a.Kp + lane] = __fdiv_rn(1.0f, __ldcg(a.total + off + cid));
     }
 }
 
