@@ -242,9 +242,9 @@ __device__ __forceinline__ void deposit4_depot(const UpdateArgs &a, int c4, floa
 }
 
 // Float4 per lane per chunk of the evaporation pass: every load of a chunk is
-// issued before its arithmetic, so a lane keeps four float4 of each input
-// matrix in flight.
-constexpr int kU = 4;
+// issued before its arithmetic, so a lane keeps three float4 of each input
+// matrix in flight (measured: 2% faster than four with the cache-policy stores).
+constexpr int kU = 3;
 constexpr int kRowWarps = 8; // warps (rows in flight) per CTA of the row kernel
 
 // Evaporation + deposit + total_info over customer row i, U float4 per lane
