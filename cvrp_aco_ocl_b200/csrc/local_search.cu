@@ -823,7 +823,7 @@ __global__ void __launch_bounds__(512, 2) route_opt_kernel(const LocalSearchArgs
             const int st = two_opt_route_local(lane, R, a.dist, a.ld, a.nn_list, a.nn_ls, loc, nodes, tk, pk, dlb, dq,
                                                a.pass_limit);
             if (st != ACO_OK && lane == 0) set_status(a.status, st);
-            for (int k = lane; k < R; k += 32) gt[rb + k] = nodes[tk[k]];
+            for (int k = lane; k < R; k += 32) __stcs(gt + rb + k, (int)nodes[tk[k]]);
             for (int k = 1 + lane; k < R; k += 32) loc[nodes[k]] = 0;
             __syncwarp();
         } else {
@@ -872,7 +872,7 @@ __global__ void __launch_bounds__(512, 2) route_opt_kernel(const LocalSearchArgs
                               : two_opt_route_regs(lane, R, rb == 0, tile, lnn, lcnt, tq, pk, dq, a.pass_limit);
         if (st != ACO_OK && lane == 0) set_status(a.status, st);
         const int node = __shfl_sync(FULL, v, tq);
-        if (lane < R) gt[rb + lane] = node;
+        if (lane < R) __stcs(gt + rb + lane, node); // evict first: not read again before the statistics
         if (lane >= 1 && lane < R) loc[v] = 0;
         __syncwarp();
         }
